@@ -1,0 +1,164 @@
+/*
+ * vxr.h — the C ABI of the B200-native rigid-body step.
+ *
+ * A drop-in for the reference's per-step pipeline (sibarum/vexelray-sim-rigid). Each entry point names the
+ * reference interface it replaces, by path inside that project:
+ *   gui  = vexelray-sim-rigid-gui/src/main/java/dev/vexelray/sim/rigid/gui/
+ *   core = vexelray-sim-rigid-core/src/main/java/dev/vexelray/sim/rigid/
+ *
+ * Plain pointers and sizes only. Host buffers are caller-owned and copied in or out before the call returns;
+ * the library owns all device memory of a world. One world = one host thread (as the reference: "not
+ * thread-safe: one stepper, one thread", core/sphere/SphereStepper.java:19) and one CUDA stream of its own.
+ * Every entry point returns a status (VXR_OK or an error below); vxr_box_error() gives the text of the last
+ * error of a world.
+ */
+#ifndef VXR_H
+#define VXR_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference throws IllegalArgumentException for bad parameters or sizes
+ * (core/box/Boxes.java:212-226, core/box/BoxStep.java:118-121) and IllegalStateException for a pass that never
+ * ends (core/sphere/SphereStepper.java:86-88); soft failures it counts in its reports. */
+#define VXR_OK 0
+#define VXR_EINVAL 1     /* bad argument: IllegalArgumentException in the reference */
+#define VXR_ECAPACITY 2  /* more candidate pairs than the world's pair capacity */
+#define VXR_EROUNDS 3    /* the device colouring did not finish within its wave limit */
+#define VXR_ENONFINITE 4 /* non-finite state */
+#define VXR_ETIMEOUT 5   /* a device wait (grid barrier) ran out: the step stopped, the GPU stays usable */
+#define VXR_ECUDA 6      /* a CUDA call failed */
+
+#define VXR_PARAM_COUNT 18   /* core/box/Boxes.java:101 */
+#define VXR_SHOWN_STRIDE 20  /* core/box/Boxes.java:781 */
+#define VXR_SLOTS 32         /* core/box/BoxBroad.java:60 */
+#define VXR_MOST_ROUNDS 32   /* core/box/BoxStep.java:81 */
+#define VXR_BOX_SHAPE 0.0f   /* core/box/Boxes.java:154 */
+#define VXR_SPHERE_SHAPE 1.0f
+
+/* The broad phase's grid: nx * ny * nz cubic cells of side `cell` from the origin
+ * (core/sphere/SphereGrid.java:11-36). */
+typedef struct {
+    int32_t nx, ny, nz;
+    float cell;
+} vxr_grid;
+
+/* A world's shape, fixed at creation: the reference's BoxStep(boxes, substeps, sweeps, symmetric, grid)
+ * (core/box/BoxStep.java:117-198). */
+typedef struct {
+    int32_t bodies;
+    int32_t substeps;
+    int32_t sweeps;      /* sweeps of the solve and as many of the relax per substep */
+    int32_t symmetric;   /* every other sweep backwards */
+    vxr_grid grid;       /* nx = 0: no grid (a lone body, or bodies that never meet) */
+    int32_t reach_cells; /* neighbourhood half-width in cells; 0 or 1 = the reference's 27 cells. Cells narrower
+                            than the reference's rule (core/box/BoxBroad.java:66-68) need 2 or more. */
+    int32_t max_pairs;   /* candidate/touching pair capacity; 0 = bodies * 32, the reference's slot count */
+    int32_t device;      /* CUDA device ordinal */
+} vxr_box_config;
+
+/* What a step took: core/box/BoxStepper.java:308-311 (Report), plus the totals over a vxr_box_step call. */
+typedef struct {
+    int32_t touching;  /* pairs whose manifolds have points (last step) */
+    int32_t points;    /* their points */
+    int32_t rounds;    /* rounds the touching pairs were coloured into */
+    int32_t unplaced;  /* touching pairs left unsolved: every round had one of their bodies */
+    int32_t unlisted;  /* partners the broad phase found and had no slot for */
+    int32_t most_rounds;
+    int64_t unplaced_total;
+    int64_t unlisted_total;
+    int32_t status;
+    int32_t steps;
+} vxr_box_report;
+
+/* Version string of the library. */
+const char* vxr_version(void);
+
+/* The 18 parameter words as f32 bits: replaces Boxes.params(h, gx, gy, gz, sx, sy, sz, muStatic, muKinetic,
+ * margin, muRolling) (core/box/Boxes.java:212-234), softness by Boxes.softness (:242-251). */
+int32_t vxr_box_make_params(double h, double gx, double gy, double gz, double sx, double sy, double sz,
+                            double mu_static, double mu_kinetic, double margin, double mu_rolling, int32_t* out18);
+
+/* The grid over the walled box: replaces BoxBroad.grid (core/box/BoxBroad.java:66-68). */
+int32_t vxr_box_make_grid(double sx, double sy, double sz, double widest_half_diagonal, double margin,
+                          vxr_grid* out);
+
+typedef struct vxr_box_world vxr_box_world;
+
+/* A world on the GPU: replaces new BoxStep(...) + new BoxSimulation(context, step)
+ * (core/box/BoxStep.java:117-198, gui/BoxSimulation.java:34-50). NULL on failure, *status says why. */
+vxr_box_world* vxr_box_create(const vxr_box_config* config, int32_t* status);
+
+/* Releases the world: replaces BoxSimulation.close (gui/BoxSimulation.java:183-188). */
+void vxr_box_destroy(vxr_box_world* world);
+
+/* The text of the world's last error. */
+const char* vxr_box_error(const vxr_box_world* world);
+
+/* Starts from a state: replaces BoxSimulation.start(x, y, z, u, v, w, spin[3][], q[4][], half[3][], shape, im,
+ * params) (gui/BoxSimulation.java:77-108). Each array holds `bodies` floats; spin is the angular velocity in the
+ * world's frame, turned into the angular momentum the body keeps (BoxDiagnostics.momentum, in doubles). Clears
+ * every impulse, as the reference's runner.clear() does. */
+int32_t vxr_box_start(vxr_box_world* world, const float* x, const float* y, const float* z, const float* u,
+                      const float* v, const float* w, const float* const* spin3, const float* const* q4,
+                      const float* const* half3, const float* shape, const float* im, const int32_t* params18);
+
+/* Starts from a state given as the 18 fields x y z u v w lx ly lz qx qy qz qw im hx hy hz shape (angular
+ * momentum, as core/box/BoxStep.java keeps it; the reference's test fixture writes these buffers directly,
+ * vexelray-sim-rigid-core/src/test/java/dev/vexelray/sim/rigid/box/BoxScene.java:141-166). Clears every impulse. */
+int32_t vxr_box_load_state(vxr_box_world* world, const float* const* fields18, const int32_t* params18);
+
+/* New parameters from the next step on: replaces BoxSimulation.params (gui/BoxSimulation.java:111-113). */
+int32_t vxr_box_params(vxr_box_world* world, const int32_t* params18);
+
+/* `steps` steps, waited for: replaces BoxSimulation.stepAndWait (gui/BoxSimulation.java:115-142), which runs
+ * BoxStepper.step (core/box/BoxStepper.java:324-368). The report is the last step's, with totals. */
+int32_t vxr_box_step(vxr_box_world* world, int32_t steps, vxr_box_report* report);
+
+/* `steps` steps enqueued on the world's stream, not waited for; vxr_box_sync waits and reports. Replaces the
+ * non-waiting SphereSimulation.step (gui/SphereSimulation.java:191-193) for boxes. */
+int32_t vxr_box_step_async(vxr_box_world* world, int32_t steps);
+int32_t vxr_box_sync(vxr_box_world* world, vxr_box_report* report);
+
+/* The world's CUDA stream (a cudaStream_t), for a caller that times or orders work against it. */
+void* vxr_box_stream(vxr_box_world* world);
+
+/* The state read back into 13 caller arrays x y z u v w lx ly lz qx qy qz qw: replaces BoxSimulation.state
+ * (gui/BoxSimulation.java:153-160). */
+int32_t vxr_box_state(vxr_box_world* world, float* const* out13);
+
+/* The last step's `shown`, 20 floats a body: replaces BoxSimulation.readShown (gui/BoxSimulation.java:163-165). */
+int32_t vxr_box_read_shown(vxr_box_world* world, float* out);
+
+/* The last step's touching pairs in slot order (the order BoxStepper reads `contacts`,
+ * core/box/BoxStepper.java:339-358): first and second body, point count, the manifold in the reference's 40-word
+ * layout (core/box/BoxContact.java:85-96) and the impulses in its 28-word layout (core/box/BoxPairs.java:48-50).
+ * Any output may be NULL. Returns the number of touching pairs, or minus a status. */
+int32_t vxr_box_touching(vxr_box_world* world, int32_t* first, int32_t* second, int32_t* points, float* manifold40,
+                         float* impulses28, int32_t capacity);
+
+/* The last step's candidate pairs (the broad phase's listed slots, core/box/BoxBroad.java:103-164), sorted
+ * (first, second) flat. Returns their number, or minus a status. */
+int32_t vxr_box_candidates(vxr_box_world* world, int32_t* pairs, int32_t capacity);
+
+/* The wall impulses in the reference's layout: lambda 48 floats a body, rub 144, roll 144
+ * (core/box/Boxes.java:142-147). Any output may be NULL. */
+int32_t vxr_box_walls(vxr_box_world* world, float* lambda48, float* rub144, float* roll144);
+
+/* How many dependency waves the last step's colouring took. */
+int32_t vxr_box_colour_waves(vxr_box_world* world);
+
+/* The narrow phase alone over a caller's pair list: replaces the collide pass BoxContact.collide
+ * (core/box/BoxContact.java:136-246) as the reference's BoxContactTest runs it. fields18 as for
+ * vxr_box_load_state; pairs = first, second, ... (second -1: an empty slot); manifold40 receives 40 floats a pair. */
+int32_t vxr_collide(int32_t bodies, const float* const* fields18, const int32_t* params18, int32_t npairs,
+                    const int32_t* pairs, float* manifold40);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VXR_H */

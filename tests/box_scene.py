@@ -85,7 +85,6 @@ class BoxScene:
                                ("shape", self.shape)):
                 self.world.set_field(name, vals)
             self.world.set_params(self.param_bits())
-            self.world.set_shown(B.shown_at_start(self.x, self.y, self.z, self.q, self.half, self.shape))
         elif backend == "gpu":
             from vxr.box_simulation import BoxSimulation
             self.world = BoxSimulation(self.n, self.substeps, self.passes, self.symmetric, self.grid, **kw)

@@ -1,0 +1,152 @@
+"""The CUDA box/mixed step against the oracle and the reference's known-answer tests, through the C-ABI.
+
+Parity bar: the broad phase's candidate pair set bit-exact (sorted); manifolds, states and impulses equal to the
+oracle's as f32 values (the kernels keep the reference's association order, compiled without contraction, so the
+stated tolerances 1e-5 relative on positions and 1e-4 on impulses are met with room to spare — equality is
+asserted, and a tolerance-based check reports the largest difference when it fails).
+"""
+import numpy as np
+import pytest
+
+import box_cases as C
+from box_scene import BoxScene
+from test_oracle_contact import CASES, check_random_pairs, collide_backend, random_pairs
+from vxr import boxes as B
+
+pytestmark = pytest.mark.gpu
+
+POS_REL = 1e-5
+IMPULSE_ABS = 1e-4
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: c.__name__)
+def test_gpu_hand_cases(case):
+    case("gpu")
+
+
+def manifold_words(m):
+    """The words of a manifold the step reads: normal, count, axis and the count points."""
+    cnt = int(m[B.COUNT])
+    return np.concatenate([m[:5], m[8:8 + 8 * cnt]])
+
+
+def test_gpu_random_pairs_match_the_oracle():
+    solids = random_pairs()
+    gpu = collide_backend("gpu", 0, *solids)
+    check_random_pairs(solids, gpu)
+    orc = collide_backend("oracle", 0, *solids)
+    for p in range(len(solids) // 2):
+        g, o = gpu[40 * p:40 * p + 40], orc[40 * p:40 * p + 40]
+        assert g[B.COUNT] == o[B.COUNT], p
+        if o[B.COUNT] > 0:
+            np.testing.assert_array_equal(manifold_words(g), manifold_words(o), err_msg=f"pair {p}")
+
+
+def run_both(make_scene, steps, **kw):
+    a = make_scene()
+    b = make_scene()
+    a.start("oracle", threads=True)
+    b.start("gpu", **kw)
+    ra = rb = None
+    for _ in range(steps):
+        ra = a.world.step(1)
+        rb = b.world.step(1)
+        assert tuple(ra) == tuple(rb), (tuple(ra), tuple(rb))
+    return a, b
+
+
+def compare_worlds(a, b, exact=True):
+    a.read()
+    b.read()
+    fa = [a.x, a.y, a.z, a.u, a.v, a.w, a.l[0], a.l[1], a.l[2], a.q[0], a.q[1], a.q[2], a.q[3]]
+    fb = [b.x, b.y, b.z, b.u, b.v, b.w, b.l[0], b.l[1], b.l[2], b.q[0], b.q[1], b.q[2], b.q[3]]
+    names = ["x", "y", "z", "u", "v", "w", "lx", "ly", "lz", "qx", "qy", "qz", "qw"]
+    for name, va, vb in zip(names, fa, fb):
+        if name in ("x", "y", "z"):
+            np.testing.assert_allclose(vb, va, rtol=POS_REL, atol=0, err_msg=name)
+        if exact:
+            np.testing.assert_array_equal(vb, va, err_msg=name)
+    pa = a.world.touching_pairs()
+    pb = b.world.touching_pairs()
+    assert pa == pb
+    ma = np.array(a.world.touching_manifolds()).reshape(-1, 40)
+    mb = np.array(b.world.touching_manifolds()).reshape(-1, 40)
+    for k in range(len(pa)):
+        np.testing.assert_array_equal(manifold_words(mb[k]), manifold_words(ma[k]), err_msg=f"manifold {k}")
+    ia = np.array(a.world.touching_impulses()).reshape(-1, 28)
+    ib = np.array(b.world.touching_impulses()).reshape(-1, 28)
+    np.testing.assert_allclose(ib, ia, atol=IMPULSE_ABS, rtol=0)
+    if exact:
+        np.testing.assert_array_equal(ib, ia)
+
+
+def test_gpu_broad_phase_is_the_oracles_pair_set():
+    scene_o = C.broad_fixture()
+    scene_g = C.broad_fixture()
+    scene_o.start("oracle")
+    scene_g.start("gpu")
+    scene_o.advance(1)
+    scene_g.advance(1)
+    co = scene_o.world.candidate_pairs()
+    cg = scene_g.world.candidate_pairs()
+    np.testing.assert_array_equal(cg, co)
+    assert scene_o.world.touching_pairs() == scene_g.world.touching_pairs()
+
+
+def test_gpu_grid_finds_every_pair():
+    C.case_grid_finds_every_pair("gpu")
+
+
+def test_gpu_single_step_of_a_pile_matches_the_oracle():
+    a, b = run_both(lambda: C.pile_scene(7), 1)
+    compare_worlds(a, b)
+
+
+def test_gpu_pile_steps_match_the_oracle_bit_for_bit():
+    a, b = run_both(lambda: C.pile_scene(7), 40)
+    compare_worlds(a, b)
+    la, ra, oa = a.world.buffer("lambda"), a.world.buffer("rub"), a.world.buffer("roll")
+    lb, rb, ob = b.world.walls()
+    np.testing.assert_array_equal(lb, la)
+    np.testing.assert_array_equal(rb, ra)
+
+
+def test_gpu_mixed_pile_steps_match_the_oracle_bit_for_bit():
+    a, b = run_both(C.mixed_pile_scene, 40)
+    compare_worlds(a, b)
+    lb, rb, ob = b.world.walls()
+    np.testing.assert_array_equal(ob, a.world.buffer("roll"))
+
+
+def test_gpu_symmetric_sweeps_match_the_oracle():
+    def make():
+        s = C.mixed_pile_scene()
+        s.symmetric = True
+        s.passes = 3
+        return s
+    a, b = run_both(make, 20)
+    compare_worlds(a, b)
+
+
+def test_gpu_show_matches_the_oracle():
+    a, b = run_both(lambda: C.column_scene(10), 3)
+    np.testing.assert_array_equal(b.world.shown(), a.world.shown())
+
+
+KNOWN = [C.case_free_fall, C.case_stable_spin, C.case_tumble_keeps_momentum_and_energy, C.case_head_on,
+         C.case_column, C.case_flat_rests_flat, C.case_slope_holds, C.case_slope_slides, C.case_ball_rests_on_box,
+         C.case_sliding_ball_rolls, C.case_rolling_resistance, C.case_ball_into_box, C.case_show,
+         C.case_mixed_pile_rests]
+
+
+@pytest.mark.parametrize("case", KNOWN, ids=lambda c: c.__name__)
+def test_gpu_known_answer(case):
+    case("gpu")
+
+
+def test_gpu_pile_of_343_rests():
+    C.case_pile("gpu")
+
+
+def test_gpu_pile_of_1000_rests():
+    C.case_pile("gpu", side=10, most_energy=1e-5, most_depth=2e-3)

@@ -1,0 +1,1526 @@
+// The box/mixed-body step on one B200: broad phase, narrow phase, warm-start carry, colouring and the
+// coloured soft-step solve, all on the device, one stream per world, no host round trip inside a step.
+//
+// The step the reference runs (paths inside sibarum/vexelray-sim-rigid, core =
+// vexelray-sim-rigid-core/src/main/java/dev/vexelray/sim/rigid/):
+//   core/box/BoxStep.java:174-189  collide list: keep, bin, sort, list, collide, carry, counts
+//   core/box/BoxStepper.java:324-368  host wait, greedy colouring, rounds written, substeps run
+//   core/box/BoxStep.java:235-267  per substep: velocities, WARM sweep, sweeps x SOLVE, positions, sweeps x RELAX;
+//                                  each sweep every round of pairs then the walls (reversed: walls first)
+// Here the same passes run as device kernels in one stream. What changes is the layout and the scheduling:
+//   * body state is five float4 arrays (pose+im, turn, half+shape, velocity, angular momentum);
+//   * the 32 slots per body are compacted into a candidate list sorted by (first, second), the slot order;
+//   * only touching pairs carry manifolds' solve data and impulses, double-buffered so "keep" is a swap;
+//   * the host's greedy colouring becomes a device colouring that reproduces it exactly (a pair's round is the
+//     least round free of the rounds of the lower-numbered pairs sharing a body, computed in dependency waves);
+//   * all substeps of a step run in one cooperative kernel, a bounded grid barrier between phases;
+//   * wall contacts that hold no impulse and whose body is far from every wall are skipped without loading
+//     their records (a per-body bit mask says which records are nonzero).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "body_math.cuh"
+#include "grid_sync.cuh"
+#include "narrow.cuh"
+#include "scan.cuh"
+#include "vxr.h"
+
+namespace vxr {
+
+constexpr int SLOTS = 32;
+constexpr int MOST_ROUNDS = 32;
+constexpr int WALL_RECORDS = 48;
+constexpr int SHOWN_STRIDE = 20;
+constexpr int THREADS = 256;
+constexpr int SOLVE_THREADS = 256;
+
+// ------------------------------------------------------------------------------------------------------------
+// Device buffers of a world.
+struct Bodies {
+    float4 *pose, *turn, *half, *vel, *mom;  // (x, y, z, im), (qx, qy, qz, qw), (hx, hy, hz, shape), (u, v, w, 0), (L, 0)
+};
+
+struct PairBuffers {  // one generation of the touching list and its solve data
+    int* tstart;      // [n+1] first touching pair of each body (as first body)
+    int* ta;          // [cap] first body
+    int* tb;          // [cap] second body
+    int* tcand;       // [cap] candidate index, where its manifold is
+    float4* head;     // [cap] per candidate: normal, count
+    float* axis;      // [cap] per candidate: the winning axis
+    float4* pa;       // [cap * 4] per candidate point: anchor on first, depth
+    float4* pb;       // [cap * 4] per candidate point: anchor on second
+    float4* imp;      // [cap * 4] per touching point: normal impulse, tangential impulse
+    float4* impr;     // [cap * 4] per touching point: rolling impulse
+};
+
+struct Counters {  // device-side counts of a step
+    int candidates;     // candidate pairs listed
+    int touching;       // touching pairs
+    int points;         // their points
+    int rounds;         // rounds used
+    int unplaced;       // touching pairs with no round
+    int unlisted;       // partners found beyond the 32 slots
+    int status;         // ST_*
+    int colour_waves;   // dependency waves the colouring took
+    int abort;
+    unsigned int bar_count, bar_gen;
+    int remaining[3];
+    int pad[3];
+};
+
+struct Totals {  // accumulated over the steps of one vxr_box_step call
+    int last[5];
+    int most_rounds;
+    long long unplaced, unlisted;
+    int status;
+    int steps;
+};
+
+}  // namespace vxr
+
+using namespace vxr;
+
+struct vxr_box_world {
+    int n = 0, substeps = 1, sweeps = 1, symmetric = 0;
+    int nx = 1, ny = 1, nz = 1, has_grid = 0, reach_cells = 1;
+    float cell = 1.0f;
+    int cap = 0;  // candidate / touching capacity
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    Params params{};
+    std::string error;
+    int sms = 148;
+    int solve_blocks = 0, colour_blocks = 0;
+    float last_ms = 0.0f;
+
+    Bodies b{};
+    float4* wall = nullptr;              // [n * 48] wall records: normal impulse, tangential impulse
+    float4* wroll = nullptr;             // [n * 6] sphere rolling impulse against each wall
+    unsigned long long* wmask = nullptr;  // [n] bit k: wall record k nonzero; bit 48 + w: roll record w nonzero
+    float* shown = nullptr;              // [n * 20]
+
+    int cells = 1;
+    int *keys = nullptr, *cell_count = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
+    int *order_tmp = nullptr, *order = nullptr;
+    float4* reach = nullptr;  // world half-extents of each body (BoxBroad.reach)
+    int *partner = nullptr, *found = nullptr, *kept = nullptr, *cand_start = nullptr;
+    int *cand_a = nullptr, *cand_b = nullptr;
+    int *tcount = nullptr;
+    int *scan_tiles = nullptr;
+    PairBuffers gen[2]{};
+    int cur = 0;  // gen[cur] is this step's, gen[cur ^ 1] the step before's
+    int *colour = nullptr, *inc_count = nullptr, *inc_start = nullptr, *inc_fill = nullptr, *inc_list = nullptr;
+    int *round_count = nullptr, *round_start = nullptr, *round_fill = nullptr, *round_list = nullptr;
+    Counters* counters = nullptr;
+    Totals* totals = nullptr;
+    Totals* host_totals = nullptr;  // pinned
+    float* pinned = nullptr;        // pinned staging for state transfers
+    size_t pinned_bytes = 0;
+    std::vector<void*> allocations;
+};
+
+namespace {
+
+#define VXR_CUDA(call)                                                                                 \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            fail(w, std::string(#call) + ": " + cudaGetErrorString(e_));                               \
+            return VXR_ECUDA;                                                                          \
+        }                                                                                              \
+    } while (0)
+
+int fail(vxr_box_world* w, const std::string& why) {
+    if (w) w->error = why;
+    return VXR_ECUDA;
+}
+
+template <typename T>
+int alloc(vxr_box_world* w, T** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        w->error = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return VXR_ECUDA;
+    }
+    w->allocations.push_back(q);
+    *p = (T*)q;
+    return VXR_OK;
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// Broad phase kernels (BoxBroad.java).
+
+struct GridDims {
+    int nx, ny, nz;
+    float cell;
+    int reach;  // neighbourhood half-width in cells
+};
+
+// bin :74-89, and reach :196-227 for the list.
+__global__ void k_bin(int n, GridDims g, const float4* __restrict__ pose, const float4* __restrict__ turn,
+                      const float4* __restrict__ half, int* __restrict__ keys, float4* __restrict__ reach,
+                      int* __restrict__ cell_count) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 p = pose[s];
+    const float at[3] = {p.x, p.y, p.z};
+    const int cells[3] = {g.nx, g.ny, g.nz};
+    int c[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) c[a] = (int)fmaxf(0.0f, fminf((float)(cells[a] - 1), floorf(at[a] / g.cell)));
+    const int key = c[0] + cells[0] * (c[1] + cells[1] * c[2]);
+    keys[s] = key;
+    atomicAdd(&cell_count[key], 1);
+    const float4 q = turn[s];
+    const float4 h = half[s];
+    const float x = q.x, y = q.y, z = q.z, w = q.w;
+    const float r[3][3] = {{1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y - z * w), 2.0f * (x * z + y * w)},
+                           {2.0f * (x * y + z * w), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z - x * w)},
+                           {2.0f * (x * z - y * w), 2.0f * (y * z + x * w), 1.0f - 2.0f * (x * x + y * y)}};
+    float out[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) out[a] = (h.x * fabsf(r[a][0]) + h.y * fabsf(r[a][1])) + h.z * fabsf(r[a][2]);
+    if (h.w > 0.5f) out[0] = out[1] = out[2] = h.x;
+    reach[s] = make_float4(out[0], out[1], out[2], 0.0f);
+}
+
+__global__ void k_scatter(int n, const int* __restrict__ keys, const int* __restrict__ cell_start,
+                          int* __restrict__ cell_fill, int* __restrict__ order_tmp) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int key = keys[s];
+    order_tmp[cell_start[key] + atomicAdd(&cell_fill[key], 1)] = s;
+}
+
+// The counting sort made stable: each body's place in its cell is the number of its cell's bodies with a
+// lower index, whatever order the atomic scatter left.
+__global__ void k_stable(int n, const int* __restrict__ keys, const int* __restrict__ cell_start,
+                         const int* __restrict__ order_tmp, int* __restrict__ order) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int key = keys[s];
+    const int start = cell_start[key], end = cell_start[key + 1];
+    int rank = 0;
+    for (int j = start; j < end; j++) rank += order_tmp[j] < s;
+    order[start + rank] = s;
+}
+
+// list :103-164 with around :230-252: the higher-numbered bodies near s, the first 32 found kept in ascending
+// order, and how many were found. With reach > 1 (cells narrower than the reference's rule) the neighbourhood
+// widens to (2 reach + 1)^3 cells; at reach 1 it is the reference's 27, visited in its order.
+__global__ void k_list(int n, GridDims g, float margin, const float4* __restrict__ pose,
+                       const float4* __restrict__ reach, const int* __restrict__ keys,
+                       const int* __restrict__ cell_start, const int* __restrict__ order, int* __restrict__ partner,
+                       int* __restrict__ found_out, int* __restrict__ kept_out, Counters* counters) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 ps = pose[s];
+    const float4 rs = reach[s];
+    const float centre[3] = {ps.x, ps.y, ps.z};
+    const float rch[3] = {rs.x, rs.y, rs.z};
+    int slot[SLOTS];
+    int found = 0;
+    const int key = keys[s];
+    const int ix = key % g.nx, iy = (key / g.nx) % g.ny, iz = key / (g.nx * g.ny);
+    const int side = 2 * g.reach + 1;
+    const int around = side * side * side;
+    for (int nn = 0; nn < around; nn++) {
+        const int jx = ix + (nn % side - g.reach);
+        const int jy = iy + ((nn / side) % side - g.reach);
+        const int jz = iz + (nn / (side * side) - g.reach);
+        if (!(jx >= 0 && jx < g.nx && jy >= 0 && jy < g.ny && jz >= 0 && jz < g.nz)) continue;
+        const int cell = jx + g.nx * (jy + g.ny * jz);
+        const int end = cell_start[cell + 1];
+        for (int k = cell_start[cell]; k < end; k++) {
+            const int o = order[k];
+            if (!(o > s)) continue;
+            const float4 po = pose[o];
+            const float4 ro = reach[o];
+            const bool close = !(fabsf(po.x - centre[0]) > (rch[0] + ro.x) + margin) &&
+                               !(fabsf(po.y - centre[1]) > (rch[1] + ro.y) + margin) &&
+                               !(fabsf(po.z - centre[2]) > (rch[2] + ro.z) + margin);
+            if (!close) continue;
+            if (found < SLOTS) {
+                int place = found;
+                while (place > 0) {
+                    const int before = slot[place - 1];
+                    if (before > o) {
+                        slot[place] = before;
+                        place--;
+                    } else {
+                        break;
+                    }
+                }
+                slot[place] = o;
+            }
+            found++;
+        }
+    }
+    const int kept = found < SLOTS ? found : SLOTS;
+    for (int m = 0; m < kept; m++) partner[(long)s * SLOTS + m] = slot[m];
+    found_out[s] = found;
+    kept_out[s] = kept;
+    if (found > SLOTS) atomicAdd(&counters->unlisted, found - SLOTS);
+}
+
+__global__ void k_candidates(int n, int cap, const int* __restrict__ kept, const int* __restrict__ cand_start,
+                             const int* __restrict__ partner, int* __restrict__ cand_a, int* __restrict__ cand_b,
+                             Counters* counters) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0) {
+        const int total = cand_start[n];
+        counters->candidates = total;
+        if (total > cap) atomicCAS(&counters->status, ST_OK, ST_CAPACITY);
+    }
+    if (s >= n) return;
+    const int base = cand_start[s];
+    const int k = kept[s];
+    for (int m = 0; m < k; m++) {
+        if (base + m < cap) {
+            cand_a[base + m] = s;
+            cand_b[base + m] = partner[(long)s * SLOTS + m];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// Narrow phase: one thread per candidate pair (BoxContact.collide).
+__global__ void __launch_bounds__(128) k_collide(const int* __restrict__ cand_start_n, int cap, float margin,
+                                                 const int* __restrict__ cand_a, const int* __restrict__ cand_b,
+                                                 const float4* __restrict__ pose, const float4* __restrict__ turn,
+                                                 const float4* __restrict__ half, float4* __restrict__ head,
+                                                 float* __restrict__ axis, float4* __restrict__ pa,
+                                                 float4* __restrict__ pb) {
+    const int total = min(*cand_start_n, cap);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
+        const int a = cand_a[c], b = cand_b[c];
+        Manifold m;
+        collide_pair(pose[a], turn[a], half[a], pose[b], turn[b], half[b], margin, m);
+        head[c] = make_float4(m.normal[0], m.normal[1], m.normal[2], (float)m.count);
+        axis[c] = m.axis;
+        for (int i = 0; i < m.count; i++) {
+            pa[(long)c * MOST_POINTS + i] = make_float4(m.a[i][0], m.a[i][1], m.a[i][2], m.depth[i]);
+            pb[(long)c * MOST_POINTS + i] = make_float4(m.b[i][0], m.b[i][1], m.b[i][2], 0.0f);
+        }
+    }
+}
+
+// Per body: how many of its candidates touch.
+__global__ void k_touch_count(int n, int cap, const int* __restrict__ cand_start, const float4* __restrict__ head,
+                              int* __restrict__ tcount) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int k = 0;
+    const int end = min(cand_start[s + 1], cap);
+    for (int c = cand_start[s]; c < end; c++) k += head[c].w > 0.0f;
+    tcount[s] = k;
+}
+
+// The touching list in slot order (BoxBroad.counts :174-188 and the order BoxStepper reads it in).
+__global__ void k_touch_list(int n, int cap, const int* __restrict__ cand_start, const int* __restrict__ cand_b,
+                             const float4* __restrict__ head, const int* __restrict__ tstart, int* __restrict__ ta,
+                             int* __restrict__ tb, int* __restrict__ tcand, Counters* counters) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0) counters->touching = tstart[n];
+    if (s >= n) return;
+    int t = tstart[s];
+    int points = 0;
+    const int end = min(cand_start[s + 1], cap);
+    for (int c = cand_start[s]; c < end; c++) {
+        const float cnt = head[c].w;
+        if (cnt > 0.0f) {
+            ta[t] = s;
+            tb[t] = cand_b[c];
+            tcand[t] = c;
+            points += (int)cnt;
+            t++;
+        }
+    }
+    if (points) atomicAdd(&counters->points, points);
+}
+
+// BoxPairs.carry :191-267: each new point takes the impulses of the nearest point of the same pair the step
+// before (anchor on the first body within 5% of its smallest half-extent), one point to one point always.
+__global__ void k_carry(const int* __restrict__ touching_n, PairBuffers now, PairBuffers was,
+                        const float4* __restrict__ half) {
+    const int total = *touching_n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int s = now.ta[t], partner = now.tb[t];
+        const int c = now.tcand[t];
+        const int count = (int)now.head[c].w;
+        int old = -1;
+        for (int u = was.tstart[s]; u < was.tstart[s + 1]; u++)
+            if (was.tb[u] == partner) old = u;
+        int before = 0;
+        int oc = 0;
+        if (old >= 0) {
+            oc = was.tcand[old];
+            before = (int)was.head[oc].w;
+        }
+        const float4 h = half[s];
+        const float smallest = fminf(h.x, fminf(h.y, h.z));
+        const float reach = (0.05f * smallest) * (0.05f * smallest);
+        for (int point = 0; point < MOST_POINTS; point++) {
+            float4 t0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), t1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (point < count) {
+                const float4 anchor = now.pa[(long)c * MOST_POINTS + point];
+                float nearest = reach;
+                for (int o = 0; o < MOST_POINTS; o++) {
+                    if (!(o < before)) continue;
+                    const float4 then = was.pa[(long)oc * MOST_POINTS + o];
+                    const float gap[3] = {anchor.x - then.x, anchor.y - then.y, anchor.z - then.z};
+                    const float d2 = dot3(gap, gap);
+                    if (d2 < nearest) {
+                        nearest = d2;
+                        t0 = was.imp[(long)old * MOST_POINTS + o];
+                        t1 = was.impr[(long)old * MOST_POINTS + o];
+                    }
+                }
+            }
+            if (point == 0 && count == 1 && before == 1) {
+                t0 = was.imp[(long)old * MOST_POINTS];
+                t1 = was.impr[(long)old * MOST_POINTS];
+            }
+            now.imp[(long)t * MOST_POINTS + point] = t0;
+            now.impr[(long)t * MOST_POINTS + point] = t1;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// Colouring (BoxStepper.java:339-358), reproduced exactly on the device.
+//
+// The host's greedy pass puts each touching pair, in slot order, into the first of 32 rounds holding neither of
+// its bodies. So a pair's round is the least round not used by the lower-numbered touching pairs that share a
+// body with it (unplaced pairs use none); it depends on those pairs alone. Waves of the cooperative kernel below
+// give every pair whose lower-numbered neighbours all have rounds its round, until none is left.
+
+__global__ void k_inc_count(const int* __restrict__ touching_n, const int* __restrict__ ta,
+                            const int* __restrict__ tb, int* __restrict__ inc_count) {
+    const int total = *touching_n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        atomicAdd(&inc_count[ta[t]], 1);
+        atomicAdd(&inc_count[tb[t]], 1);
+    }
+}
+
+__global__ void k_inc_fill(const int* __restrict__ touching_n, const int* __restrict__ ta,
+                           const int* __restrict__ tb, const int* __restrict__ inc_start, int* __restrict__ inc_fill,
+                           int* __restrict__ inc_list) {
+    const int total = *touching_n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int a = ta[t], b = tb[t];
+        inc_list[inc_start[a] + atomicAdd(&inc_fill[a], 1)] = t;
+        inc_list[inc_start[b] + atomicAdd(&inc_fill[b], 1)] = t;
+    }
+}
+
+__device__ __forceinline__ bool lower_rounds(int t, int body, const int* inc_start, const int* inc_list,
+                                             const int* colour, unsigned int& used) {
+    for (int k = inc_start[body]; k < inc_start[body + 1]; k++) {
+        const int u = inc_list[k];
+        if (u < t) {
+            const int cu = *(volatile const int*)&colour[u];
+            if (cu < 0) return false;
+            if (cu < MOST_ROUNDS) used |= 1u << cu;
+        }
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(THREADS) k_colour(const int* __restrict__ touching_n, const int* __restrict__ ta,
+                                                    const int* __restrict__ tb, const int* __restrict__ inc_start,
+                                                    const int* __restrict__ inc_list, int* colour,
+                                                    Counters* counters, GridBarrier bar) {
+    const int total = *touching_n;
+    const int threads = gridDim.x * blockDim.x;
+    const int me = blockIdx.x * blockDim.x + threadIdx.x;
+    // Each thread takes a contiguous run of pairs, so a body's consecutive pairs resolve in one wave.
+    const int per = (total + threads - 1) / threads;
+    const int lo = me * per, hi = min(total, lo + per);
+    __shared__ int left_block;
+    for (int wave = 0;; wave++) {
+        if (threadIdx.x == 0) left_block = 0;
+        __syncthreads();
+        int left = 0;
+        for (int t = lo; t < hi; t++) {
+            if (colour[t] >= 0) continue;
+            unsigned int used = 0u;
+            if (lower_rounds(t, ta[t], inc_start, inc_list, colour, used) &&
+                lower_rounds(t, tb[t], inc_start, inc_list, colour, used)) {
+                const int r = used == 0xffffffffu ? MOST_ROUNDS : __ffs(~used) - 1;
+                *(volatile int*)&colour[t] = r;
+            } else {
+                left++;
+            }
+        }
+        if (left) atomicAdd(&left_block, left);
+        __syncthreads();
+        if (threadIdx.x == 0 && left_block) atomicAdd(&counters->remaining[wave % 3], left_block);
+        if (!grid_sync(bar)) return;
+        const int remaining = *(volatile int*)&counters->remaining[wave % 3];
+        if (blockIdx.x == 0 && threadIdx.x == 0) counters->remaining[(wave + 2) % 3] = 0;
+        if (remaining == 0) {
+            if (me == 0) counters->colour_waves = wave + 1;
+            return;
+        }
+        if (wave > total + 1) {
+            if (me == 0) atomicCAS(&counters->status, ST_OK, ST_ROUNDS);
+            return;
+        }
+    }
+}
+
+__global__ void k_round_count(const int* __restrict__ touching_n, const int* __restrict__ colour,
+                              int* __restrict__ round_count, Counters* counters) {
+    const int total = *touching_n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int c = colour[t];
+        if (c < MOST_ROUNDS) {
+            atomicAdd(&round_count[c], 1);
+            atomicMax(&counters->rounds, c + 1);
+        } else {
+            atomicAdd(&counters->unplaced, 1);
+        }
+    }
+}
+
+__global__ void k_round_fill(const int* __restrict__ touching_n, const int* __restrict__ colour,
+                             const int* __restrict__ round_start, int* __restrict__ round_fill,
+                             int* __restrict__ round_list) {
+    const int total = *touching_n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int c = colour[t];
+        if (c < MOST_ROUNDS) round_list[round_start[c] + atomicAdd(&round_fill[c], 1)] = t;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// The substeps: one cooperative kernel, a grid barrier between phases.
+
+struct SolveArgs {
+    int n;
+    Bodies b;
+    float4* wall;
+    float4* wroll;
+    unsigned long long* wmask;
+    PairBuffers pairs;
+    const int* round_start;
+    const int* round_list;
+    Counters* counters;
+    int substeps, sweeps, symmetric;
+    Params params;
+    GridBarrier bar;
+};
+
+__device__ __forceinline__ void load_held(Held& h, const Bodies& b, int s) {
+    h.load(b.pose[s], b.turn[s], b.half[s], b.vel[s], b.mom[s]);
+}
+__device__ __forceinline__ void store_held(const Held& h, const Bodies& b, int s) {
+    b.vel[s] = make_float4(h.velocity[0], h.velocity[1], h.velocity[2], 0.0f);
+    b.mom[s] = make_float4(h.momentum[0], h.momentum[1], h.momentum[2], 0.0f);
+}
+
+// Boxes.velocities :276-289.
+__device__ void phase_velocities(const SolveArgs& A) {
+    const int stride = gridDim.x * blockDim.x;
+    const float h = A.params.w[P_H];
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += stride) {
+        if (!(A.b.pose[s].w > 0.0f)) continue;
+        float4 v = A.b.vel[s];
+        v.x = v.x + h * A.params.w[P_GX];
+        v.y = v.y + h * A.params.w[P_GY];
+        v.z = v.z + h * A.params.w[P_GZ];
+        A.b.vel[s] = v;
+    }
+}
+
+// Boxes.positions :299-342.
+__device__ void phase_positions(const SolveArgs& A) {
+    const int stride = gridDim.x * blockDim.x;
+    const float h = A.params.w[P_H];
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += stride) {
+        float4 p = A.b.pose[s];
+        const float im = p.w;
+        if (!(im > 0.0f)) continue;
+        const float4 v = A.b.vel[s];
+        p.x = p.x + h * v.x;
+        p.y = p.y + h * v.y;
+        p.z = p.z + h * v.z;
+        A.b.pose[s] = p;
+        const float4 tq = A.b.turn[s];
+        const float q[4] = {tq.x, tq.y, tq.z, tq.w};
+        const float4 l = A.b.mom[s];
+        const float momentum[3] = {l.x, l.y, l.z};
+        float inverse[3];
+        inverse_inertia(A.b.half[s], im, inverse);
+        float omega[3], mid[4], omega_mid[3], end[4];
+        {
+            const float c[4] = {-q[0], -q[1], -q[2], q[3]};
+            float own[3], scaled[3];
+            rotateq(c, momentum, own);
+            for (int a = 0; a < 3; a++) scaled[a] = inverse[a] * own[a];
+            rotateq(q, scaled, omega);
+        }
+        const float half_h = 0.5f * h;
+        turned(q, omega, half_h, mid);
+        {
+            const float c[4] = {-mid[0], -mid[1], -mid[2], mid[3]};
+            float own[3], scaled[3];
+            rotateq(c, momentum, own);
+            for (int a = 0; a < 3; a++) scaled[a] = inverse[a] * own[a];
+            rotateq(mid, scaled, omega_mid);
+        }
+        turned(q, omega_mid, h, end);
+        A.b.turn[s] = make_float4(end[0], end[1], end[2], end[3]);
+    }
+}
+
+// Boxes.walls :357-416: each body's corners (a sphere: its nearest point) against the six walls.
+__device__ void phase_walls(const SolveArgs& A, int sweep, bool reverse) {
+    const int stride = gridDim.x * blockDim.x;
+    const Params& P = A.params;
+    const float margin = P.w[P_MARGIN];
+    const float extent[3] = {P.w[P_SX], P.w[P_SY], P.w[P_SZ]};
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += stride) {
+        const float4 pose = A.b.pose[s];
+        if (!(pose.w > 0.0f)) continue;
+        unsigned long long mask = A.wmask[s];
+        const float4 hw = A.b.half[s];
+        const bool sphere = hw.w > 0.5f;
+        if (mask == 0ull) {
+            if (sweep == WARM) continue;  // nothing held: the warm start applies nothing
+            // Far from every wall with nothing held: every contact's gap exceeds the margin (a bound that holds
+            // through f32 rounding), so no record is read or written.
+            const float r = sphere ? hw.x : sqrtf((hw.x * hw.x + hw.y * hw.y) + hw.z * hw.z);
+            const float bound = r * 1.01f + 1e-3f + margin;
+            if (pose.x - bound > 0.0f && (extent[0] - pose.x) - bound > 0.0f && pose.y - bound > 0.0f &&
+                (extent[1] - pose.y) - bound > 0.0f && pose.z - bound > 0.0f && (extent[2] - pose.z) - bound > 0.0f)
+                continue;
+        }
+        Held box;
+        load_held(box, A.b, s);
+        const Soft soft(P, true);
+        bool touched = false;
+        for (int order = 0; order < 6; order++) {
+            const int wall = reverse ? 5 - order : order;
+            const int axis = wall / 2;
+            const bool high = wall % 2 == 1;
+            float n[3];
+            for (int a = 0; a < 3; a++) n[a] = a == axis ? (high ? -1.0f : 1.0f) : 0.0f;
+            if (sphere) {
+                float r[3];
+                for (int a = 0; a < 3; a++) r[a] = -(box.half[0] * n[a]);
+                const float reach = box.at[axis] + r[axis];
+                const float gap = high ? extent[axis] - reach : reach;
+                const int bit = wall * 8, rbit = 48 + wall;
+                const bool held = (mask >> bit) & 1ull, rolled = (mask >> rbit) & 1ull;
+                const bool need = held || (sweep != WARM && gap < margin);
+                float4 rec = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                const long at = (long)s * WALL_RECORDS + wall * 8;
+                if (need) {
+                    rec = held ? A.wall[at] : rec;
+                    contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft);
+                    if (sweep != WARM) {
+                        A.wall[at] = rec;
+                        mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
+                    }
+                    touched = true;
+                }
+                if (rolled || (sweep != WARM && nonzero_bits(rec))) {
+                    float4 rr = rolled ? A.wroll[(long)s * 6 + wall] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    roll<false>(sweep, box, box, box.half[0], rec.x, rr, P.w[P_MU_ROLLING]);
+                    if (sweep != WARM) {
+                        A.wroll[(long)s * 6 + wall] = rr;
+                        mask = nonzero_bits(rr) ? (mask | (1ull << rbit)) : (mask & ~(1ull << rbit));
+                    }
+                    touched = true;
+                }
+            } else {
+                for (int k = 0; k < 8; k++) {
+                    const int c = reverse ? 7 - k : k;
+                    float offset[3], r[3];
+                    for (int a = 0; a < 3; a++) {
+                        const int bit = (c >> a) & 1;
+                        offset[a] = box.half[a] * (2.0f * (float)bit - 1.0f);
+                    }
+                    rotateq(box.q, offset, r);
+                    const float reach = box.at[axis] + r[axis];
+                    const float gap = high ? extent[axis] - reach : reach;
+                    const int bit = wall * 8 + c;
+                    const bool held = (mask >> bit) & 1ull;
+                    if (!(held || (sweep != WARM && gap < margin))) continue;
+                    const long at = (long)s * WALL_RECORDS + bit;
+                    float4 rec = held ? A.wall[at] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft);
+                    if (sweep != WARM) {
+                        A.wall[at] = rec;
+                        mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
+                    }
+                    touched = true;
+                }
+            }
+        }
+        if (touched) {
+            store_held(box, A.b, s);
+            A.wmask[s] = mask;
+        }
+    }
+}
+
+// BoxPairs.solve :64-151: one round of pairs that share no body.
+__device__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r) {
+    const int stride = gridDim.x * blockDim.x;
+    const Params& P = A.params;
+    const int lo = A.round_start[r], hi = A.round_start[r + 1];
+    for (int k = lo + blockIdx.x * blockDim.x + threadIdx.x; k < hi; k += stride) {
+        const int t = A.round_list[k];
+        const int c = A.pairs.tcand[t];
+        const float4 head = A.pairs.head[c];
+        const int count = (int)head.w;
+        const int ia = A.pairs.ta[t], ib = A.pairs.tb[t];
+        Held first, second;
+        load_held(first, A.b, ia);
+        load_held(second, A.b, ib);
+        Soft soft(P, false);
+        if (first.im == 0.0f || second.im == 0.0f) {
+            soft.bias = P.w[P_STATIC_BIAS];
+            soft.mass_scale = P.w[P_STATIC_MASS_SCALE];
+            soft.impulse_scale = P.w[P_STATIC_IMPULSE_SCALE];
+        }
+        const float n[3] = {head.x, head.y, head.z};
+        const bool anySphere = first.sphere() || second.sphere();
+        for (int order = 0; order < MOST_POINTS; order++) {
+            const int slot = reverse ? MOST_POINTS - 1 - order : order;
+            if (!(slot < count)) continue;
+            const float4 qa = A.pairs.pa[(long)c * MOST_POINTS + slot];
+            const float4 qb = A.pairs.pb[(long)c * MOST_POINTS + slot];
+            const float anchorA[3] = {qa.x, qa.y, qa.z}, anchorB[3] = {qb.x, qb.y, qb.z};
+            float rA[3], rB[3];
+            rotateq(first.q, anchorA, rA);
+            rotateq(second.q, anchorB, rB);
+            if (first.sphere())
+                for (int a = 0; a < 3; a++) rA[a] = first.half[0] * n[a];
+            if (second.sphere())
+                for (int a = 0; a < 3; a++) rB[a] = -(second.half[0] * n[a]);
+            float gap = ((second.at[0] + rB[0]) - (first.at[0] + rA[0])) * n[0] +
+                        ((second.at[1] + rB[1]) - (first.at[1] + rA[1])) * n[1];
+            gap = gap + ((second.at[2] + rB[2]) - (first.at[2] + rA[2])) * n[2];
+            const long at = (long)t * MOST_POINTS + slot;
+            float4 rec = A.pairs.imp[at];
+            contact<true>(sweep, gap, n, first, rA, second, rB, rec, soft);
+            if (sweep != WARM) A.pairs.imp[at] = rec;
+            if (anySphere) {
+                float radius = second.half[0];
+                if (first.sphere()) radius = first.half[0];
+                if (first.sphere() && second.sphere())
+                    radius = (first.half[0] * second.half[0]) / (first.half[0] + second.half[0]);
+                float4 rr = A.pairs.impr[at];
+                roll<true>(sweep, first, second, radius, rec.x, rr, P.w[P_MU_ROLLING]);
+                if (sweep != WARM) A.pairs.impr[at] = rr;
+            }
+        }
+        store_held(first, A.b, ia);
+        store_held(second, A.b, ib);
+    }
+}
+
+__device__ bool sweep_all(const SolveArgs& A, int kind, bool reverse, int rounds) {
+    if (reverse) {
+        phase_walls(A, kind, true);
+        if (!grid_sync(A.bar)) return false;
+    }
+    for (int order = 0; order < rounds; order++) {
+        const int r = reverse ? rounds - 1 - order : order;
+        phase_round(A, kind, reverse, r);
+        if (!grid_sync(A.bar)) return false;
+    }
+    if (!reverse) {
+        phase_walls(A, kind, false);
+        if (!grid_sync(A.bar)) return false;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(SOLVE_THREADS) k_solve(SolveArgs A) {
+    const int rounds = *(volatile int*)&A.counters->rounds;
+    for (int sub = 0; sub < A.substeps; sub++) {
+        phase_velocities(A);
+        if (!grid_sync(A.bar)) return;
+        if (!sweep_all(A, WARM, false, rounds)) return;
+        for (int sw = 0; sw < A.sweeps; sw++)
+            if (!sweep_all(A, SOLVE, A.symmetric && sw % 2 == 1, rounds)) return;
+        phase_positions(A);
+        if (!grid_sync(A.bar)) return;
+        for (int sw = 0; sw < A.sweeps; sw++)
+            if (!sweep_all(A, RELAX, A.symmetric && sw % 2 == 1, rounds)) return;
+    }
+}
+
+// Boxes.show :801-820.
+__global__ void k_show(int n, const Bodies b, float* __restrict__ shown) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    float* sh = shown + (long)s * SHOWN_STRIDE;
+    const float4 p = b.pose[s], q = b.turn[s], h = b.half[s];
+    sh[0] = sh[4];
+    sh[1] = sh[5];
+    sh[2] = sh[6];
+    sh[4] = p.x;
+    sh[5] = p.y;
+    sh[6] = p.z;
+    sh[8] = h.x;
+    sh[9] = h.y;
+    sh[10] = h.z;
+    sh[12] = sh[16];
+    sh[13] = sh[17];
+    sh[14] = sh[18];
+    sh[15] = sh[19];
+    sh[16] = q.x;
+    sh[17] = q.y;
+    sh[18] = q.z;
+    sh[19] = q.w;
+    sh[3] = h.w;
+}
+
+__global__ void k_totals(const Counters* c, Totals* t) {
+    t->last[0] = c->touching;
+    t->last[1] = c->points;
+    t->last[2] = c->rounds;
+    t->last[3] = c->unplaced;
+    t->last[4] = c->unlisted;
+    t->most_rounds = max(t->most_rounds, c->rounds);
+    t->unplaced += c->unplaced;
+    t->unlisted += c->unlisted;
+    if (t->status == ST_OK) t->status = c->status;
+    t->steps += 1;
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// Host orchestration.
+
+int blocks_for(long n, int threads) { return (int)std::max<long>(1, (n + threads - 1) / threads); }
+
+int launch_cooperative(vxr_box_world* w, const void* fn, int blocks, int threads, void** args) {
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, 0, w->stream);
+    if (e != cudaSuccess) return fail(w, std::string("cooperative launch: ") + cudaGetErrorString(e));
+    return VXR_OK;
+}
+
+GridBarrier barrier_of(vxr_box_world* w) {
+    GridBarrier g;
+    g.count = &w->counters->bar_count;
+    g.generation = &w->counters->bar_gen;
+    g.abort = &w->counters->abort;
+    g.status = &w->counters->status;
+    g.limit_ns = 2000000000ull;  // 2 s: far above any barrier's honest wait
+    return g;
+}
+
+// One whole step, enqueued on the world's stream.
+int enqueue_step(vxr_box_world* w) {
+    cudaStream_t st = w->stream;
+    const int n = w->n;
+    VXR_CUDA(cudaMemsetAsync(w->counters, 0, sizeof(Counters), st));
+    PairBuffers& now = w->gen[w->cur];
+    PairBuffers& was = w->gen[w->cur ^ 1];
+    if (w->has_grid) {
+        GridDims g{w->nx, w->ny, w->nz, w->cell, w->reach_cells};
+        const float margin = w->params.w[P_MARGIN];
+        VXR_CUDA(cudaMemsetAsync(w->cell_count, 0, sizeof(int) * w->cells, st));
+        VXR_CUDA(cudaMemsetAsync(w->cell_fill, 0, sizeof(int) * w->cells, st));
+        k_bin<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, g, w->b.pose, w->b.turn, w->b.half, w->keys, w->reach,
+                                                         w->cell_count);
+        exclusive_scan(w->cell_count, w->cell_start, w->cells, w->scan_tiles, st);
+        k_scatter<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->keys, w->cell_start, w->cell_fill,
+                                                             w->order_tmp);
+        k_stable<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->keys, w->cell_start, w->order_tmp, w->order);
+        k_list<<<blocks_for(n, 128), 128, 0, st>>>(n, g, margin, w->b.pose, w->reach, w->keys, w->cell_start,
+                                                  w->order, w->partner, w->found, w->kept, w->counters);
+        exclusive_scan(w->kept, w->cand_start, n, w->scan_tiles, st);
+        k_candidates<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->kept, w->cand_start, w->partner,
+                                                                w->cand_a, w->cand_b, w->counters);
+        const int cblocks = w->sms * 8;
+        k_collide<<<cblocks, 128, 0, st>>>(w->cand_start + n, w->cap, margin, w->cand_a, w->cand_b, w->b.pose,
+                                            w->b.turn, w->b.half, now.head, now.axis, now.pa, now.pb);
+        k_touch_count<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->cand_start, now.head, w->tcount);
+        exclusive_scan(w->tcount, now.tstart, n, w->scan_tiles, st);
+        k_touch_list<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->cand_start, w->cand_b, now.head,
+                                                                now.tstart, now.ta, now.tb, now.tcand, w->counters);
+        const int tblocks = w->sms * 4;
+        k_carry<<<tblocks, THREADS, 0, st>>>(now.tstart + n, now, was, w->b.half);
+        // colouring
+        VXR_CUDA(cudaMemsetAsync(w->inc_count, 0, sizeof(int) * n, st));
+        VXR_CUDA(cudaMemsetAsync(w->inc_fill, 0, sizeof(int) * n, st));
+        VXR_CUDA(cudaMemsetAsync(w->colour, 0xff, sizeof(int) * w->cap, st));
+        k_inc_count<<<tblocks, THREADS, 0, st>>>(now.tstart + n, now.ta, now.tb, w->inc_count);
+        exclusive_scan(w->inc_count, w->inc_start, n, w->scan_tiles, st);
+        k_inc_fill<<<tblocks, THREADS, 0, st>>>(now.tstart + n, now.ta, now.tb, w->inc_start, w->inc_fill,
+                                               w->inc_list);
+        {
+            const int* tn = now.tstart + n;
+            GridBarrier bar = barrier_of(w);
+            void* args[] = {(void*)&tn, (void*)&now.ta, (void*)&now.tb, (void*)&w->inc_start, (void*)&w->inc_list,
+                            (void*)&w->colour, (void*)&w->counters, (void*)&bar};
+            int rc = launch_cooperative(w, (const void*)k_colour, w->colour_blocks, THREADS, args);
+            if (rc) return rc;
+        }
+        VXR_CUDA(cudaMemsetAsync(w->round_count, 0, sizeof(int) * (MOST_ROUNDS + 1), st));
+        VXR_CUDA(cudaMemsetAsync(w->round_fill, 0, sizeof(int) * (MOST_ROUNDS + 1), st));
+        k_round_count<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_count, w->counters);
+        exclusive_scan(w->round_count, w->round_start, MOST_ROUNDS, w->scan_tiles, st);
+        k_round_fill<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_start, w->round_fill,
+                                                 w->round_list);
+    }
+    {
+        SolveArgs A;
+        A.n = n;
+        A.b = w->b;
+        A.wall = w->wall;
+        A.wroll = w->wroll;
+        A.wmask = w->wmask;
+        A.pairs = now;
+        A.round_start = w->round_start;
+        A.round_list = w->round_list;
+        A.counters = w->counters;
+        A.substeps = w->substeps;
+        A.sweeps = w->sweeps;
+        A.symmetric = w->symmetric;
+        A.params = w->params;
+        A.bar = barrier_of(w);
+        VXR_CUDA(cudaMemsetAsync(&w->counters->bar_count, 0, 2 * sizeof(unsigned int), st));
+        void* args[] = {(void*)&A};
+        int rc = launch_cooperative(w, (const void*)k_solve, w->solve_blocks, SOLVE_THREADS, args);
+        if (rc) return rc;
+    }
+    k_show<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->b, w->shown);
+    k_totals<<<1, 1, 0, st>>>(w->counters, w->totals);
+    VXR_CUDA(cudaGetLastError());
+    if (w->has_grid) w->cur ^= 1;
+    return VXR_OK;
+}
+
+// Every impulse, wall record and pair list back to zero, as the reference's runner.clear() leaves them.
+int clear_dynamic(vxr_box_world* w) {
+    cudaStream_t st = w->stream;
+    const int n = w->n;
+    VXR_CUDA(cudaMemsetAsync(w->wall, 0, sizeof(float4) * (size_t)n * WALL_RECORDS, st));
+    VXR_CUDA(cudaMemsetAsync(w->wroll, 0, sizeof(float4) * (size_t)n * 6, st));
+    VXR_CUDA(cudaMemsetAsync(w->wmask, 0, sizeof(unsigned long long) * n, st));
+    VXR_CUDA(cudaMemsetAsync(w->shown, 0, sizeof(float) * (size_t)n * SHOWN_STRIDE, st));
+    VXR_CUDA(cudaMemsetAsync(w->totals, 0, sizeof(Totals), st));
+    if (w->has_grid)
+        for (int g = 0; g < 2; g++) VXR_CUDA(cudaMemsetAsync(w->gen[g].tstart, 0, sizeof(int) * ((size_t)n + 1), st));
+    w->cur = 0;
+    return VXR_OK;
+}
+
+int ensure_pinned(vxr_box_world* w, size_t bytes) {
+    if (w->pinned_bytes >= bytes) return VXR_OK;
+    if (w->pinned) cudaFreeHost(w->pinned);
+    w->pinned = nullptr;
+    w->pinned_bytes = 0;
+    VXR_CUDA(cudaMallocHost(&w->pinned, bytes));
+    w->pinned_bytes = bytes;
+    return VXR_OK;
+}
+
+// float4 array <- four host arrays (any may be null: then `fill`)
+int upload4(vxr_box_world* w, float4* dst, const float* a, const float* b, const float* c, const float* d,
+            float fill_d) {
+    const int n = w->n;
+    int rc = ensure_pinned(w, sizeof(float4) * (size_t)n);
+    if (rc) return rc;
+    float* p = w->pinned;
+    for (int s = 0; s < n; s++) {
+        p[4 * s + 0] = a ? a[s] : 0.0f;
+        p[4 * s + 1] = b ? b[s] : 0.0f;
+        p[4 * s + 2] = c ? c[s] : 0.0f;
+        p[4 * s + 3] = d ? d[s] : fill_d;
+    }
+    VXR_CUDA(cudaMemcpyAsync(dst, p, sizeof(float4) * (size_t)n, cudaMemcpyHostToDevice, w->stream));
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    return VXR_OK;
+}
+
+int download4(vxr_box_world* w, const float4* src, float* a, float* b, float* c, float* d) {
+    const int n = w->n;
+    int rc = ensure_pinned(w, sizeof(float4) * (size_t)n);
+    if (rc) return rc;
+    VXR_CUDA(cudaMemcpyAsync(w->pinned, src, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost, w->stream));
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    const float* p = w->pinned;
+    for (int s = 0; s < n; s++) {
+        if (a) a[s] = p[4 * s + 0];
+        if (b) b[s] = p[4 * s + 1];
+        if (c) c[s] = p[4 * s + 2];
+        if (d) d[s] = p[4 * s + 3];
+    }
+    return VXR_OK;
+}
+
+// Boxes.params / softness (Boxes.java:212-251), computed in double and rounded to f32 bits.
+int32_t f32bits(double v) {
+    float f = (float)v;
+    int32_t i;
+    std::memcpy(&i, &f, 4);
+    return i;
+}
+void softness(double hertz, double zeta, double h, double* out) {
+    if (hertz == 0) {
+        out[0] = 0;
+        out[1] = 1;
+        out[2] = 0;
+        return;
+    }
+    const double omega = 2 * M_PI * hertz;
+    const double a1 = 2 * zeta + h * omega;
+    const double a2 = h * omega * a1;
+    const double a3 = 1 / (1 + a2);
+    out[0] = omega / a1;
+    out[1] = a2 * a3;
+    out[2] = a3;
+}
+
+// BoxDiagnostics.momentum in doubles (BoxDiagnostics.java:46-53): L = R I Rᵀ ω.
+void rotate_d(const double* q, const double* p, double* out) {
+    const double t0 = 2 * (q[1] * p[2] - q[2] * p[1]), t1 = 2 * (q[2] * p[0] - q[0] * p[2]),
+                 t2 = 2 * (q[0] * p[1] - q[1] * p[0]);
+    const double t[3] = {t0, t1, t2};
+    const double qt[3] = {q[1] * t[2] - q[2] * t[1], q[2] * t[0] - q[0] * t[2], q[0] * t[1] - q[1] * t[0]};
+    for (int a = 0; a < 3; a++) out[a] = p[a] + q[3] * t[a] + qt[a];
+}
+
+}  // namespace
+
+// ================================================================================================================
+// C-ABI
+extern "C" {
+
+const char* vxr_version(void) { return "vxr-b200 0.1 (sm_100a)"; }
+
+int32_t vxr_box_make_params(double h, double gx, double gy, double gz, double sx, double sy, double sz,
+                            double mu_static, double mu_kinetic, double margin, double mu_rolling, int32_t* out) {
+    if (!out) return VXR_EINVAL;
+    if (!(mu_rolling >= 0) || std::isinf(mu_rolling)) return VXR_EINVAL;
+    if (!(margin >= 0) || std::isinf(margin)) return VXR_EINVAL;
+    if (!(h > 0) || !(sx > 0) || !(sy > 0) || !(sz > 0)) return VXR_EINVAL;
+    if (!(mu_static >= 0) || !(mu_kinetic >= 0) || std::isinf(mu_static) || std::isinf(mu_kinetic)) return VXR_EINVAL;
+    const double hertz = std::min(150.0, 0.25 / h);
+    double soft[3], stiff[3];
+    softness(hertz, 10.0, h, soft);
+    softness(2 * hertz, 10.0, h, stiff);
+    const double v[18] = {h, gx, gy, gz, sx, sy, sz, mu_static, mu_kinetic, margin, soft[0], soft[1], soft[2],
+                          stiff[0], stiff[1], stiff[2], 3.0, mu_rolling};
+    for (int k = 0; k < 18; k++) out[k] = f32bits(v[k]);
+    return VXR_OK;
+}
+
+int32_t vxr_box_make_grid(double sx, double sy, double sz, double widest_half_diagonal, double margin,
+                          vxr_grid* out) {
+    if (!out) return VXR_EINVAL;
+    const double widest = 2 * widest_half_diagonal + margin;
+    if (!(widest > 0)) return VXR_EINVAL;
+    out->nx = std::max(1, (int)std::ceil(sx / widest));
+    out->ny = std::max(1, (int)std::ceil(sy / widest));
+    out->nz = std::max(1, (int)std::ceil(sz / widest));
+    out->cell = (float)widest;
+    return VXR_OK;
+}
+
+vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
+    auto set = [&](int32_t s) {
+        if (status) *status = s;
+    };
+    if (!cfg || cfg->bodies < 1 || cfg->substeps < 1 || cfg->sweeps < 1) {
+        set(VXR_EINVAL);
+        return nullptr;
+    }
+    vxr_box_world* w = new vxr_box_world();
+    w->n = cfg->bodies;
+    w->substeps = cfg->substeps;
+    w->sweeps = cfg->sweeps;
+    w->symmetric = cfg->symmetric ? 1 : 0;
+    w->device = cfg->device;
+    w->has_grid = (cfg->bodies > 1 && cfg->grid.nx > 0 && cfg->grid.ny > 0 && cfg->grid.nz > 0 && cfg->grid.cell > 0)
+                      ? 1 : 0;
+    if (w->has_grid) {
+        w->nx = cfg->grid.nx;
+        w->ny = cfg->grid.ny;
+        w->nz = cfg->grid.nz;
+        w->cell = cfg->grid.cell;
+        w->reach_cells = cfg->reach_cells > 0 ? cfg->reach_cells : 1;
+        long cells = (long)w->nx * w->ny * w->nz;
+        if (cells > (1L << 30)) {
+            set(VXR_EINVAL);
+            delete w;
+            return nullptr;
+        }
+        w->cells = (int)cells;
+    }
+    long cap = cfg->max_pairs > 0 ? cfg->max_pairs : (long)w->n * SLOTS;
+    if (cap > (1L << 30)) cap = 1L << 30;
+    w->cap = (int)cap;
+    auto bad = [&](int rc) {
+        set(rc);
+        vxr_box_destroy(w);
+        return (vxr_box_world*)nullptr;
+    };
+    if (cudaSetDevice(w->device) != cudaSuccess) return bad(VXR_ECUDA);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, w->device) != cudaSuccess) return bad(VXR_ECUDA);
+    w->sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(VXR_ECUDA);
+    cudaEventCreate(&w->ev0);
+    cudaEventCreate(&w->ev1);
+    const int n = w->n;
+    int rc = 0;
+    rc |= alloc(w, &w->b.pose, n);
+    rc |= alloc(w, &w->b.turn, n);
+    rc |= alloc(w, &w->b.half, n);
+    rc |= alloc(w, &w->b.vel, n);
+    rc |= alloc(w, &w->b.mom, n);
+    rc |= alloc(w, &w->wall, (size_t)n * WALL_RECORDS);
+    rc |= alloc(w, &w->wroll, (size_t)n * 6);
+    rc |= alloc(w, &w->wmask, n);
+    rc |= alloc(w, &w->shown, (size_t)n * SHOWN_STRIDE);
+    rc |= alloc(w, &w->counters, 1);
+    rc |= alloc(w, &w->totals, 1);
+    rc |= alloc(w, &w->scan_tiles, scan_tiles_for(std::max(n, w->cells)) + 1);
+    rc |= alloc(w, &w->round_count, MOST_ROUNDS + 1);
+    rc |= alloc(w, &w->round_start, MOST_ROUNDS + 2);
+    rc |= alloc(w, &w->round_fill, MOST_ROUNDS + 1);
+    if (w->has_grid) {
+        rc |= alloc(w, &w->keys, n);
+        rc |= alloc(w, &w->cell_count, w->cells);
+        rc |= alloc(w, &w->cell_start, (size_t)w->cells + 1);
+        rc |= alloc(w, &w->cell_fill, w->cells);
+        rc |= alloc(w, &w->order_tmp, n);
+        rc |= alloc(w, &w->order, n);
+        rc |= alloc(w, &w->reach, n);
+        rc |= alloc(w, &w->partner, (size_t)n * SLOTS);
+        rc |= alloc(w, &w->found, n);
+        rc |= alloc(w, &w->kept, n);
+        rc |= alloc(w, &w->cand_start, (size_t)n + 1);
+        rc |= alloc(w, &w->cand_a, w->cap);
+        rc |= alloc(w, &w->cand_b, w->cap);
+        rc |= alloc(w, &w->tcount, n);
+        for (int g = 0; g < 2; g++) {
+            PairBuffers& p = w->gen[g];
+            rc |= alloc(w, &p.tstart, (size_t)n + 1);
+            rc |= alloc(w, &p.ta, w->cap);
+            rc |= alloc(w, &p.tb, w->cap);
+            rc |= alloc(w, &p.tcand, w->cap);
+            rc |= alloc(w, &p.head, w->cap);
+            rc |= alloc(w, &p.axis, w->cap);
+            rc |= alloc(w, &p.pa, (size_t)w->cap * MOST_POINTS);
+            rc |= alloc(w, &p.pb, (size_t)w->cap * MOST_POINTS);
+            rc |= alloc(w, &p.imp, (size_t)w->cap * MOST_POINTS);
+            rc |= alloc(w, &p.impr, (size_t)w->cap * MOST_POINTS);
+        }
+        rc |= alloc(w, &w->colour, w->cap);
+        rc |= alloc(w, &w->inc_count, n);
+        rc |= alloc(w, &w->inc_start, (size_t)n + 1);
+        rc |= alloc(w, &w->inc_fill, n);
+        rc |= alloc(w, &w->inc_list, (size_t)w->cap * 2);
+        rc |= alloc(w, &w->round_list, w->cap);
+    }
+    if (rc) return bad(VXR_ECUDA);
+    if (cudaMallocHost(&w->host_totals, sizeof(Totals)) != cudaSuccess) return bad(VXR_ECUDA);
+    // Occupancy of the cooperative kernels: every block must be resident at once.
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve, SOLVE_THREADS, 0);
+    w->solve_blocks = std::max(1, per_sm) * w->sms;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_colour, THREADS, 0);
+    w->colour_blocks = std::max(1, per_sm) * w->sms;
+    // Everything starts at zero, as the reference's buffers do; every orientation the identity.
+    cudaStream_t st = w->stream;
+    cudaMemsetAsync(w->b.pose, 0, sizeof(float4) * n, st);
+    cudaMemsetAsync(w->b.vel, 0, sizeof(float4) * n, st);
+    cudaMemsetAsync(w->b.mom, 0, sizeof(float4) * n, st);
+    cudaMemsetAsync(w->b.half, 0, sizeof(float4) * n, st);
+    cudaMemsetAsync(w->wall, 0, sizeof(float4) * (size_t)n * WALL_RECORDS, st);
+    cudaMemsetAsync(w->wroll, 0, sizeof(float4) * (size_t)n * 6, st);
+    cudaMemsetAsync(w->wmask, 0, sizeof(unsigned long long) * n, st);
+    cudaMemsetAsync(w->shown, 0, sizeof(float) * (size_t)n * SHOWN_STRIDE, st);
+    cudaMemsetAsync(w->counters, 0, sizeof(Counters), st);
+    cudaMemsetAsync(w->totals, 0, sizeof(Totals), st);
+    if (w->has_grid) {
+        for (int g = 0; g < 2; g++) {
+            cudaMemsetAsync(w->gen[g].tstart, 0, sizeof(int) * ((size_t)n + 1), st);
+        }
+    }
+    if (upload4(w, w->b.turn, nullptr, nullptr, nullptr, nullptr, 1.0f)) return bad(VXR_ECUDA);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return bad(VXR_ECUDA);
+    set(VXR_OK);
+    return w;
+}
+
+void vxr_box_destroy(vxr_box_world* w) {
+    if (!w) return;
+    if (w->stream) cudaStreamSynchronize(w->stream);
+    for (void* p : w->allocations) cudaFree(p);
+    if (w->pinned) cudaFreeHost(w->pinned);
+    if (w->host_totals) cudaFreeHost(w->host_totals);
+    if (w->ev0) cudaEventDestroy(w->ev0);
+    if (w->ev1) cudaEventDestroy(w->ev1);
+    if (w->stream) cudaStreamDestroy(w->stream);
+    delete w;
+}
+
+const char* vxr_box_error(const vxr_box_world* w) { return w ? w->error.c_str() : "no world"; }
+
+int32_t vxr_box_params(vxr_box_world* w, const int32_t* params) {
+    if (!w || !params) return VXR_EINVAL;
+    std::memcpy(w->params.w, params, sizeof(float) * P_COUNT);
+    return VXR_OK;
+}
+
+int32_t vxr_box_load_state(vxr_box_world* w, const float* const* f, const int32_t* params) {
+    if (!w || !f) return VXR_EINVAL;
+    for (int k = 0; k < 18; k++)
+        if (!f[k]) return VXR_EINVAL;
+    cudaSetDevice(w->device);
+    int rc = clear_dynamic(w);
+    if (rc) return rc;
+    rc |= upload4(w, w->b.pose, f[0], f[1], f[2], f[13], 0.0f);
+    rc |= upload4(w, w->b.vel, f[3], f[4], f[5], nullptr, 0.0f);
+    rc |= upload4(w, w->b.mom, f[6], f[7], f[8], nullptr, 0.0f);
+    rc |= upload4(w, w->b.turn, f[9], f[10], f[11], f[12], 1.0f);
+    rc |= upload4(w, w->b.half, f[14], f[15], f[16], f[17], 0.0f);
+    if (rc) return VXR_ECUDA;
+    if (params) vxr_box_params(w, params);
+    return VXR_OK;
+}
+
+int32_t vxr_box_start(vxr_box_world* w, const float* x, const float* y, const float* z, const float* u,
+                      const float* v, const float* wv, const float* const* spin, const float* const* q,
+                      const float* const* half, const float* shape, const float* im, const int32_t* params) {
+    if (!w || !x || !y || !z || !u || !v || !wv || !spin || !q || !half || !shape || !im || !params)
+        return VXR_EINVAL;
+    const int n = w->n;
+    std::vector<float> l[3];
+    for (int a = 0; a < 3; a++) l[a].assign(n, 0.0f);
+    for (int s = 0; s < n; s++) {
+        if (im[s] <= 0) continue;
+        const double m = 1.0 / im[s];
+        double moment[3];
+        if (shape[s] > 0.5f) {
+            const double mo = 0.4 * m * half[0][s] * half[0][s];
+            moment[0] = moment[1] = moment[2] = mo;
+        } else {
+            const double hx = half[0][s], hy = half[1][s], hz = half[2][s];
+            moment[0] = m * (hy * hy + hz * hz) / 3;
+            moment[1] = m * (hx * hx + hz * hz) / 3;
+            moment[2] = m * (hx * hx + hy * hy) / 3;
+        }
+        const double qq[4] = {q[0][s], q[1][s], q[2][s], q[3][s]};
+        const double cq[4] = {-qq[0], -qq[1], -qq[2], qq[3]};
+        const double om[3] = {spin[0][s], spin[1][s], spin[2][s]};
+        double own[3], lb[3];
+        rotate_d(cq, om, own);
+        for (int a = 0; a < 3; a++) own[a] *= moment[a];
+        rotate_d(qq, own, lb);
+        for (int a = 0; a < 3; a++) l[a][s] = (float)lb[a];
+    }
+    const float* f[18] = {x, y, z, u, v, wv, l[0].data(), l[1].data(), l[2].data(), q[0], q[1], q[2], q[3],
+                          im, half[0], half[1], half[2], shape};
+    int rc = vxr_box_load_state(w, f, params);
+    if (rc) return rc;
+    // shown from the starting state (Boxes.shownAtStart :827-842)
+    std::vector<float> shown((size_t)n * SHOWN_STRIDE, 0.0f);
+    for (int s = 0; s < n; s++) {
+        float* sh = &shown[(size_t)s * SHOWN_STRIDE];
+        const float at[3] = {x[s], y[s], z[s]};
+        for (int a = 0; a < 3; a++) {
+            sh[0 + a] = sh[4 + a] = at[a];
+            sh[8 + a] = half[a][s];
+        }
+        sh[3] = shape[s];
+        for (int k = 0; k < 4; k++) sh[12 + k] = sh[16 + k] = q[k][s];
+    }
+    VXR_CUDA(cudaMemcpy(w->shown, shown.data(), sizeof(float) * shown.size(), cudaMemcpyHostToDevice));
+    return VXR_OK;
+}
+
+int32_t vxr_box_step_async(vxr_box_world* w, int32_t steps) {
+    if (!w || steps < 0) return VXR_EINVAL;
+    cudaSetDevice(w->device);
+    for (int k = 0; k < steps; k++) {
+        int rc = enqueue_step(w);
+        if (rc) return rc;
+    }
+    return VXR_OK;
+}
+
+int32_t vxr_box_sync(vxr_box_world* w, vxr_box_report* report) {
+    if (!w) return VXR_EINVAL;
+    VXR_CUDA(cudaMemcpyAsync(w->host_totals, w->totals, sizeof(Totals), cudaMemcpyDeviceToHost, w->stream));
+    VXR_CUDA(cudaMemsetAsync(w->totals, 0, sizeof(Totals), w->stream));
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    const Totals& t = *w->host_totals;
+    if (report) {
+        report->touching = t.last[0];
+        report->points = t.last[1];
+        report->rounds = t.last[2];
+        report->unplaced = t.last[3];
+        report->unlisted = t.last[4];
+        report->most_rounds = t.most_rounds;
+        report->unplaced_total = t.unplaced;
+        report->unlisted_total = t.unlisted;
+        report->status = t.status;
+        report->steps = t.steps;
+    }
+    switch (t.status) {
+        case ST_OK: return VXR_OK;
+        case ST_CAPACITY: w->error = "pair capacity exceeded"; return VXR_ECAPACITY;
+        case ST_ROUNDS: w->error = "colouring did not finish"; return VXR_EROUNDS;
+        case ST_TIMEOUT: w->error = "a grid barrier timed out"; return VXR_ETIMEOUT;
+        default: w->error = "step failed"; return VXR_ECUDA;
+    }
+}
+
+int32_t vxr_box_step(vxr_box_world* w, int32_t steps, vxr_box_report* report) {
+    int rc = vxr_box_step_async(w, steps);
+    if (rc) return rc;
+    return vxr_box_sync(w, report);
+}
+
+void* vxr_box_stream(vxr_box_world* w) { return w ? (void*)w->stream : nullptr; }
+
+int32_t vxr_box_state(vxr_box_world* w, float* const* out) {
+    if (!w || !out) return VXR_EINVAL;
+    cudaSetDevice(w->device);
+    int rc = 0;
+    rc |= download4(w, w->b.pose, out[0], out[1], out[2], nullptr);
+    rc |= download4(w, w->b.vel, out[3], out[4], out[5], nullptr);
+    rc |= download4(w, w->b.mom, out[6], out[7], out[8], nullptr);
+    rc |= download4(w, w->b.turn, out[9], out[10], out[11], out[12]);
+    return rc ? VXR_ECUDA : VXR_OK;
+}
+
+int32_t vxr_box_read_shown(vxr_box_world* w, float* out) {
+    if (!w || !out) return VXR_EINVAL;
+    VXR_CUDA(cudaMemcpyAsync(out, w->shown, sizeof(float) * (size_t)w->n * SHOWN_STRIDE, cudaMemcpyDeviceToHost,
+                             w->stream));
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    return VXR_OK;
+}
+
+int32_t vxr_box_touching(vxr_box_world* w, int32_t* first, int32_t* second, int32_t* points, float* manifold,
+                         float* impulses, int32_t capacity) {
+    if (!w) return -VXR_EINVAL;
+    if (!w->has_grid) return 0;
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    const PairBuffers& p = w->gen[w->cur ^ 1];  // the last step's
+    int P = 0;
+    VXR_CUDA(cudaMemcpy(&P, p.tstart + w->n, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!first && !second && !points && !manifold && !impulses) return P;
+    if (P > capacity) return -VXR_ECAPACITY;
+    std::vector<int> ta(P), tb(P), tc(P);
+    VXR_CUDA(cudaMemcpy(ta.data(), p.ta, sizeof(int) * P, cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(tb.data(), p.tb, sizeof(int) * P, cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(tc.data(), p.tcand, sizeof(int) * P, cudaMemcpyDeviceToHost));
+    std::vector<float4> head(1), pa(MOST_POINTS), pb(MOST_POINTS), imp((size_t)P * MOST_POINTS),
+        impr((size_t)P * MOST_POINTS);
+    if (impulses && P) {
+        VXR_CUDA(cudaMemcpy(imp.data(), p.imp, sizeof(float4) * P * MOST_POINTS, cudaMemcpyDeviceToHost));
+        VXR_CUDA(cudaMemcpy(impr.data(), p.impr, sizeof(float4) * P * MOST_POINTS, cudaMemcpyDeviceToHost));
+    }
+    for (int t = 0; t < P; t++) {
+        if (first) first[t] = ta[t];
+        if (second) second[t] = tb[t];
+        float ax = 0.0f;
+        VXR_CUDA(cudaMemcpy(head.data(), p.head + tc[t], sizeof(float4), cudaMemcpyDeviceToHost));
+        const int cnt = (int)head[0].w;
+        if (points) points[t] = cnt;
+        if (manifold) {
+            VXR_CUDA(cudaMemcpy(&ax, p.axis + tc[t], sizeof(float), cudaMemcpyDeviceToHost));
+            VXR_CUDA(cudaMemcpy(pa.data(), p.pa + (size_t)tc[t] * MOST_POINTS, sizeof(float4) * MOST_POINTS,
+                                cudaMemcpyDeviceToHost));
+            VXR_CUDA(cudaMemcpy(pb.data(), p.pb + (size_t)tc[t] * MOST_POINTS, sizeof(float4) * MOST_POINTS,
+                                cudaMemcpyDeviceToHost));
+            float* m = manifold + (size_t)t * MANIFOLD_WORDS;
+            std::memset(m, 0, sizeof(float) * MANIFOLD_WORDS);
+            m[0] = head[0].x;
+            m[1] = head[0].y;
+            m[2] = head[0].z;
+            m[3] = head[0].w;
+            m[4] = ax;
+            for (int i = 0; i < cnt && i < MOST_POINTS; i++) {
+                float* q = m + M_POINTS + i * M_POINT_WORDS;
+                q[0] = pa[i].x;
+                q[1] = pa[i].y;
+                q[2] = pa[i].z;
+                q[3] = pb[i].x;
+                q[4] = pb[i].y;
+                q[5] = pb[i].z;
+                q[6] = pa[i].w;
+            }
+        }
+        if (impulses) {
+            float* r = impulses + (size_t)t * 28;
+            for (int i = 0; i < MOST_POINTS; i++) {
+                const float4 a = imp[(size_t)t * MOST_POINTS + i], b = impr[(size_t)t * MOST_POINTS + i];
+                r[7 * i + 0] = a.x;
+                r[7 * i + 1] = a.y;
+                r[7 * i + 2] = a.z;
+                r[7 * i + 3] = a.w;
+                r[7 * i + 4] = b.x;
+                r[7 * i + 5] = b.y;
+                r[7 * i + 6] = b.z;
+            }
+        }
+    }
+    return P;
+}
+
+int32_t vxr_box_candidates(vxr_box_world* w, int32_t* pairs, int32_t capacity) {
+    if (!w) return -VXR_EINVAL;
+    if (!w->has_grid) return 0;
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    int C = 0;
+    VXR_CUDA(cudaMemcpy(&C, w->cand_start + w->n, sizeof(int), cudaMemcpyDeviceToHost));
+    C = std::min(C, w->cap);
+    if (!pairs) return C;
+    if (C > capacity) return -VXR_ECAPACITY;
+    std::vector<int> a(C), b(C);
+    VXR_CUDA(cudaMemcpy(a.data(), w->cand_a, sizeof(int) * C, cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(b.data(), w->cand_b, sizeof(int) * C, cudaMemcpyDeviceToHost));
+    for (int c = 0; c < C; c++) {
+        pairs[2 * c] = a[c];
+        pairs[2 * c + 1] = b[c];
+    }
+    return C;
+}
+
+int32_t vxr_box_walls(vxr_box_world* w, float* lambda, float* rub, float* rollw) {
+    if (!w) return VXR_EINVAL;
+    const int n = w->n;
+    std::vector<float4> rec((size_t)n * WALL_RECORDS), rr((size_t)n * 6);
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    VXR_CUDA(cudaMemcpy(rec.data(), w->wall, sizeof(float4) * rec.size(), cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(rr.data(), w->wroll, sizeof(float4) * rr.size(), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < rec.size(); i++) {
+        if (lambda) lambda[i] = rec[i].x;
+        if (rub) {
+            rub[3 * i] = rec[i].y;
+            rub[3 * i + 1] = rec[i].z;
+            rub[3 * i + 2] = rec[i].w;
+        }
+    }
+    if (rollw) {
+        std::memset(rollw, 0, sizeof(float) * (size_t)n * 144);
+        for (int s = 0; s < n; s++)
+            for (int wl = 0; wl < 6; wl++) {
+                const size_t at = ((size_t)s * WALL_RECORDS + wl * 8) * 3;
+                rollw[at] = rr[(size_t)s * 6 + wl].x;
+                rollw[at + 1] = rr[(size_t)s * 6 + wl].y;
+                rollw[at + 2] = rr[(size_t)s * 6 + wl].z;
+            }
+    }
+    return VXR_OK;
+}
+
+int32_t vxr_box_colour_waves(vxr_box_world* w) {
+    if (!w) return -VXR_EINVAL;
+    Counters c;
+    if (cudaMemcpy(&c, w->counters, sizeof(Counters), cudaMemcpyDeviceToHost) != cudaSuccess) return -VXR_ECUDA;
+    return c.colour_waves;
+}
+
+// The narrow phase alone over a caller's pairs (BoxContact.collide :136-246): host buffers in and out.
+int32_t vxr_collide(int32_t bodies, const float* const* f, const int32_t* params, int32_t npairs,
+                    const int32_t* pairs, float* manifold) {
+    if (bodies < 1 || !f || !params || npairs < 0 || !pairs || !manifold) return VXR_EINVAL;
+    for (int k = 0; k < 18; k++)
+        if (!f[k]) return VXR_EINVAL;
+    for (int p = 0; p < 2 * npairs; p++)
+        if (pairs[p] >= bodies || pairs[p] < -1) return VXR_EINVAL;
+    vxr_box_config cfg{};
+    cfg.bodies = bodies;
+    cfg.substeps = 1;
+    cfg.sweeps = 1;
+    int32_t st = 0;
+    vxr_box_world* w = vxr_box_create(&cfg, &st);
+    if (!w) return st;
+    int rc = vxr_box_load_state(w, f, params);
+    std::vector<int> a(std::max(npairs, 1)), b(std::max(npairs, 1));
+    for (int p = 0; p < npairs; p++) {
+        a[p] = pairs[2 * p];
+        b[p] = pairs[2 * p + 1];
+    }
+    int *da = nullptr, *db = nullptr, *dn = nullptr;
+    float4 *head = nullptr, *pa = nullptr, *pb = nullptr;
+    float* axis = nullptr;
+    rc = rc ? rc : alloc(w, &da, npairs);
+    rc = rc ? rc : alloc(w, &db, npairs);
+    rc = rc ? rc : alloc(w, &dn, 1);
+    rc = rc ? rc : alloc(w, &head, npairs);
+    rc = rc ? rc : alloc(w, &axis, npairs);
+    rc = rc ? rc : alloc(w, &pa, (size_t)npairs * MOST_POINTS);
+    rc = rc ? rc : alloc(w, &pb, (size_t)npairs * MOST_POINTS);
+    if (!rc && npairs > 0) {
+        // a pair whose second is -1 is empty: count 0 (BoxContact.java:147-150)
+        std::vector<int> na(a), nb(b);
+        int live = 0;
+        std::vector<int> where(npairs, -1);
+        for (int p = 0; p < npairs; p++)
+            if (b[p] >= 0 && a[p] >= 0) {
+                na[live] = a[p];
+                nb[live] = b[p];
+                where[p] = live++;
+            }
+        cudaMemcpy(da, na.data(), sizeof(int) * npairs, cudaMemcpyHostToDevice);
+        cudaMemcpy(db, nb.data(), sizeof(int) * npairs, cudaMemcpyHostToDevice);
+        cudaMemcpy(dn, &live, sizeof(int), cudaMemcpyHostToDevice);
+        k_collide<<<w->sms * 8, 128, 0, w->stream>>>(dn, npairs, w->params.w[P_MARGIN], da, db, w->b.pose,
+                                                      w->b.turn, w->b.half, head, axis, pa, pb);
+        std::vector<float4> h(npairs), A((size_t)npairs * MOST_POINTS), B((size_t)npairs * MOST_POINTS);
+        std::vector<float> ax(npairs);
+        if (cudaStreamSynchronize(w->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+            rc = VXR_ECUDA;
+        } else {
+            cudaMemcpy(h.data(), head, sizeof(float4) * npairs, cudaMemcpyDeviceToHost);
+            cudaMemcpy(ax.data(), axis, sizeof(float) * npairs, cudaMemcpyDeviceToHost);
+            cudaMemcpy(A.data(), pa, sizeof(float4) * A.size(), cudaMemcpyDeviceToHost);
+            cudaMemcpy(B.data(), pb, sizeof(float4) * B.size(), cudaMemcpyDeviceToHost);
+            for (int p = 0; p < npairs; p++) {
+                float* m = manifold + (size_t)p * MANIFOLD_WORDS;
+                std::memset(m, 0, sizeof(float) * MANIFOLD_WORDS);
+                const int q = where[p];
+                if (q < 0) continue;
+                const int cnt = (int)h[q].w;
+                m[0] = h[q].x;
+                m[1] = h[q].y;
+                m[2] = h[q].z;
+                m[3] = h[q].w;
+                m[4] = ax[q];
+                for (int i = 0; i < cnt; i++) {
+                    float* r = m + M_POINTS + i * M_POINT_WORDS;
+                    const float4 u = A[(size_t)q * MOST_POINTS + i], v = B[(size_t)q * MOST_POINTS + i];
+                    r[0] = u.x;
+                    r[1] = u.y;
+                    r[2] = u.z;
+                    r[3] = v.x;
+                    r[4] = v.y;
+                    r[5] = v.z;
+                    r[6] = u.w;
+                }
+            }
+        }
+    }
+    vxr_box_destroy(w);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,108 @@
+"""ctypes binding of libvxr.so, the C-ABI declared in include/vxr.h.
+
+The library is built in-tree (vexelray-sim-rigid_b200/csrc/Makefile). Loading it needs no GPU; stepping a world
+does, and fails loudly (an exception carrying the library's status and message) when there is none: there is no
+CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvxr.so")
+
+VXR_OK, VXR_EINVAL, VXR_ECAPACITY, VXR_EROUNDS, VXR_ENONFINITE, VXR_ETIMEOUT, VXR_ECUDA = range(7)
+STATUS_NAMES = {0: "VXR_OK", 1: "VXR_EINVAL", 2: "VXR_ECAPACITY", 3: "VXR_EROUNDS", 4: "VXR_ENONFINITE",
+                5: "VXR_ETIMEOUT", 6: "VXR_ECUDA"}
+
+#: Every symbol include/vxr.h declares (checked by the CPU test suite).
+SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_create", "vxr_box_destroy",
+           "vxr_box_error", "vxr_box_start", "vxr_box_load_state", "vxr_box_params", "vxr_box_step",
+           "vxr_box_step_async", "vxr_box_sync", "vxr_box_stream", "vxr_box_state", "vxr_box_read_shown",
+           "vxr_box_touching", "vxr_box_candidates", "vxr_box_walls", "vxr_box_colour_waves", "vxr_collide"]
+
+
+class VxrError(RuntimeError):
+    def __init__(self, status: int, message: str = ""):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("cell", ctypes.c_float)]
+
+
+class BoxConfig(ctypes.Structure):
+    _fields_ = [("bodies", ctypes.c_int32), ("substeps", ctypes.c_int32), ("sweeps", ctypes.c_int32),
+                ("symmetric", ctypes.c_int32), ("grid", Grid), ("reach_cells", ctypes.c_int32),
+                ("max_pairs", ctypes.c_int32), ("device", ctypes.c_int32)]
+
+
+class BoxReport(ctypes.Structure):
+    _fields_ = [("touching", ctypes.c_int32), ("points", ctypes.c_int32), ("rounds", ctypes.c_int32),
+                ("unplaced", ctypes.c_int32), ("unlisted", ctypes.c_int32), ("most_rounds", ctypes.c_int32),
+                ("unplaced_total", ctypes.c_int64), ("unlisted_total", ctypes.c_int64), ("status", ctypes.c_int32),
+                ("steps", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is not built: run `make -C vexelray-sim-rigid_b200/csrc` "
+                          "(or __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, f64, f32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_float
+        L.vxr_version.restype = ctypes.c_char_p
+        L.vxr_box_make_params.argtypes = [f64] * 11 + [vp]
+        L.vxr_box_make_params.restype = i32
+        L.vxr_box_make_grid.argtypes = [f64] * 5 + [ctypes.POINTER(Grid)]
+        L.vxr_box_make_grid.restype = i32
+        L.vxr_box_create.argtypes = [ctypes.POINTER(BoxConfig), ctypes.POINTER(i32)]
+        L.vxr_box_create.restype = vp
+        L.vxr_box_destroy.argtypes = [vp]
+        L.vxr_box_error.argtypes = [vp]
+        L.vxr_box_error.restype = ctypes.c_char_p
+        L.vxr_box_start.argtypes = [vp] + [vp] * 11 + [vp]
+        L.vxr_box_start.restype = i32
+        L.vxr_box_load_state.argtypes = [vp, vp, vp]
+        L.vxr_box_load_state.restype = i32
+        L.vxr_box_params.argtypes = [vp, vp]
+        L.vxr_box_params.restype = i32
+        L.vxr_box_step.argtypes = [vp, i32, ctypes.POINTER(BoxReport)]
+        L.vxr_box_step.restype = i32
+        L.vxr_box_step_async.argtypes = [vp, i32]
+        L.vxr_box_step_async.restype = i32
+        L.vxr_box_sync.argtypes = [vp, ctypes.POINTER(BoxReport)]
+        L.vxr_box_sync.restype = i32
+        L.vxr_box_stream.argtypes = [vp]
+        L.vxr_box_stream.restype = vp
+        L.vxr_box_state.argtypes = [vp, vp]
+        L.vxr_box_state.restype = i32
+        L.vxr_box_read_shown.argtypes = [vp, vp]
+        L.vxr_box_read_shown.restype = i32
+        L.vxr_box_touching.argtypes = [vp, vp, vp, vp, vp, vp, i32]
+        L.vxr_box_touching.restype = i32
+        L.vxr_box_candidates.argtypes = [vp, vp, i32]
+        L.vxr_box_candidates.restype = i32
+        L.vxr_box_walls.argtypes = [vp, vp, vp, vp]
+        L.vxr_box_walls.restype = i32
+        L.vxr_box_colour_waves.argtypes = [vp]
+        L.vxr_box_colour_waves.restype = i32
+        L.vxr_collide.argtypes = [i32, vp, vp, i32, vp, vp]
+        L.vxr_collide.restype = i32
+        _ = f32
+        _lib = L
+    return _lib
+
+
+def ptr(a) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+def ptr_array(arrays) -> ctypes.Array:
+    return (ctypes.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])

@@ -1,0 +1,216 @@
+"""BoxSimulation: the reference's box/mixed simulation API, on the B200 through the C-ABI.
+
+Mirrors gui/BoxSimulation.java (vexelray-sim-rigid-gui/src/main/java/dev/vexelray/sim/rigid/gui/BoxSimulation.java):
+``start`` :77-108, ``params`` :111-113, ``step_and_wait`` :115-142, ``last`` :145-147, ``state`` :153-160,
+``read_shown`` :163-165, ``close`` :183-188; and the step shape of core/box/BoxStep.java:117-198. Every call goes
+through libvxr.so; nothing here computes the step.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import boxes as B
+from ._lib import BoxConfig, BoxReport, Grid, VxrError, lib, ptr, ptr_array
+
+STATE_FIELDS = ["x", "y", "z", "u", "v", "w", "lx", "ly", "lz", "qx", "qy", "qz", "qw"]
+ALL_FIELDS = STATE_FIELDS + ["im", "hx", "hy", "hz", "shape"]
+
+
+@dataclass
+class Report:
+    """BoxStepper.Report (core/box/BoxStepper.java:308-311) of the last step, with totals over the call."""
+    touching: int
+    points: int
+    rounds: int
+    unplaced: int
+    unlisted: int
+    most_rounds: int = 0
+    unplaced_total: int = 0
+    unlisted_total: int = 0
+    steps: int = 0
+
+    def __iter__(self):
+        return iter((self.touching, self.points, self.rounds, self.unplaced, self.unlisted))
+
+
+def make_params(h, gx, gy, gz, sx, sy, sz, mu_static=0.0, mu_kinetic=0.0, margin=0.0, mu_rolling=0.0):
+    """Boxes.params through the library (the same words as vxr.boxes.params)."""
+    out = np.zeros(18, dtype=np.int32)
+    rc = lib().vxr_box_make_params(h, gx, gy, gz, sx, sy, sz, mu_static, mu_kinetic, margin, mu_rolling, ptr(out))
+    if rc:
+        raise VxrError(rc, "bad parameters")
+    return out
+
+
+class BoxSimulation:
+    """A box/mixed world on one GPU: BoxStep's shape plus BoxSimulation's calls."""
+
+    def __init__(self, bodies: int, substeps: int, sweeps: int = B.WALL_PASSES, symmetric: bool = False,
+                 grid: B.Grid | None = None, reach_cells: int = 0, max_pairs: int = 0, device: int = 0):
+        if bodies < 1 or substeps < 1 or sweeps < 1:
+            raise ValueError(f"a step needs bodies, substeps and sweeps, got {bodies}, {substeps} and {sweeps}")
+        self.L = lib()
+        cfg = BoxConfig()
+        cfg.bodies, cfg.substeps, cfg.sweeps, cfg.symmetric = bodies, substeps, sweeps, int(bool(symmetric))
+        if grid is not None:
+            cfg.grid = Grid(grid.nx, grid.ny, grid.nz, grid.cell)
+        cfg.reach_cells = reach_cells
+        cfg.max_pairs = max_pairs
+        cfg.device = device
+        status = ctypes.c_int32(0)
+        self.h = self.L.vxr_box_create(ctypes.byref(cfg), ctypes.byref(status))
+        if not self.h:
+            raise VxrError(status.value, "vxr_box_create failed")
+        self.n = bodies
+        self.grid = grid
+        self._last = Report(0, 0, 0, 0, 0)
+
+    # --- the reference's calls ---------------------------------------------------------------------------------
+
+    def start(self, x, y, z, u, v, w, spin, q, half, shape, im, params):
+        """BoxSimulation.start: angular velocities in, angular momentum kept."""
+        f = [np.ascontiguousarray(a, dtype=np.float32) for a in (x, y, z, u, v, w)]
+        sp = [np.ascontiguousarray(a, dtype=np.float32) for a in spin]
+        qq = [np.ascontiguousarray(a, dtype=np.float32) for a in q]
+        hh = [np.ascontiguousarray(a, dtype=np.float32) for a in half]
+        sh = np.ascontiguousarray(shape, dtype=np.float32)
+        mm = np.ascontiguousarray(im, dtype=np.float32)
+        pb = np.ascontiguousarray(params, dtype=np.int32)
+        rc = self.L.vxr_box_start(self.h, *[ptr(a) for a in f], ptr_array(sp), ptr_array(qq), ptr_array(hh),
+                                  ptr(sh), ptr(mm), ptr(pb))
+        self._check(rc)
+
+    def start_momentum(self, x, y, z, u, v, w, l, q, half, shape, im, params):
+        """Starts from a state with angular momentum given directly (the test fixture's way)."""
+        arrays = [x, y, z, u, v, w, l[0], l[1], l[2], q[0], q[1], q[2], q[3], im, half[0], half[1], half[2], shape]
+        f = [np.ascontiguousarray(a, dtype=np.float32) for a in arrays]
+        for a in f:
+            if a.shape != (self.n,):
+                raise ValueError(f"every field holds {self.n} floats")
+        pb = np.ascontiguousarray(params, dtype=np.int32)
+        self._check(self.L.vxr_box_load_state(self.h, ptr_array(f), ptr(pb)))
+
+    def params(self, params):
+        pb = np.ascontiguousarray(params, dtype=np.int32)
+        self._check(self.L.vxr_box_params(self.h, ptr(pb)))
+
+    def step_and_wait(self, steps: int = 1) -> Report:
+        rep = BoxReport()
+        rc = self.L.vxr_box_step(self.h, steps, ctypes.byref(rep))
+        self._check(rc)
+        self._last = Report(rep.touching, rep.points, rep.rounds, rep.unplaced, rep.unlisted, rep.most_rounds,
+                            rep.unplaced_total, rep.unlisted_total, rep.steps)
+        return self._last
+
+    def step(self, steps: int = 1) -> Report:
+        return self.step_and_wait(steps)
+
+    def step_async(self, steps: int = 1):
+        self._check(self.L.vxr_box_step_async(self.h, steps))
+
+    def sync(self) -> Report:
+        rep = BoxReport()
+        self._check(self.L.vxr_box_sync(self.h, ctypes.byref(rep)))
+        self._last = Report(rep.touching, rep.points, rep.rounds, rep.unplaced, rep.unlisted, rep.most_rounds,
+                            rep.unplaced_total, rep.unlisted_total, rep.steps)
+        return self._last
+
+    def last(self) -> Report:
+        return self._last
+
+    def state(self) -> list[np.ndarray]:
+        """x y z u v w lx ly lz qx qy qz qw, read back."""
+        out = [np.empty(self.n, dtype=np.float32) for _ in STATE_FIELDS]
+        self._check(self.L.vxr_box_state(self.h, ptr_array(out)))
+        return out
+
+    def field(self, name: str) -> np.ndarray:
+        return self.state()[STATE_FIELDS.index(name)]
+
+    def read_shown(self) -> np.ndarray:
+        out = np.empty(B.SHOWN_STRIDE * self.n, dtype=np.float32)
+        self._check(self.L.vxr_box_read_shown(self.h, ptr(out)))
+        return out
+
+    shown = read_shown
+
+    @property
+    def stream(self) -> int:
+        return self.L.vxr_box_stream(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.vxr_box_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    # --- inspection, for parity -------------------------------------------------------------------------------
+
+    def touching(self):
+        """(first, second, points, manifolds (P, 40), impulses (P, 28)) of the last step's touching pairs."""
+        n = self.L.vxr_box_touching(self.h, None, None, None, None, None, 0)
+        if n < 0:
+            raise VxrError(-n, self.error())
+        a = np.zeros(n, np.int32)
+        b = np.zeros(n, np.int32)
+        c = np.zeros(n, np.int32)
+        m = np.zeros((n, 40), np.float32)
+        imp = np.zeros((n, 28), np.float32)
+        got = self.L.vxr_box_touching(self.h, ptr(a), ptr(b), ptr(c), ptr(m), ptr(imp), n)
+        if got < 0:
+            raise VxrError(-got, self.error())
+        return a, b, c, m, imp
+
+    def touching_pairs(self):
+        a, b, c, _, _ = self.touching()
+        return [(int(x), int(y), int(z)) for x, y, z in zip(a, b, c)]
+
+    def touching_manifolds(self):
+        return list(self.touching()[3])
+
+    def touching_impulses(self):
+        return list(self.touching()[4])
+
+    def candidate_pairs(self) -> np.ndarray:
+        n = self.L.vxr_box_candidates(self.h, None, 0)
+        if n < 0:
+            raise VxrError(-n, self.error())
+        out = np.zeros(2 * n, np.int32)
+        got = self.L.vxr_box_candidates(self.h, ptr(out), n)
+        if got < 0:
+            raise VxrError(-got, self.error())
+        return out.reshape(-1, 2)
+
+    def walls(self):
+        lam = np.zeros(48 * self.n, np.float32)
+        rub = np.zeros(144 * self.n, np.float32)
+        rol = np.zeros(144 * self.n, np.float32)
+        self._check(self.L.vxr_box_walls(self.h, ptr(lam), ptr(rub), ptr(rol)))
+        return lam, rub, rol
+
+    def colour_waves(self) -> int:
+        return self.L.vxr_box_colour_waves(self.h)
+
+    def error(self) -> str:
+        return self.L.vxr_box_error(self.h).decode() if self.h else ""
+
+    def _check(self, rc):
+        if rc:
+            raise VxrError(rc, self.error())
+
+
+def collide_pairs(fields18, param_bits, pairs) -> np.ndarray:
+    """The narrow phase alone over a flat pair list, through vxr_collide: 40 words per pair."""
+    arrs = [np.ascontiguousarray(f, dtype=np.float32) for f in fields18]
+    pb = np.ascontiguousarray(param_bits, dtype=np.int32)
+    pr = np.ascontiguousarray(pairs, dtype=np.int32)
+    npairs = len(pr) // 2
+    out = np.zeros(40 * npairs, dtype=np.float32)
+    rc = lib().vxr_collide(len(arrs[0]), ptr_array(arrs), ptr(pb), npairs, ptr(pr), ptr(out))
+    if rc:
+        raise VxrError(rc, "vxr_collide failed")
+    return out
