@@ -1,0 +1,323 @@
+"""Benchmark: body-steps/s of the box/mixed rigid-body step on the large mixed scene (262,144 bodies).
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vxr|reference]
+
+One "step" is one simulation step of the scene: broad phase, narrow phase, warm-start carry, colouring and four
+substeps of ten sweeps of the coloured soft-step solve, all on the GPU. The scene is the large mixed configuration
+(seeded synthetic bodies of its shapes, sizes and distributions). The timed steps are steps W..W+K-1 of the drop.
+
+value : body-steps/s with the state resident in HBM, each step timed with CUDA events on the world's stream, L2
+        flushed (a 256 MiB write) before every timed step, summed over the K steps; max over ranks.
+e2e   : the same metric through the C-ABI with host buffers: each step new parameters copied in, one
+        vxr_box_step, and the state (13 floats a body) read back to host memory; wall clock, max over ranks.
+roofline : the solve kernel (the dominant one), algorithmic bytes per launch from the activity counted in the run
+        over its CUDA-event time, against the measured HBM copy bandwidth.
+cpu_baseline : the CPU oracle (a C++ restatement of the reference's kernels; the reference itself is Java built
+        on a library absent from this machine) with OpenMP on every host core, on a 1/16-volume sample of the scene.
+
+With N > 1 GPUs the scene does not shard (one connected pile): each rank steps its own replica (a different seed),
+and value sums the ranks' body-steps over the slowest rank's time ("replicas only").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "vexelray-sim-rigid_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "body-steps/s on 1 B200; solver iters to residual≤1e-4 m, warm-start vs plain"
+UNIT = "body-steps/s"
+BODIES = 262_144
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clocks and throttle reasons while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if len(s) > 8 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 8 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, name in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def all_max(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def all_sum(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def make_world(scene, device, max_pairs=0):
+    from vxr.box_simulation import BoxSimulation
+    w = BoxSimulation(scene["bodies"], scene["substeps"], scene["sweeps"], False, scene["grid"], device=device,
+                      max_pairs=max_pairs)
+    l = [scene["lx"], scene["ly"], scene["lz"]]
+    q = [scene["qx"], scene["qy"], scene["qz"], scene["qw"]]
+    h = [scene["hx"], scene["hy"], scene["hz"]]
+    w.start_momentum(scene["x"], scene["y"], scene["z"], scene["u"], scene["v"], scene["w"], l, q, h,
+                     scene["shape"], scene["im"], scene["params"])
+    return w
+
+
+def algorithmic_solve_bytes(n, substeps, sweeps, touching, points, active, wall_records):
+    """Bytes one solve launch (a step's substeps) must move: S [124 N + (2I+1)(96 N_c + P (16 + 88 k) + 56 W)],
+    P touching pairs, k points per pair, N_c bodies in a contact, W wall contact records held."""
+    k = points / touching if touching else 0.0
+    per_sweep = 96 * active + touching * (16 + 88 * k) + 56 * wall_records
+    return substeps * (124 * n + (2 * sweeps + 1) * per_sweep)
+
+
+def cpu_baseline(steps_timed: int = 24, warm: int = 2, fraction: float = 1 / 16):
+    """The oracle with OpenMP on every host core, on a 1/16-volume sample of the scene (same density)."""
+    from oracle.box import OracleBoxWorld, lib as orc_lib
+    from vxr import scenes
+    scene = scenes.sub_volume(BODIES, fraction)
+    w = OracleBoxWorld(scene["bodies"], scene["substeps"], scene["sweeps"], False, scene["grid"], threads=True)
+    for k in scenes.FIELDS:
+        w.set_field(k, scene[k])
+    w.set_params(scene["params"])
+    w.step(warm)
+    t0 = time.perf_counter()
+    w.step(steps_timed)
+    dt = time.perf_counter() - t0
+    cores = int(orc_lib(True).orc_threads())
+    w.close()
+    return {"value": scene["bodies"] * steps_timed / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{scene['bodies']} bodies (1/16 of the volume at the same density), steps {warm}.."
+                      f"{warm + steps_timed - 1} of the drop, {dt:.1f} s, OpenMP C++ oracle"}
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_setup()
+    if rank != 0:
+        return 0
+    steps = min(args.steps, 24)
+    warm = min(args.warmup, 3)
+    base = cpu_baseline(steps_timed=steps, warm=warm)
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "large mixed scene (262,144 bodies, 80% spheres / 20% boxes), bounded "
+                                   "1/16-volume sample per step", "bodies": BODIES, "substeps": 4, "sweeps": 10,
+                       "dt": 1 / 120},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference (Java on the SupirVast IR) cannot run here; its CPU path is restated as the "
+                    "C++ oracle, timed with every host thread"}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vxr", choices=["vxr", "reference"])
+    ap.add_argument("--bodies", type=int, default=BODIES)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--max-pairs", type=int, default=0, help="pair capacity of the world (0: 32 a body)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world_size, rank, local, pg = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from vxr import scenes
+
+    if args.bodies == BODIES:
+        scene = scenes.large_mixed(args.bodies, seed=1 + rank)
+    else:  # a smaller case of the same scene: the same body density over a smaller footprint
+        scene = scenes.sub_volume(BODIES, args.bodies / BODIES, seed=1 + rank)
+    w = make_world(scene, local, args.max_pairs)
+    stream = torch.cuda.ExternalStream(w.stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    # warm-up: steps 0..W-1
+    w.step_async(args.warmup)
+    w.sync()
+    launches0 = w.launches()
+    w.profile(True)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    activity = []
+    barrier(pg)
+    torch.cuda.synchronize()
+    with Clocks(local) as clocks:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                starts[k].record(stream)
+            w.step_async(1)
+            with torch.cuda.stream(stream):
+                ends[k].record(stream)
+            if k % 20 == 19:
+                rep = w.sync()
+        rep = w.sync()
+    torch.cuda.synchronize()
+    barrier(pg)
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    phases = w.profile(False)
+    launches = w.launches() - launches0
+    activity = w.activity()
+    total_ms = float(sum(step_ms))
+    slowest_ms = all_max(pg, total_ms)
+    bodies_all = all_sum(pg, float(scene["bodies"]))
+    value = bodies_all * args.steps / (slowest_ms / 1e3)
+
+    # roofline of the solve kernel: bytes per launch from the last step's activity, time per launch from events
+    hbm, which = peaks()
+    solve_ms = phases[3] / args.steps
+    b_solve = algorithmic_solve_bytes(scene["bodies"], scene["substeps"], scene["sweeps"], activity["touching"],
+                                      activity["points"], activity["bodies_active"], activity["wall_records"])
+    achieved = b_solve / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
+
+    e2e = None
+    if not args.no_e2e:
+        w2 = make_world(scene, local, args.max_pairs)
+        for _ in range(args.warmup):
+            w2.step_and_wait(1)
+            w2.state()
+        barrier(pg)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            w2.params(scene["params"])
+            w2.step_and_wait(1)
+            w2.state()
+        e2e_s = time.perf_counter() - t0
+        w2.close()
+        e2e_s = all_max(pg, e2e_s)
+        e2e = {"value": bodies_all * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 18 * 4,
+               "d2h_bytes_per_step": 13 * 4 * scene["bodies"]}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": slowest_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"large mixed scene: {scene['bodies']} bodies, 80% spheres r log-U[0.2,0.8] m, "
+                               "20% boxes half U[0.2,0.6] m, 128x64x128 m drop, v N(0,1), rho U[500,2000]",
+                   "bodies": scene["bodies"], "dt": scene["dt"], "substeps": scene["substeps"],
+                   "sweeps": scene["sweeps"], "mu": scene["mu"], "mu_rolling": scene["mu_rolling"],
+                   "grid": [scene["grid"].nx, scene["grid"].ny, scene["grid"].nz, scene["grid"].cell],
+                   "timed_steps": f"{args.warmup}..{args.warmup + args.steps - 1} of the drop",
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": "replicas" if world_size > 1 else "single"},
+        "phase_ms_per_step": {"broad": phases[0] / args.steps, "narrow": phases[1] / args.steps,
+                              "colour": phases[2] / args.steps, "solve": phases[3] / args.steps},
+        "last_step": {"touching": rep.touching, "points": rep.points, "rounds": rep.rounds,
+                      "unplaced": rep.unplaced, "unlisted": rep.unlisted, **activity},
+        "roofline": {"bound": "hbm", "kernel": "k_solve", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "peak_source": which,
+                     "bytes_per_launch": b_solve, "ms_per_launch": solve_ms},
+        "gpu_launches": int(launches),
+        "e2e": e2e,
+    }
+    line["clocks"] = clocks.summary()
+    if rank == 0 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_baseline()
+        except Exception as e:  # the baseline is reported, not required
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(e)}
+    w.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -151,6 +151,25 @@ int32_t vxr_box_walls(vxr_box_world* world, float* lambda48, float* rub144, floa
 /* How many dependency waves the last step's colouring took. */
 int32_t vxr_box_colour_waves(vxr_box_world* world);
 
+/* Kernels this world has launched since creation (each step launches the same number). */
+long long vxr_box_launches(vxr_box_world* world);
+
+/* Per-phase device time: with enable = 1 each following step records CUDA events on the world's stream around
+ * its broad phase, narrow phase (with the carry), colouring and solve; phase_ms4 receives the milliseconds
+ * summed since the last call (resolved at vxr_box_sync), and the sums restart. The reference reports one GPU
+ * time a step from Vulkan timestamps (gui/BoxSimulation.java:140-141). */
+int32_t vxr_box_profile(vxr_box_world* world, int32_t enable, double* phase_ms4);
+
+/* Phase trace of the solve: with enable = 1 each following step's solve kernel records, at the end of every
+ * phase, (phase code << 48) | device nanoseconds, where the code is kind | sweep << 4 | round << 8 (kinds: 0 start,
+ * 1 velocities, 2 walls, 3 positions, 4 a round of pairs, 5 the wall list). out receives the last traced step's
+ * entries; returns their number, or minus a status. */
+int32_t vxr_box_trace(vxr_box_world* world, int32_t enable, int64_t* out, int32_t capacity);
+
+/* Activity of the last step: touching pairs, their points, bodies in a touching pair or holding a wall impulse,
+ * and wall contact records held. */
+int32_t vxr_box_activity(vxr_box_world* world, int64_t* out4);
+
 /* The narrow phase alone over a caller's pair list: replaces the collide pass BoxContact.collide
  * (core/box/BoxContact.java:136-246) as the reference's BoxContactTest runs it. fields18 as for
  * vxr_box_load_state; pairs = first, second, ... (second -1: an empty slot); manifold40 receives 40 floats a pair. */

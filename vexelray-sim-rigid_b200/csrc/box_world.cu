@@ -47,17 +47,25 @@ struct Bodies {
     float4 *pose, *turn, *half, *vel, *mom;  // (x, y, z, im), (qx, qy, qz, qw), (hx, hy, hz, shape), (u, v, w, 0), (L, 0)
 };
 
-struct PairBuffers {  // one generation of the touching list and its solve data
-    int* tstart;      // [n+1] first touching pair of each body (as first body)
-    int* ta;          // [cap] first body
-    int* tb;          // [cap] second body
-    int* tcand;       // [cap] candidate index, where its manifold is
-    float4* head;     // [cap] per candidate: normal, count
-    float* axis;      // [cap] per candidate: the winning axis
-    float4* pa;       // [cap * 4] per candidate point: anchor on first, depth
-    float4* pb;       // [cap * 4] per candidate point: anchor on second
-    float4* imp;      // [cap * 4] per touching point: normal impulse, tangential impulse
-    float4* impr;     // [cap * 4] per touching point: rolling impulse
+struct Manifolds {  // the narrow phase's output, by candidate pair (the current step's)
+    float4* head;  // [cap] normal, point count
+    float* axis;   // [cap] the winning axis
+    float4* pa;    // [cap * 4] anchor on the first body, depth
+    float4* pb;    // [cap * 4] anchor on the second body
+};
+
+// One generation of the touching pairs, in round order (the order the solve reads them), with everything the
+// solve needs and the impulses they carry. The step before's generation is what the carry reads.
+struct PairGen {
+    int* tstart;     // [n+1] first touching pair of each body, in slot order
+    int* tb;         // [cap] second body of touching pair t (slot order)
+    int* pos;        // [cap] round-order position of touching pair t
+    int4* pair;      // [cap] by position: first, second, point count, t
+    float4* normal;  // [cap] by position: normal, winning axis
+    float4* pa;      // [cap * 4] by position: anchor on first, depth
+    float4* pb;      // [cap * 4] by position: anchor on second
+    float4* imp;     // [cap * 4] by position: normal impulse, tangential impulse
+    float4* impr;    // [cap * 4] by position: rolling impulse
 };
 
 struct Counters {  // device-side counts of a step
@@ -72,7 +80,8 @@ struct Counters {  // device-side counts of a step
     int abort;
     unsigned int bar_count, bar_gen;
     int remaining[3];
-    int pad[3];
+    int trace_len;
+    int pad[2];
 };
 
 struct Totals {  // accumulated over the steps of one vxr_box_step call
@@ -115,16 +124,30 @@ struct vxr_box_world {
     int *cand_a = nullptr, *cand_b = nullptr;
     int *tcount = nullptr;
     int *scan_tiles = nullptr;
-    PairBuffers gen[2]{};
+    Manifolds man{};
+    int *ta = nullptr, *tcand = nullptr;    // this step's touching pairs in slot order: first body, candidate
+    float4 *imp_t = nullptr, *impr_t = nullptr;  // carried impulses in slot order, before the round order
+    PairGen gen[2]{};
     int cur = 0;  // gen[cur] is this step's, gen[cur ^ 1] the step before's
+    int* wall_list = nullptr;    // [n] bodies near a wall or holding a wall impulse, rebuilt twice a substep
+    int* wall_count = nullptr;   // [2 * substeps] their counts
+    unsigned long long* trace = nullptr;  // phase end times of the last traced step
+    int trace_cap = 0, tracing = 0;
     int *colour = nullptr, *inc_count = nullptr, *inc_start = nullptr, *inc_fill = nullptr, *inc_list = nullptr;
-    int *round_count = nullptr, *round_start = nullptr, *round_fill = nullptr, *round_list = nullptr;
+    int *round_count = nullptr, *round_start = nullptr, *round_fill = nullptr;
     Counters* counters = nullptr;
     Totals* totals = nullptr;
     Totals* host_totals = nullptr;  // pinned
     float* pinned = nullptr;        // pinned staging for state transfers
     size_t pinned_bytes = 0;
     std::vector<void*> allocations;
+    long long launches = 0;  // kernels this world has launched
+    // phase timing: events around the broad phase, the narrow phase, the colouring and the solve of each step
+    int profile = 0;
+    std::vector<cudaEvent_t> events;  // 5 a step while profiling
+    int events_used = 0;
+    double phase_ms[4] = {0, 0, 0, 0};
+    long long* activity = nullptr;  // device scratch for vxr_box_activity
 };
 
 namespace {
@@ -349,22 +372,25 @@ __global__ void k_touch_list(int n, int cap, const int* __restrict__ cand_start,
 }
 
 // BoxPairs.carry :191-267: each new point takes the impulses of the nearest point of the same pair the step
-// before (anchor on the first body within 5% of its smallest half-extent), one point to one point always.
-__global__ void k_carry(const int* __restrict__ touching_n, PairBuffers now, PairBuffers was,
-                        const float4* __restrict__ half) {
+// before (anchor on the first body within 5% of its smallest half-extent), one point to one point always. The
+// pair the step before is found among its first body's touching pairs by the partner, as the reference finds its
+// slot; pairs that did not touch then carried nothing, as their slots held no points.
+__global__ void k_carry(const int* __restrict__ touching_n, const int* __restrict__ ta, const int* __restrict__ tb,
+                        const int* __restrict__ tcand, const Manifolds m, const PairGen was,
+                        const float4* __restrict__ half, float4* __restrict__ imp_t, float4* __restrict__ impr_t) {
     const int total = *touching_n;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const int s = now.ta[t], partner = now.tb[t];
-        const int c = now.tcand[t];
-        const int count = (int)now.head[c].w;
+        const int s = ta[t], partner = tb[t];
+        const int c = tcand[t];
+        const int count = (int)m.head[c].w;
         int old = -1;
         for (int u = was.tstart[s]; u < was.tstart[s + 1]; u++)
             if (was.tb[u] == partner) old = u;
         int before = 0;
-        int oc = 0;
+        long op = 0;
         if (old >= 0) {
-            oc = was.tcand[old];
-            before = (int)was.head[oc].w;
+            op = was.pos[old];
+            before = was.pair[op].z;
         }
         const float4 h = half[s];
         const float smallest = fminf(h.x, fminf(h.y, h.z));
@@ -372,26 +398,26 @@ __global__ void k_carry(const int* __restrict__ touching_n, PairBuffers now, Pai
         for (int point = 0; point < MOST_POINTS; point++) {
             float4 t0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), t1 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             if (point < count) {
-                const float4 anchor = now.pa[(long)c * MOST_POINTS + point];
+                const float4 anchor = m.pa[(long)c * MOST_POINTS + point];
                 float nearest = reach;
                 for (int o = 0; o < MOST_POINTS; o++) {
                     if (!(o < before)) continue;
-                    const float4 then = was.pa[(long)oc * MOST_POINTS + o];
+                    const float4 then = was.pa[op * MOST_POINTS + o];
                     const float gap[3] = {anchor.x - then.x, anchor.y - then.y, anchor.z - then.z};
                     const float d2 = dot3(gap, gap);
                     if (d2 < nearest) {
                         nearest = d2;
-                        t0 = was.imp[(long)old * MOST_POINTS + o];
-                        t1 = was.impr[(long)old * MOST_POINTS + o];
+                        t0 = was.imp[op * MOST_POINTS + o];
+                        t1 = was.impr[op * MOST_POINTS + o];
                     }
                 }
             }
             if (point == 0 && count == 1 && before == 1) {
-                t0 = was.imp[(long)old * MOST_POINTS];
-                t1 = was.impr[(long)old * MOST_POINTS];
+                t0 = was.imp[op * MOST_POINTS];
+                t1 = was.impr[op * MOST_POINTS];
             }
-            now.imp[(long)t * MOST_POINTS + point] = t0;
-            now.impr[(long)t * MOST_POINTS + point] = t1;
+            imp_t[(long)t * MOST_POINTS + point] = t0;
+            impr_t[(long)t * MOST_POINTS + point] = t1;
         }
     }
 }
@@ -448,6 +474,7 @@ __global__ void __launch_bounds__(THREADS) k_colour(const int* __restrict__ touc
     const int per = (total + threads - 1) / threads;
     const int lo = me * per, hi = min(total, lo + per);
     __shared__ int left_block;
+    unsigned int epoch = 0;
     for (int wave = 0;; wave++) {
         if (threadIdx.x == 0) left_block = 0;
         __syncthreads();
@@ -466,7 +493,7 @@ __global__ void __launch_bounds__(THREADS) k_colour(const int* __restrict__ touc
         if (left) atomicAdd(&left_block, left);
         __syncthreads();
         if (threadIdx.x == 0 && left_block) atomicAdd(&counters->remaining[wave % 3], left_block);
-        if (!grid_sync(bar)) return;
+        if (!grid_sync(bar, epoch)) return;
         const int remaining = *(volatile int*)&counters->remaining[wave % 3];
         if (blockIdx.x == 0 && threadIdx.x == 0) counters->remaining[(wave + 2) % 3] = 0;
         if (remaining == 0) {
@@ -484,23 +511,41 @@ __global__ void k_round_count(const int* __restrict__ touching_n, const int* __r
                               int* __restrict__ round_count, Counters* counters) {
     const int total = *touching_n;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const int c = colour[t];
-        if (c < MOST_ROUNDS) {
-            atomicAdd(&round_count[c], 1);
-            atomicMax(&counters->rounds, c + 1);
-        } else {
-            atomicAdd(&counters->unplaced, 1);
+        int c = colour[t];
+        if (c < 0 || c > MOST_ROUNDS) {  // never coloured: the colouring stopped early
+            atomicCAS(&counters->status, ST_OK, ST_ROUNDS);
+            c = MOST_ROUNDS;
         }
+        atomicAdd(&round_count[c], 1);
+        if (c < MOST_ROUNDS) atomicMax(&counters->rounds, c + 1);
+        else atomicAdd(&counters->unplaced, 1);
     }
 }
 
-__global__ void k_round_fill(const int* __restrict__ touching_n, const int* __restrict__ colour,
-                             const int* __restrict__ round_start, int* __restrict__ round_fill,
-                             int* __restrict__ round_list) {
+// The touching pairs gathered into round order: rounds 0..31, then the unplaced, each pair with its manifold and
+// carried impulses next to it, so a solve phase reads one contiguous record per pair. Within a round the order is
+// the atomic fill's: the pairs of a round share no body, so their order does not change any result.
+__global__ void k_order(const int* __restrict__ touching_n, const int* __restrict__ colour,
+                        const int* __restrict__ round_start, int* __restrict__ round_fill, const int* __restrict__ ta,
+                        const int* __restrict__ tcand, const Manifolds m, const float4* __restrict__ imp_t,
+                        const float4* __restrict__ impr_t, PairGen now) {
     const int total = *touching_n;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const int c = colour[t];
-        if (c < MOST_ROUNDS) round_list[round_start[c] + atomicAdd(&round_fill[c], 1)] = t;
+        int c = colour[t];
+        if (c < 0 || c > MOST_ROUNDS) c = MOST_ROUNDS;
+        const int p = round_start[c] + atomicAdd(&round_fill[c], 1);
+        now.pos[t] = p;
+        const int cd = tcand[t];
+        const float4 head = m.head[cd];
+        const int count = (int)head.w;
+        now.pair[p] = make_int4(ta[t], now.tb[t], count, t);
+        now.normal[p] = make_float4(head.x, head.y, head.z, m.axis[cd]);
+        for (int i = 0; i < count; i++) {
+            now.pa[(long)p * MOST_POINTS + i] = m.pa[(long)cd * MOST_POINTS + i];
+            now.pb[(long)p * MOST_POINTS + i] = m.pb[(long)cd * MOST_POINTS + i];
+            now.imp[(long)p * MOST_POINTS + i] = imp_t[(long)t * MOST_POINTS + i];
+            now.impr[(long)p * MOST_POINTS + i] = impr_t[(long)t * MOST_POINTS + i];
+        }
     }
 }
 
@@ -513,39 +558,30 @@ struct SolveArgs {
     float4* wall;
     float4* wroll;
     unsigned long long* wmask;
-    PairBuffers pairs;
+    int* wall_list;   // bodies that may touch a wall until positions next change, rebuilt twice a substep
+    int* wall_count;  // [2 * substeps] their counts
+    PairGen pairs;
     const int* round_start;
-    const int* round_list;
     Counters* counters;
     int substeps, sweeps, symmetric;
     Params params;
     GridBarrier bar;
+    unsigned long long* trace;  // null: not traced
+    int trace_cap;
 };
 
 __device__ __forceinline__ void load_held(Held& h, const Bodies& b, int s) {
-    h.load(b.pose[s], b.turn[s], b.half[s], b.vel[s], b.mom[s]);
+    h.load(b.pose[s], b.turn[s], __ldg(&b.half[s]), b.vel[s], b.mom[s]);
 }
 __device__ __forceinline__ void store_held(const Held& h, const Bodies& b, int s) {
     b.vel[s] = make_float4(h.velocity[0], h.velocity[1], h.velocity[2], 0.0f);
     b.mom[s] = make_float4(h.momentum[0], h.momentum[1], h.momentum[2], 0.0f);
 }
 
-// Boxes.velocities :276-289.
-__device__ void phase_velocities(const SolveArgs& A) {
-    const int stride = gridDim.x * blockDim.x;
-    const float h = A.params.w[P_H];
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += stride) {
-        if (!(A.b.pose[s].w > 0.0f)) continue;
-        float4 v = A.b.vel[s];
-        v.x = v.x + h * A.params.w[P_GX];
-        v.y = v.y + h * A.params.w[P_GY];
-        v.z = v.z + h * A.params.w[P_GZ];
-        A.b.vel[s] = v;
-    }
-}
+__device__ __forceinline__ void list_wall_body(const SolveArgs& A, int s, float4 pose, int slot);
 
-// Boxes.positions :299-342.
-__device__ void phase_positions(const SolveArgs& A) {
+// Boxes.positions :299-342, and the body listed for the relax sweeps' walls from where it now is.
+__device__ __forceinline__ void phase_positions(const SolveArgs& A, int slot) {
     const int stride = gridDim.x * blockDim.x;
     const float h = A.params.w[P_H];
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += stride) {
@@ -562,7 +598,7 @@ __device__ void phase_positions(const SolveArgs& A) {
         const float4 l = A.b.mom[s];
         const float momentum[3] = {l.x, l.y, l.z};
         float inverse[3];
-        inverse_inertia(A.b.half[s], im, inverse);
+        inverse_inertia(__ldg(&A.b.half[s]), im, inverse);
         float omega[3], mid[4], omega_mid[3], end[4];
         {
             const float c[4] = {-q[0], -q[1], -q[2], q[3]};
@@ -582,112 +618,161 @@ __device__ void phase_positions(const SolveArgs& A) {
         }
         turned(q, omega_mid, h, end);
         A.b.turn[s] = make_float4(end[0], end[1], end[2], end[3]);
+        list_wall_body(A, s, p, slot);
     }
 }
 
-// Boxes.walls :357-416: each body's corners (a sphere: its nearest point) against the six walls.
-__device__ void phase_walls(const SolveArgs& A, int sweep, bool reverse) {
-    const int stride = gridDim.x * blockDim.x;
-    const Params& P = A.params;
+// v[i] for a runtime i without indexing a local array (which would move the array to local memory).
+__device__ __forceinline__ float pick3(const float* v, int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
+
+// Which walls a body may touch: bit w set where the body's bounding sphere comes within the margin of wall w
+// (a bound that holds through f32 rounding: every corner's gap to a wall not in the set exceeds the margin).
+__device__ __forceinline__ unsigned near_walls(float4 pose, float4 hw, const Params& P) {
     const float margin = P.w[P_MARGIN];
+    const float r = hw.w > 0.5f ? hw.x : sqrtf((hw.x * hw.x + hw.y * hw.y) + hw.z * hw.z);
+    const float bound = r * 1.01f + 1e-3f + margin;
+    const float at[3] = {pose.x, pose.y, pose.z};
     const float extent[3] = {P.w[P_SX], P.w[P_SY], P.w[P_SZ]};
+    unsigned near = 0u;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (!(at[a] - bound > 0.0f)) near |= 1u << (2 * a);
+        if (!((extent[a] - at[a]) - bound > 0.0f)) near |= 1u << (2 * a + 1);
+    }
+    return near;
+}
+
+// The bodies the walls' sweeps must visit until positions next change: near a wall, or holding a wall impulse.
+// The order of the list does not matter: each body's walls touch that body alone.
+__device__ __forceinline__ void list_wall_body(const SolveArgs& A, int s, float4 pose, int slot) {
+    if (A.wmask[s] != 0ull || near_walls(pose, __ldg(&A.b.half[s]), A.params) != 0u)
+        A.wall_list[atomicAdd(&A.wall_count[slot], 1)] = s;
+}
+
+__device__ __forceinline__ void phase_velocities_and_list(const SolveArgs& A, int slot) {
+    const int stride = gridDim.x * blockDim.x;
+    const float h = A.params.w[P_H];
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += stride) {
         const float4 pose = A.b.pose[s];
         if (!(pose.w > 0.0f)) continue;
-        unsigned long long mask = A.wmask[s];
-        const float4 hw = A.b.half[s];
-        const bool sphere = hw.w > 0.5f;
-        if (mask == 0ull) {
-            if (sweep == WARM) continue;  // nothing held: the warm start applies nothing
-            // Far from every wall with nothing held: every contact's gap exceeds the margin (a bound that holds
-            // through f32 rounding), so no record is read or written.
-            const float r = sphere ? hw.x : sqrtf((hw.x * hw.x + hw.y * hw.y) + hw.z * hw.z);
-            const float bound = r * 1.01f + 1e-3f + margin;
-            if (pose.x - bound > 0.0f && (extent[0] - pose.x) - bound > 0.0f && pose.y - bound > 0.0f &&
-                (extent[1] - pose.y) - bound > 0.0f && pose.z - bound > 0.0f && (extent[2] - pose.z) - bound > 0.0f)
-                continue;
-        }
-        Held box;
-        load_held(box, A.b, s);
-        const Soft soft(P, true);
-        bool touched = false;
-        for (int order = 0; order < 6; order++) {
-            const int wall = reverse ? 5 - order : order;
-            const int axis = wall / 2;
-            const bool high = wall % 2 == 1;
-            float n[3];
-            for (int a = 0; a < 3; a++) n[a] = a == axis ? (high ? -1.0f : 1.0f) : 0.0f;
-            if (sphere) {
-                float r[3];
-                for (int a = 0; a < 3; a++) r[a] = -(box.half[0] * n[a]);
-                const float reach = box.at[axis] + r[axis];
-                const float gap = high ? extent[axis] - reach : reach;
-                const int bit = wall * 8, rbit = 48 + wall;
-                const bool held = (mask >> bit) & 1ull, rolled = (mask >> rbit) & 1ull;
-                const bool need = held || (sweep != WARM && gap < margin);
-                float4 rec = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                const long at = (long)s * WALL_RECORDS + wall * 8;
-                if (need) {
-                    rec = held ? A.wall[at] : rec;
-                    contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft);
-                    if (sweep != WARM) {
-                        A.wall[at] = rec;
-                        mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
-                    }
-                    touched = true;
-                }
-                if (rolled || (sweep != WARM && nonzero_bits(rec))) {
-                    float4 rr = rolled ? A.wroll[(long)s * 6 + wall] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                    roll<false>(sweep, box, box, box.half[0], rec.x, rr, P.w[P_MU_ROLLING]);
-                    if (sweep != WARM) {
-                        A.wroll[(long)s * 6 + wall] = rr;
-                        mask = nonzero_bits(rr) ? (mask | (1ull << rbit)) : (mask & ~(1ull << rbit));
-                    }
-                    touched = true;
-                }
-            } else {
-                for (int k = 0; k < 8; k++) {
-                    const int c = reverse ? 7 - k : k;
-                    float offset[3], r[3];
-                    for (int a = 0; a < 3; a++) {
-                        const int bit = (c >> a) & 1;
-                        offset[a] = box.half[a] * (2.0f * (float)bit - 1.0f);
-                    }
-                    rotateq(box.q, offset, r);
-                    const float reach = box.at[axis] + r[axis];
-                    const float gap = high ? extent[axis] - reach : reach;
-                    const int bit = wall * 8 + c;
-                    const bool held = (mask >> bit) & 1ull;
-                    if (!(held || (sweep != WARM && gap < margin))) continue;
-                    const long at = (long)s * WALL_RECORDS + bit;
-                    float4 rec = held ? A.wall[at] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                    contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft);
-                    if (sweep != WARM) {
-                        A.wall[at] = rec;
-                        mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
-                    }
-                    touched = true;
-                }
-            }
-        }
-        if (touched) {
-            store_held(box, A.b, s);
-            A.wmask[s] = mask;
-        }
+        float4 v = A.b.vel[s];
+        v.x = v.x + h * A.params.w[P_GX];
+        v.y = v.y + h * A.params.w[P_GY];
+        v.z = v.z + h * A.params.w[P_GZ];
+        A.b.vel[s] = v;
+        list_wall_body(A, s, pose, slot);
     }
 }
 
-// BoxPairs.solve :64-151: one round of pairs that share no body.
-__device__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r) {
+// Boxes.walls :357-416 for one body held in registers: its corners (a sphere: its nearest point) against the six
+// walls. A wall the body is far from, with no impulse held against it, is skipped: its contacts would neither
+// start nor apply. Returns whether anything was applied (the caller then stores the body).
+__device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, int sweep, bool reverse) {
+    const Params& P = A.params;
+    const float margin = P.w[P_MARGIN];
+    const float extent[3] = {P.w[P_SX], P.w[P_SY], P.w[P_SZ]};
+    unsigned long long mask = A.wmask[s];
+    const float4 pose = make_float4(box.at[0], box.at[1], box.at[2], box.im);
+    const float4 hw = make_float4(box.half[0], box.half[1], box.half[2], box.shape);
+    const bool sphere = hw.w > 0.5f;
+    const unsigned near = sweep == WARM ? 0u : near_walls(pose, hw, P);
+    unsigned held_walls = 0u;
+#pragma unroll
+    for (int wl = 0; wl < 6; wl++) {
+        const unsigned long long bits = (0xffull << (8 * wl)) | (1ull << (48 + wl));
+        if (mask & bits) held_walls |= 1u << wl;
+    }
+    const unsigned visit = near | held_walls;
+    if (visit == 0u) return false;
+    const Soft soft(P, true);
+    bool touched = false;
+    for (int order = 0; order < 6; order++) {
+        const int wall = reverse ? 5 - order : order;
+        if (!((visit >> wall) & 1u)) continue;
+        const int axis = wall / 2;
+        const bool high = wall % 2 == 1;
+        float n[3];
+        for (int a = 0; a < 3; a++) n[a] = a == axis ? (high ? -1.0f : 1.0f) : 0.0f;
+        if (sphere) {
+            float r[3];
+            for (int a = 0; a < 3; a++) r[a] = -(box.half[0] * n[a]);
+            const float reach = pick3(box.at, axis) + pick3(r, axis);
+            const float gap = high ? pick3(extent, axis) - reach : reach;
+            const int bit = wall * 8, rbit = 48 + wall;
+            const bool held = (mask >> bit) & 1ull, rolled = (mask >> rbit) & 1ull;
+            const bool need = held || (sweep != WARM && gap < margin);
+            float4 rec = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const long at = (long)s * WALL_RECORDS + wall * 8;
+            if (need) {
+                rec = held ? A.wall[at] : rec;
+                contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft);
+                if (sweep != WARM) {
+                    A.wall[at] = rec;
+                    mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
+                }
+                touched = true;
+            }
+            if (rolled || (sweep != WARM && nonzero_bits(rec))) {
+                float4 rr = rolled ? A.wroll[(long)s * 6 + wall] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                roll<false>(sweep, box, box, box.half[0], rec.x, rr, P.w[P_MU_ROLLING]);
+                if (sweep != WARM) {
+                    A.wroll[(long)s * 6 + wall] = rr;
+                    mask = nonzero_bits(rr) ? (mask | (1ull << rbit)) : (mask & ~(1ull << rbit));
+                }
+                touched = true;
+            }
+        } else {
+            for (int k2 = 0; k2 < 8; k2++) {
+                const int c = reverse ? 7 - k2 : k2;
+                const int bit = wall * 8 + c;
+                const bool held = (mask >> bit) & 1ull;
+                if (!held && (sweep == WARM || !((near >> wall) & 1u))) continue;
+                float offset[3], r[3];
+                for (int a = 0; a < 3; a++) {
+                    const int sgn = (c >> a) & 1;
+                    offset[a] = box.half[a] * (2.0f * (float)sgn - 1.0f);
+                }
+                rotateq(box.q, offset, r);
+                const float reach = pick3(box.at, axis) + pick3(r, axis);
+                const float gap = high ? pick3(extent, axis) - reach : reach;
+                if (!(held || (sweep != WARM && gap < margin))) continue;
+                const long at = (long)s * WALL_RECORDS + bit;
+                float4 rec = held ? A.wall[at] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft);
+                if (sweep != WARM) {
+                    A.wall[at] = rec;
+                    mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
+                }
+                touched = true;
+            }
+        }
+    }
+    if (touched) A.wmask[s] = mask;
+    return touched;
+}
+
+// Boxes.walls :357-416 over the listed bodies, each loaded afresh (its angular velocity from its angular
+// momentum, as the reference's walls kernel loads it).
+__device__ __forceinline__ void phase_walls(const SolveArgs& A, int sweep, bool reverse, int slot) {
+    const int stride = gridDim.x * blockDim.x;
+    const int listed = *(volatile int*)&A.wall_count[slot];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < listed; k += stride) {
+        const int s = A.wall_list[k];
+        Held box;
+        load_held(box, A.b, s);
+        if (walls_of(A, box, s, sweep, reverse)) store_held(box, A.b, s);
+    }
+}
+
+// BoxPairs.solve :64-151: one round of pairs that share no body, each read as one record in round order.
+__device__ __forceinline__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r) {
     const int stride = gridDim.x * blockDim.x;
     const Params& P = A.params;
     const int lo = A.round_start[r], hi = A.round_start[r + 1];
     for (int k = lo + blockIdx.x * blockDim.x + threadIdx.x; k < hi; k += stride) {
-        const int t = A.round_list[k];
-        const int c = A.pairs.tcand[t];
-        const float4 head = A.pairs.head[c];
-        const int count = (int)head.w;
-        const int ia = A.pairs.ta[t], ib = A.pairs.tb[t];
+        const int4 rec4 = A.pairs.pair[k];
+        const float4 head = A.pairs.normal[k];
+        const int ia = rec4.x, ib = rec4.y, count = rec4.z;
         Held first, second;
         load_held(first, A.b, ia);
         load_held(second, A.b, ib);
@@ -702,8 +787,9 @@ __device__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r) 
         for (int order = 0; order < MOST_POINTS; order++) {
             const int slot = reverse ? MOST_POINTS - 1 - order : order;
             if (!(slot < count)) continue;
-            const float4 qa = A.pairs.pa[(long)c * MOST_POINTS + slot];
-            const float4 qb = A.pairs.pb[(long)c * MOST_POINTS + slot];
+            const long at = (long)k * MOST_POINTS + slot;
+            const float4 qa = A.pairs.pa[at];
+            const float4 qb = A.pairs.pb[at];
             const float anchorA[3] = {qa.x, qa.y, qa.z}, anchorB[3] = {qb.x, qb.y, qb.z};
             float rA[3], rB[3];
             rotateq(first.q, anchorA, rA);
@@ -715,7 +801,6 @@ __device__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r) 
             float gap = ((second.at[0] + rB[0]) - (first.at[0] + rA[0])) * n[0] +
                         ((second.at[1] + rB[1]) - (first.at[1] + rA[1])) * n[1];
             gap = gap + ((second.at[2] + rB[2]) - (first.at[2] + rA[2])) * n[2];
-            const long at = (long)t * MOST_POINTS + slot;
             float4 rec = A.pairs.imp[at];
             contact<true>(sweep, gap, n, first, rA, second, rB, rec, soft);
             if (sweep != WARM) A.pairs.imp[at] = rec;
@@ -734,36 +819,60 @@ __device__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r) 
     }
 }
 
-__device__ bool sweep_all(const SolveArgs& A, int kind, bool reverse, int rounds) {
+// Phase codes of the trace: kind | sweep << 4 | round << 8.
+enum : int { TR_START = 0, TR_VELOCITIES = 1, TR_WALLS = 2, TR_POSITIONS = 3, TR_ROUND = 4, TR_WALL_LIST = 5 };
+
+struct Tracer {
+    unsigned long long* out;
+    int cap, len;
+    __device__ __forceinline__ void mark(int code) {
+        if (out && blockIdx.x == 0 && threadIdx.x == 0 && len < cap)
+            out[len++] = ((unsigned long long)code << 48) | (global_ns() & 0xffffffffffffull);
+    }
+};
+
+// One sweep (BoxStep.sweep :253-267): every round of pairs, then the walls; backward, the walls first and the
+// rounds last to first.
+__device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsigned int& epoch, int kind, bool reverse,
+                                          int rounds, int slot) {
     if (reverse) {
-        phase_walls(A, kind, true);
-        if (!grid_sync(A.bar)) return false;
+        phase_walls(A, kind, true, slot);
+        if (!grid_sync(A.bar, epoch)) return false;
+        tr.mark(TR_WALLS | kind << 4);
     }
     for (int order = 0; order < rounds; order++) {
         const int r = reverse ? rounds - 1 - order : order;
         phase_round(A, kind, reverse, r);
-        if (!grid_sync(A.bar)) return false;
+        if (!grid_sync(A.bar, epoch)) return false;
+        tr.mark(TR_ROUND | kind << 4 | r << 8);
     }
     if (!reverse) {
-        phase_walls(A, kind, false);
-        if (!grid_sync(A.bar)) return false;
+        phase_walls(A, kind, false, slot);
+        if (!grid_sync(A.bar, epoch)) return false;
+        tr.mark(TR_WALLS | kind << 4);
     }
     return true;
 }
 
 __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(SolveArgs A) {
     const int rounds = *(volatile int*)&A.counters->rounds;
+    Tracer tr{A.trace, A.trace_cap, 0};
+    unsigned int epoch = 0;
+    tr.mark(TR_START);
     for (int sub = 0; sub < A.substeps; sub++) {
-        phase_velocities(A);
-        if (!grid_sync(A.bar)) return;
-        if (!sweep_all(A, WARM, false, rounds)) return;
+        phase_velocities_and_list(A, 2 * sub);
+        if (!grid_sync(A.bar, epoch)) return;
+        tr.mark(TR_VELOCITIES);
+        if (!sweep_all(A, tr, epoch, WARM, false, rounds, 2 * sub)) return;
         for (int sw = 0; sw < A.sweeps; sw++)
-            if (!sweep_all(A, SOLVE, A.symmetric && sw % 2 == 1, rounds)) return;
-        phase_positions(A);
-        if (!grid_sync(A.bar)) return;
+            if (!sweep_all(A, tr, epoch, SOLVE, A.symmetric && sw % 2 == 1, rounds, 2 * sub)) return;
+        phase_positions(A, 2 * sub + 1);
+        if (!grid_sync(A.bar, epoch)) return;
+        tr.mark(TR_POSITIONS);
         for (int sw = 0; sw < A.sweeps; sw++)
-            if (!sweep_all(A, RELAX, A.symmetric && sw % 2 == 1, rounds)) return;
+            if (!sweep_all(A, tr, epoch, RELAX, A.symmetric && sw % 2 == 1, rounds, 2 * sub + 1)) return;
     }
+    if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) A.counters->trace_len = tr.len;
 }
 
 // Boxes.show :801-820.
@@ -805,6 +914,18 @@ __global__ void k_totals(const Counters* c, Totals* t) {
     t->steps += 1;
 }
 
+// Activity of the last step, for the solve's algorithmic byte count: bodies in a touching pair or holding a
+// wall impulse, and wall records held.
+__global__ void k_activity(int n, const int* __restrict__ inc_count, const unsigned long long* __restrict__ wmask,
+                           long long* out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const unsigned long long m = wmask[s];
+    const bool paired = inc_count != nullptr && inc_count[s] > 0;
+    if (paired || m) atomicAdd((unsigned long long*)&out[0], 1ull);
+    if (m) atomicAdd((unsigned long long*)&out[1], (unsigned long long)__popcll(m));
+}
+
 // ------------------------------------------------------------------------------------------------------------
 // Host orchestration.
 
@@ -826,13 +947,32 @@ GridBarrier barrier_of(vxr_box_world* w) {
     return g;
 }
 
+int mark(vxr_box_world* w, int which) {
+    if (!w->profile) return VXR_OK;
+    const int need = w->events_used + 1;
+    while ((int)w->events.size() < need) {
+        cudaEvent_t e;
+        VXR_CUDA(cudaEventCreate(&e));
+        w->events.push_back(e);
+    }
+    (void)which;
+    VXR_CUDA(cudaEventRecord(w->events[w->events_used++], w->stream));
+    return VXR_OK;
+}
+
+// Launches per step, counted as they are made.
+#define LAUNCHED(k) (w->launches += (k))
+
 // One whole step, enqueued on the world's stream.
 int enqueue_step(vxr_box_world* w) {
     cudaStream_t st = w->stream;
     const int n = w->n;
+    int rc0 = mark(w, 0);
+    if (rc0) return rc0;
     VXR_CUDA(cudaMemsetAsync(w->counters, 0, sizeof(Counters), st));
-    PairBuffers& now = w->gen[w->cur];
-    PairBuffers& was = w->gen[w->cur ^ 1];
+    VXR_CUDA(cudaMemsetAsync(w->wall_count, 0, sizeof(int) * 2 * w->substeps, st));
+    PairGen& now = w->gen[w->cur];
+    PairGen& was = w->gen[w->cur ^ 1];
     if (w->has_grid) {
         GridDims g{w->nx, w->ny, w->nz, w->cell, w->reach_cells};
         const float margin = w->params.w[P_MARGIN];
@@ -849,27 +989,33 @@ int enqueue_step(vxr_box_world* w) {
         exclusive_scan(w->kept, w->cand_start, n, w->scan_tiles, st);
         k_candidates<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->kept, w->cand_start, w->partner,
                                                                 w->cand_a, w->cand_b, w->counters);
+        LAUNCHED(4 + 3 + 3 + 1);  // bin, scatter, stable, list, two scans of three, candidates
+        if (int rc = mark(w, 1)) return rc;
         const int cblocks = w->sms * 8;
         k_collide<<<cblocks, 128, 0, st>>>(w->cand_start + n, w->cap, margin, w->cand_a, w->cand_b, w->b.pose,
-                                            w->b.turn, w->b.half, now.head, now.axis, now.pa, now.pb);
-        k_touch_count<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->cand_start, now.head, w->tcount);
+                                            w->b.turn, w->b.half, w->man.head, w->man.axis, w->man.pa, w->man.pb);
+        k_touch_count<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->cand_start, w->man.head,
+                                                                 w->tcount);
         exclusive_scan(w->tcount, now.tstart, n, w->scan_tiles, st);
-        k_touch_list<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->cand_start, w->cand_b, now.head,
-                                                                now.tstart, now.ta, now.tb, now.tcand, w->counters);
+        k_touch_list<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->cand_start, w->cand_b, w->man.head,
+                                                                now.tstart, w->ta, now.tb, w->tcand, w->counters);
         const int tblocks = w->sms * 4;
-        k_carry<<<tblocks, THREADS, 0, st>>>(now.tstart + n, now, was, w->b.half);
+        k_carry<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->ta, now.tb, w->tcand, w->man, was, w->b.half,
+                                            w->imp_t, w->impr_t);
+        LAUNCHED(1 + 1 + 3 + 1 + 1);  // collide, touch count, scan, touch list, carry
+        if (int rc = mark(w, 2)) return rc;
         // colouring
         VXR_CUDA(cudaMemsetAsync(w->inc_count, 0, sizeof(int) * n, st));
         VXR_CUDA(cudaMemsetAsync(w->inc_fill, 0, sizeof(int) * n, st));
         VXR_CUDA(cudaMemsetAsync(w->colour, 0xff, sizeof(int) * w->cap, st));
-        k_inc_count<<<tblocks, THREADS, 0, st>>>(now.tstart + n, now.ta, now.tb, w->inc_count);
+        k_inc_count<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->ta, now.tb, w->inc_count);
         exclusive_scan(w->inc_count, w->inc_start, n, w->scan_tiles, st);
-        k_inc_fill<<<tblocks, THREADS, 0, st>>>(now.tstart + n, now.ta, now.tb, w->inc_start, w->inc_fill,
+        k_inc_fill<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->ta, now.tb, w->inc_start, w->inc_fill,
                                                w->inc_list);
         {
             const int* tn = now.tstart + n;
             GridBarrier bar = barrier_of(w);
-            void* args[] = {(void*)&tn, (void*)&now.ta, (void*)&now.tb, (void*)&w->inc_start, (void*)&w->inc_list,
+            void* args[] = {(void*)&tn, (void*)&w->ta, (void*)&now.tb, (void*)&w->inc_start, (void*)&w->inc_list,
                             (void*)&w->colour, (void*)&w->counters, (void*)&bar};
             int rc = launch_cooperative(w, (const void*)k_colour, w->colour_blocks, THREADS, args);
             if (rc) return rc;
@@ -877,10 +1023,15 @@ int enqueue_step(vxr_box_world* w) {
         VXR_CUDA(cudaMemsetAsync(w->round_count, 0, sizeof(int) * (MOST_ROUNDS + 1), st));
         VXR_CUDA(cudaMemsetAsync(w->round_fill, 0, sizeof(int) * (MOST_ROUNDS + 1), st));
         k_round_count<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_count, w->counters);
-        exclusive_scan(w->round_count, w->round_start, MOST_ROUNDS, w->scan_tiles, st);
-        k_round_fill<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_start, w->round_fill,
-                                                 w->round_list);
+        exclusive_scan(w->round_count, w->round_start, MOST_ROUNDS + 1, w->scan_tiles, st);
+        k_order<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_start, w->round_fill, w->ta,
+                                            w->tcand, w->man, w->imp_t, w->impr_t, now);
+        LAUNCHED(1 + 3 + 1 + 1 + 1 + 3 + 1);  // inc count, scan, inc fill, colour, round count, scan, order
+    } else {
+        if (int rc = mark(w, 1)) return rc;
+        if (int rc = mark(w, 2)) return rc;
     }
+    if (int rc = mark(w, 3)) return rc;
     {
         SolveArgs A;
         A.n = n;
@@ -888,22 +1039,27 @@ int enqueue_step(vxr_box_world* w) {
         A.wall = w->wall;
         A.wroll = w->wroll;
         A.wmask = w->wmask;
+        A.wall_list = w->wall_list;
+        A.wall_count = w->wall_count;
         A.pairs = now;
         A.round_start = w->round_start;
-        A.round_list = w->round_list;
         A.counters = w->counters;
         A.substeps = w->substeps;
         A.sweeps = w->sweeps;
         A.symmetric = w->symmetric;
         A.params = w->params;
         A.bar = barrier_of(w);
+        A.trace = w->tracing ? w->trace : nullptr;
+        A.trace_cap = w->trace_cap;
         VXR_CUDA(cudaMemsetAsync(&w->counters->bar_count, 0, 2 * sizeof(unsigned int), st));
         void* args[] = {(void*)&A};
         int rc = launch_cooperative(w, (const void*)k_solve, w->solve_blocks, SOLVE_THREADS, args);
         if (rc) return rc;
     }
+    if (int rc = mark(w, 4)) return rc;
     k_show<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->b, w->shown);
     k_totals<<<1, 1, 0, st>>>(w->counters, w->totals);
+    LAUNCHED(1 + 2);  // solve, show, totals
     VXR_CUDA(cudaGetLastError());
     if (w->has_grid) w->cur ^= 1;
     return VXR_OK;
@@ -1098,6 +1254,8 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     rc |= alloc(w, &w->scan_tiles, scan_tiles_for(std::max(n, w->cells)) + 1);
     rc |= alloc(w, &w->round_count, MOST_ROUNDS + 1);
     rc |= alloc(w, &w->round_start, MOST_ROUNDS + 2);
+    rc |= alloc(w, &w->wall_list, n);
+    rc |= alloc(w, &w->wall_count, 2 * (size_t)w->substeps);
     rc |= alloc(w, &w->round_fill, MOST_ROUNDS + 1);
     if (w->has_grid) {
         rc |= alloc(w, &w->keys, n);
@@ -1114,14 +1272,21 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
         rc |= alloc(w, &w->cand_a, w->cap);
         rc |= alloc(w, &w->cand_b, w->cap);
         rc |= alloc(w, &w->tcount, n);
+        rc |= alloc(w, &w->man.head, w->cap);
+        rc |= alloc(w, &w->man.axis, w->cap);
+        rc |= alloc(w, &w->man.pa, (size_t)w->cap * MOST_POINTS);
+        rc |= alloc(w, &w->man.pb, (size_t)w->cap * MOST_POINTS);
+        rc |= alloc(w, &w->ta, w->cap);
+        rc |= alloc(w, &w->tcand, w->cap);
+        rc |= alloc(w, &w->imp_t, (size_t)w->cap * MOST_POINTS);
+        rc |= alloc(w, &w->impr_t, (size_t)w->cap * MOST_POINTS);
         for (int g = 0; g < 2; g++) {
-            PairBuffers& p = w->gen[g];
+            PairGen& p = w->gen[g];
             rc |= alloc(w, &p.tstart, (size_t)n + 1);
-            rc |= alloc(w, &p.ta, w->cap);
             rc |= alloc(w, &p.tb, w->cap);
-            rc |= alloc(w, &p.tcand, w->cap);
-            rc |= alloc(w, &p.head, w->cap);
-            rc |= alloc(w, &p.axis, w->cap);
+            rc |= alloc(w, &p.pos, w->cap);
+            rc |= alloc(w, &p.pair, w->cap);
+            rc |= alloc(w, &p.normal, w->cap);
             rc |= alloc(w, &p.pa, (size_t)w->cap * MOST_POINTS);
             rc |= alloc(w, &p.pb, (size_t)w->cap * MOST_POINTS);
             rc |= alloc(w, &p.imp, (size_t)w->cap * MOST_POINTS);
@@ -1132,7 +1297,6 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
         rc |= alloc(w, &w->inc_start, (size_t)n + 1);
         rc |= alloc(w, &w->inc_fill, n);
         rc |= alloc(w, &w->inc_list, (size_t)w->cap * 2);
-        rc |= alloc(w, &w->round_list, w->cap);
     }
     if (rc) return bad(VXR_ECUDA);
     if (cudaMallocHost(&w->host_totals, sizeof(Totals)) != cudaSuccess) return bad(VXR_ECUDA);
@@ -1173,6 +1337,7 @@ void vxr_box_destroy(vxr_box_world* w) {
     if (w->host_totals) cudaFreeHost(w->host_totals);
     if (w->ev0) cudaEventDestroy(w->ev0);
     if (w->ev1) cudaEventDestroy(w->ev1);
+    for (cudaEvent_t e : w->events) cudaEventDestroy(e);
     if (w->stream) cudaStreamDestroy(w->stream);
     delete w;
 }
@@ -1267,6 +1432,14 @@ int32_t vxr_box_sync(vxr_box_world* w, vxr_box_report* report) {
     VXR_CUDA(cudaMemcpyAsync(w->host_totals, w->totals, sizeof(Totals), cudaMemcpyDeviceToHost, w->stream));
     VXR_CUDA(cudaMemsetAsync(w->totals, 0, sizeof(Totals), w->stream));
     VXR_CUDA(cudaStreamSynchronize(w->stream));
+    for (int e = 0; e + 4 < w->events_used; e += 5) {
+        for (int k = 0; k < 4; k++) {
+            float ms = 0.0f;
+            VXR_CUDA(cudaEventElapsedTime(&ms, w->events[e + k], w->events[e + k + 1]));
+            w->phase_ms[k] += ms;
+        }
+    }
+    w->events_used = 0;
     const Totals& t = *w->host_totals;
     if (report) {
         report->touching = t.last[0];
@@ -1321,56 +1494,54 @@ int32_t vxr_box_touching(vxr_box_world* w, int32_t* first, int32_t* second, int3
     if (!w) return -VXR_EINVAL;
     if (!w->has_grid) return 0;
     VXR_CUDA(cudaStreamSynchronize(w->stream));
-    const PairBuffers& p = w->gen[w->cur ^ 1];  // the last step's
+    const PairGen& g = w->gen[w->cur ^ 1];  // the last step's
     int P = 0;
-    VXR_CUDA(cudaMemcpy(&P, p.tstart + w->n, sizeof(int), cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(&P, g.tstart + w->n, sizeof(int), cudaMemcpyDeviceToHost));
     if (!first && !second && !points && !manifold && !impulses) return P;
     if (P > capacity) return -VXR_ECAPACITY;
-    std::vector<int> ta(P), tb(P), tc(P);
-    VXR_CUDA(cudaMemcpy(ta.data(), p.ta, sizeof(int) * P, cudaMemcpyDeviceToHost));
-    VXR_CUDA(cudaMemcpy(tb.data(), p.tb, sizeof(int) * P, cudaMemcpyDeviceToHost));
-    VXR_CUDA(cudaMemcpy(tc.data(), p.tcand, sizeof(int) * P, cudaMemcpyDeviceToHost));
-    std::vector<float4> head(1), pa(MOST_POINTS), pb(MOST_POINTS), imp((size_t)P * MOST_POINTS),
-        impr((size_t)P * MOST_POINTS);
-    if (impulses && P) {
-        VXR_CUDA(cudaMemcpy(imp.data(), p.imp, sizeof(float4) * P * MOST_POINTS, cudaMemcpyDeviceToHost));
-        VXR_CUDA(cudaMemcpy(impr.data(), p.impr, sizeof(float4) * P * MOST_POINTS, cudaMemcpyDeviceToHost));
-    }
+    if (P == 0) return 0;
+    std::vector<int> pos(P);
+    std::vector<int4> pair(P);
+    std::vector<float4> normal(P), pa((size_t)P * MOST_POINTS), pb((size_t)P * MOST_POINTS),
+        imp((size_t)P * MOST_POINTS), impr((size_t)P * MOST_POINTS);
+    VXR_CUDA(cudaMemcpy(pos.data(), g.pos, sizeof(int) * P, cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(pair.data(), g.pair, sizeof(int4) * P, cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(normal.data(), g.normal, sizeof(float4) * P, cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(pa.data(), g.pa, sizeof(float4) * pa.size(), cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(pb.data(), g.pb, sizeof(float4) * pb.size(), cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(imp.data(), g.imp, sizeof(float4) * imp.size(), cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(impr.data(), g.impr, sizeof(float4) * impr.size(), cudaMemcpyDeviceToHost));
     for (int t = 0; t < P; t++) {
-        if (first) first[t] = ta[t];
-        if (second) second[t] = tb[t];
-        float ax = 0.0f;
-        VXR_CUDA(cudaMemcpy(head.data(), p.head + tc[t], sizeof(float4), cudaMemcpyDeviceToHost));
-        const int cnt = (int)head[0].w;
+        const int p = pos[t];
+        const int cnt = pair[p].z;
+        if (first) first[t] = pair[p].x;
+        if (second) second[t] = pair[p].y;
         if (points) points[t] = cnt;
         if (manifold) {
-            VXR_CUDA(cudaMemcpy(&ax, p.axis + tc[t], sizeof(float), cudaMemcpyDeviceToHost));
-            VXR_CUDA(cudaMemcpy(pa.data(), p.pa + (size_t)tc[t] * MOST_POINTS, sizeof(float4) * MOST_POINTS,
-                                cudaMemcpyDeviceToHost));
-            VXR_CUDA(cudaMemcpy(pb.data(), p.pb + (size_t)tc[t] * MOST_POINTS, sizeof(float4) * MOST_POINTS,
-                                cudaMemcpyDeviceToHost));
             float* m = manifold + (size_t)t * MANIFOLD_WORDS;
             std::memset(m, 0, sizeof(float) * MANIFOLD_WORDS);
-            m[0] = head[0].x;
-            m[1] = head[0].y;
-            m[2] = head[0].z;
-            m[3] = head[0].w;
-            m[4] = ax;
+            m[0] = normal[p].x;
+            m[1] = normal[p].y;
+            m[2] = normal[p].z;
+            m[3] = (float)cnt;
+            m[4] = normal[p].w;
             for (int i = 0; i < cnt && i < MOST_POINTS; i++) {
                 float* q = m + M_POINTS + i * M_POINT_WORDS;
-                q[0] = pa[i].x;
-                q[1] = pa[i].y;
-                q[2] = pa[i].z;
-                q[3] = pb[i].x;
-                q[4] = pb[i].y;
-                q[5] = pb[i].z;
-                q[6] = pa[i].w;
+                const float4 a = pa[(size_t)p * MOST_POINTS + i], b = pb[(size_t)p * MOST_POINTS + i];
+                q[0] = a.x;
+                q[1] = a.y;
+                q[2] = a.z;
+                q[3] = b.x;
+                q[4] = b.y;
+                q[5] = b.z;
+                q[6] = a.w;
             }
         }
         if (impulses) {
             float* r = impulses + (size_t)t * 28;
-            for (int i = 0; i < MOST_POINTS; i++) {
-                const float4 a = imp[(size_t)t * MOST_POINTS + i], b = impr[(size_t)t * MOST_POINTS + i];
+            std::memset(r, 0, sizeof(float) * 28);
+            for (int i = 0; i < cnt && i < MOST_POINTS; i++) {
+                const float4 a = imp[(size_t)p * MOST_POINTS + i], b = impr[(size_t)p * MOST_POINTS + i];
                 r[7 * i + 0] = a.x;
                 r[7 * i + 1] = a.y;
                 r[7 * i + 2] = a.z;
@@ -1382,6 +1553,24 @@ int32_t vxr_box_touching(vxr_box_world* w, int32_t* first, int32_t* second, int3
         }
     }
     return P;
+}
+
+int32_t vxr_box_trace(vxr_box_world* w, int32_t enable, int64_t* out, int32_t capacity) {
+    if (!w) return -VXR_EINVAL;
+    int len = 0;
+    if (out && w->trace) {
+        Counters c;
+        VXR_CUDA(cudaStreamSynchronize(w->stream));
+        VXR_CUDA(cudaMemcpy(&c, w->counters, sizeof(Counters), cudaMemcpyDeviceToHost));
+        len = std::min(c.trace_len, std::min(capacity, w->trace_cap));
+        if (len > 0) VXR_CUDA(cudaMemcpy(out, w->trace, sizeof(int64_t) * len, cudaMemcpyDeviceToHost));
+    }
+    if (enable && !w->trace) {
+        w->trace_cap = 1 << 16;
+        if (alloc(w, &w->trace, w->trace_cap)) return -VXR_ECUDA;
+    }
+    w->tracing = enable ? 1 : 0;
+    return len;
 }
 
 int32_t vxr_box_candidates(vxr_box_world* w, int32_t* pairs, int32_t capacity) {
@@ -1436,6 +1625,37 @@ int32_t vxr_box_colour_waves(vxr_box_world* w) {
     Counters c;
     if (cudaMemcpy(&c, w->counters, sizeof(Counters), cudaMemcpyDeviceToHost) != cudaSuccess) return -VXR_ECUDA;
     return c.colour_waves;
+}
+
+long long vxr_box_launches(vxr_box_world* w) { return w ? w->launches : -1; }
+
+int32_t vxr_box_profile(vxr_box_world* w, int32_t enable, double* phase_ms4) {
+    if (!w) return VXR_EINVAL;
+    if (phase_ms4)
+        for (int k = 0; k < 4; k++) phase_ms4[k] = w->phase_ms[k];
+    for (int k = 0; k < 4; k++) w->phase_ms[k] = 0.0;
+    w->profile = enable ? 1 : 0;
+    return VXR_OK;
+}
+
+int32_t vxr_box_activity(vxr_box_world* w, int64_t* out4) {
+    if (!w || !out4) return VXR_EINVAL;
+    if (!w->activity) {
+        if (alloc(w, &w->activity, 2)) return VXR_ECUDA;
+    }
+    VXR_CUDA(cudaMemsetAsync(w->activity, 0, 2 * sizeof(long long), w->stream));
+    k_activity<<<blocks_for(w->n, THREADS), THREADS, 0, w->stream>>>(w->n, w->has_grid ? w->inc_count : nullptr,
+                                                                      w->wmask, w->activity);
+    long long host[2];
+    VXR_CUDA(cudaMemcpyAsync(host, w->activity, sizeof(host), cudaMemcpyDeviceToHost, w->stream));
+    Counters c;
+    VXR_CUDA(cudaMemcpyAsync(&c, w->counters, sizeof(Counters), cudaMemcpyDeviceToHost, w->stream));
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    out4[0] = c.touching;
+    out4[1] = c.points;
+    out4[2] = host[0];
+    out4[3] = host[1];
+    return VXR_OK;
 }
 
 // The narrow phase alone over a caller's pairs (BoxContact.collide :136-246): host buffers in and out.

@@ -1,9 +1,10 @@
 // A grid-wide barrier for a cooperative (all blocks co-resident) launch, with a bounded wait.
 //
-// Arrival is an atomic add on a counter; the last block to arrive resets it and bumps a generation word the
-// others poll. Every wait gives up after a time limit (the device's global nanosecond timer): the waiter then
-// raises the abort word and the status word, and every block leaves at its next barrier, so a barrier that can
-// never complete ends the kernel with an error the host reads, not a hung GPU.
+// Arrival is one atomic add per block on a counter that only grows during the kernel (zeroed before the
+// launch): barrier number e is passed once the counter reaches (e + 1) x blocks, so no block resets anything
+// and no second word is needed. Every wait gives up after a time limit (the device's global nanosecond timer):
+// the waiter then raises the abort word and the status word, and every block leaves at its next barrier, so a
+// barrier that can never complete ends the kernel with an error the host reads, not a hung GPU.
 #pragma once
 #include <cstdint>
 
@@ -12,8 +13,8 @@ namespace vxr {
 enum : int { ST_OK = 0, ST_CAPACITY = 2, ST_ROUNDS = 3, ST_NONFINITE = 4, ST_TIMEOUT = 5 };
 
 struct GridBarrier {
-    unsigned int* count;       // arrivals this generation
-    unsigned int* generation;  // bumped once per completed barrier
+    unsigned int* count;       // arrivals since the launch
+    unsigned int* generation;  // unused by this barrier; kept zero
     int* abort;                // nonzero: every block leaves
     int* status;               // the step's status word
     unsigned long long limit_ns;
@@ -25,36 +26,38 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// Returns false when the kernel must stop (a wait ran out here or elsewhere).
-__device__ __forceinline__ bool grid_sync(const GridBarrier& b) {
+__device__ __forceinline__ unsigned int load_acquire(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Returns false when the kernel must stop (a wait ran out here or elsewhere). `epoch` counts this block's
+// barriers since the launch; every block passes the same barriers in the same order.
+__device__ __forceinline__ bool grid_sync(const GridBarrier& b, unsigned int& epoch) {
     __syncthreads();
     __shared__ int leave;
     if (threadIdx.x == 0) {
         leave = 0;
-        volatile unsigned int* gen = b.generation;
-        const unsigned int g = *gen;
+        const unsigned int target = (epoch + 1) * gridDim.x;
         __threadfence();
-        const unsigned int arrived = atomicAdd(b.count, 1u);
-        if (arrived == gridDim.x - 1) {
-            *b.count = 0u;
-            __threadfence();
-            atomicAdd(b.generation, 1u);
-        } else {
+        atomicAdd(b.count, 1u);
+        if (load_acquire(b.count) < target) {
             const unsigned long long start = global_ns();
             unsigned int spins = 0;
-            while (*gen == g) {
+            while (load_acquire(b.count) < target) {
                 if (*(volatile int*)b.abort) break;
-                if ((++spins & 63u) == 0u && global_ns() - start > b.limit_ns) {
+                if ((++spins & 255u) == 0u && global_ns() - start > b.limit_ns) {
                     atomicExch(b.abort, 1);
                     atomicCAS(b.status, ST_OK, ST_TIMEOUT);
                     break;
                 }
-                __nanosleep(32);
             }
         }
         __threadfence();
         if (*(volatile int*)b.abort) leave = 1;
     }
+    epoch++;
     __syncthreads();
     return leave == 0;
 }

@@ -20,7 +20,8 @@ STATUS_NAMES = {0: "VXR_OK", 1: "VXR_EINVAL", 2: "VXR_ECAPACITY", 3: "VXR_EROUND
 SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_create", "vxr_box_destroy",
            "vxr_box_error", "vxr_box_start", "vxr_box_load_state", "vxr_box_params", "vxr_box_step",
            "vxr_box_step_async", "vxr_box_sync", "vxr_box_stream", "vxr_box_state", "vxr_box_read_shown",
-           "vxr_box_touching", "vxr_box_candidates", "vxr_box_walls", "vxr_box_colour_waves", "vxr_collide"]
+           "vxr_box_touching", "vxr_box_candidates", "vxr_box_walls", "vxr_box_colour_waves", "vxr_collide",
+           "vxr_box_launches", "vxr_box_profile", "vxr_box_activity", "vxr_box_trace"]
 
 
 class VxrError(RuntimeError):
@@ -93,6 +94,14 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_walls.restype = i32
         L.vxr_box_colour_waves.argtypes = [vp]
         L.vxr_box_colour_waves.restype = i32
+        L.vxr_box_launches.argtypes = [vp]
+        L.vxr_box_launches.restype = ctypes.c_longlong
+        L.vxr_box_profile.argtypes = [vp, i32, vp]
+        L.vxr_box_profile.restype = i32
+        L.vxr_box_activity.argtypes = [vp, vp]
+        L.vxr_box_activity.restype = i32
+        L.vxr_box_trace.argtypes = [vp, i32, vp, i32]
+        L.vxr_box_trace.restype = i32
         L.vxr_collide.argtypes = [i32, vp, vp, i32, vp, vp]
         L.vxr_collide.restype = i32
         _ = f32

@@ -195,6 +195,32 @@ class BoxSimulation:
     def colour_waves(self) -> int:
         return self.L.vxr_box_colour_waves(self.h)
 
+    def launches(self) -> int:
+        return int(self.L.vxr_box_launches(self.h))
+
+    def profile(self, enable: bool) -> np.ndarray:
+        """Turns per-phase timing on or off; returns the milliseconds summed since the last call
+        (broad phase, narrow phase with carry, colouring, solve)."""
+        out = np.zeros(4, np.float64)
+        self._check(self.L.vxr_box_profile(self.h, int(bool(enable)), ptr(out)))
+        return out
+
+    def activity(self) -> dict:
+        out = np.zeros(4, np.int64)
+        self._check(self.L.vxr_box_activity(self.h, ptr(out)))
+        return {"touching": int(out[0]), "points": int(out[1]), "bodies_active": int(out[2]),
+                "wall_records": int(out[3])}
+
+    def trace(self, enable: bool = True) -> np.ndarray:
+        """Turns the solve's phase trace on or off; returns the last traced step's entries as (code, ns) rows."""
+        out = np.zeros(1 << 16, np.int64)
+        n = self.L.vxr_box_trace(self.h, int(bool(enable)), ptr(out), len(out))
+        if n < 0:
+            raise VxrError(-n, self.error())
+        raw = out[:n].astype(np.uint64)
+        return np.stack([(raw >> np.uint64(48)).astype(np.int64),
+                         (raw & np.uint64((1 << 48) - 1)).astype(np.int64)], axis=1)
+
     def error(self) -> str:
         return self.L.vxr_box_error(self.h).decode() if self.h else ""
 

@@ -1,0 +1,86 @@
+"""Seeded synthetic scenes of the shapes the benchmark configurations name.
+
+No public dataset is involved: each scene is drawn from numpy's PCG64 with a fixed seed, with the sizes and
+distributions of its configuration. A scene is a dict of f32 arrays (x y z u v w lx ly lz qx qy qz qw im hx hy
+hz shape) plus the walled box, step shape and parameters, ready for BoxSimulation.start_momentum (or the
+oracle's world).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import boxes as B
+
+FIELDS = ["x", "y", "z", "u", "v", "w", "lx", "ly", "lz", "qx", "qy", "qz", "qw", "im", "hx", "hy", "hz", "shape"]
+
+
+def _random_quaternions(rng, n):
+    """Uniformly random unit quaternions (Shoemake's method)."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    a, b = np.sqrt(1 - u1), np.sqrt(u1)
+    return np.stack([a * np.sin(2 * np.pi * u2), a * np.cos(2 * np.pi * u2), b * np.sin(2 * np.pi * u3),
+                     b * np.cos(2 * np.pi * u3)])
+
+
+def large_mixed(bodies: int = 262_144, seed: int = 1, volume=(128.0, 64.0, 128.0), sphere_share: float = 0.8,
+                mu: float = 0.5, mu_rolling: float = 0.1, margin: float = 0.005, dt: float = 1 / 120,
+                substeps: int = 4, sweeps: int = 10, height: float | None = None) -> dict:
+    """The large mixed scene: 80% spheres (radius log-uniform in 0.2-0.8 m), 20% boxes (half-extents uniform in
+    0.2-0.6 m, uniformly random orientations), centres uniform in a 128 x 64 x 128 m volume above the floor,
+    velocities N(0, 1 m/s) per axis, densities uniform in 500-2000 kg/m^3; dt 1/120 s, 4 substeps, 10 sweeps.
+
+    The walls are the reference's walled box [0, sx] x [0, sy] x [0, sz] (core/box/Boxes.java:89-90): the volume's
+    footprint, and a ceiling twice the volume's height. Friction and rolling resistance are not fixed by the
+    configuration; mu 0.5 and mu_r 0.1 are used (the reference's own tests use 0.5 and 0.1-0.3).
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n = bodies
+    vx, vy, vz = volume
+    sphere = rng.random(n) < sphere_share
+    radius = np.exp(rng.uniform(math.log(0.2), math.log(0.8), n))
+    halves = rng.uniform(0.2, 0.6, (3, n))
+    half = np.where(sphere, radius, halves)
+    q = _random_quaternions(rng, n)
+    q[:, sphere] = np.array([0.0, 0.0, 0.0, 1.0])[:, None]
+    edge = 1.05  # no body starts in a wall: the widest reaches 1.04 m from its centre
+    x = rng.uniform(edge, vx - edge, n)
+    y = rng.uniform(edge, vy + edge, n)
+    z = rng.uniform(edge, vz - edge, n)
+    vel = rng.normal(0.0, 1.0, (3, n))
+    density = rng.uniform(500.0, 2000.0, n)
+    volume_of = np.where(sphere, 4.0 / 3.0 * np.pi * radius ** 3, 8.0 * halves[0] * halves[1] * halves[2])
+    im = 1.0 / (density * volume_of)
+    f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)  # noqa: E731
+    scene = {
+        "x": f32(x), "y": f32(y), "z": f32(z), "u": f32(vel[0]), "v": f32(vel[1]), "w": f32(vel[2]),
+        "lx": np.zeros(n, np.float32), "ly": np.zeros(n, np.float32), "lz": np.zeros(n, np.float32),
+        "qx": f32(q[0]), "qy": f32(q[1]), "qz": f32(q[2]), "qw": f32(q[3]), "im": f32(im),
+        "hx": f32(half[0]), "hy": f32(half[1]), "hz": f32(half[2]),
+        "shape": np.where(sphere, B.SPHERE_SHAPE, B.BOX_SHAPE).astype(np.float32),
+    }
+    sy = height if height is not None else 2 * vy
+    h3 = np.stack([scene["hx"], scene["hy"], scene["hz"]])
+    # the widest bounding sphere (BoxBroad.grid's rule): a box's half-diagonal, a sphere's radius
+    boxes_only = h3[:, ~sphere] if (~sphere).any() else np.zeros((3, 1), np.float32)
+    widest = max(B.widest_half_diagonal(boxes_only), float(np.max(scene["hx"][sphere])) if sphere.any() else 0.0)
+    scene.update({
+        "bodies": n, "walls": (vx, sy, vz), "dt": dt, "substeps": substeps, "sweeps": sweeps, "margin": margin,
+        "mu": mu, "mu_rolling": mu_rolling, "widest": widest,
+        "grid": B.grid(vx, sy, vz, widest, margin),
+        "params": B.params(dt / substeps, 0.0, -9.81, 0.0, vx, sy, vz, mu, mu, margin, mu_rolling),
+        "name": f"large mixed scene, {n} bodies ({sphere_share:.0%} spheres), seed {seed}",
+    })
+    return scene
+
+
+def sub_volume(bodies_full: int, fraction: float, seed: int = 1) -> dict:
+    """The large mixed scene's distribution over a fraction of its volume (same body density): a bounded
+    sample for a CPU baseline. The footprint shrinks, the height stays."""
+    side = math.sqrt(fraction)
+    return large_mixed(int(round(bodies_full * fraction)), seed=seed, volume=(128.0 * side, 64.0, 128.0 * side))
+
+
+def fields(scene: dict) -> list:
+    return [scene[k] for k in FIELDS]
