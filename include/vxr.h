@@ -58,6 +58,9 @@ typedef struct {
                             than the reference's rule (core/box/BoxBroad.java:66-68) need 2 or more. */
     int32_t max_pairs;   /* candidate/touching pair capacity; 0 = bodies * 32, the reference's slot count */
     int32_t device;      /* CUDA device ordinal */
+    int32_t schedule;    /* 0: a grid-wide barrier after every round (default); 1: dependency-driven, each pair or
+                            wall item waiting only for its own bodies. Both keep the reference's per-body order of
+                            operations and give the same results. */
 } vxr_box_config;
 
 /* What a step took: core/box/BoxStepper.java:308-311 (Report), plus the totals over a vxr_box_step call. */

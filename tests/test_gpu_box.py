@@ -118,13 +118,31 @@ def test_gpu_mixed_pile_steps_match_the_oracle_bit_for_bit():
     np.testing.assert_array_equal(ob, a.world.buffer("roll"))
 
 
-def test_gpu_symmetric_sweeps_match_the_oracle():
+@pytest.mark.parametrize("schedule", [0, 1], ids=["barrier", "dependency"])
+def test_gpu_symmetric_sweeps_match_the_oracle(schedule):
     def make():
         s = C.mixed_pile_scene()
         s.symmetric = True
         s.passes = 3
         return s
-    a, b = run_both(make, 20)
+    a, b = run_both(make, 20, schedule=schedule)
+    compare_worlds(a, b)
+
+
+def test_gpu_dependency_schedule_matches_the_oracle():
+    a, b = run_both(lambda: C.pile_scene(7), 30, schedule=1)
+    compare_worlds(a, b)
+
+
+def test_gpu_fixed_bodies_and_spheres_match_the_oracle():
+    """A mixed pile on four fixed balls and a fixed slab: fixed bodies take part in pairs (their angular
+    momentum is written, as the reference writes it) and stiffen their contacts."""
+    def make():
+        s = C.mixed_pile_scene()
+        for k in range(0, 8):
+            s.im[k] = 0.0
+        return s
+    a, b = run_both(make, 30)
     compare_worlds(a, b)
 
 

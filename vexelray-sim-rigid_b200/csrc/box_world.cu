@@ -40,6 +40,10 @@ constexpr int WALL_RECORDS = 48;
 constexpr int SHOWN_STRIDE = 20;
 constexpr int THREADS = 256;
 constexpr int SOLVE_THREADS = 256;
+// Within a round, pairs are grouped by kind so a warp's lanes take the same path: two spheres, a sphere and a box,
+// then two boxes by point count (1 to 4).
+constexpr int PAIR_KINDS = 6;
+constexpr int BUCKETS = (MOST_ROUNDS + 1) * PAIR_KINDS;
 
 // ------------------------------------------------------------------------------------------------------------
 // Device buffers of a world.
@@ -130,11 +134,16 @@ struct vxr_box_world {
     PairGen gen[2]{};
     int cur = 0;  // gen[cur] is this step's, gen[cur ^ 1] the step before's
     int* wall_list = nullptr;    // [n] bodies near a wall or holding a wall impulse, rebuilt twice a substep
-    int* wall_count = nullptr;   // [2 * substeps] their counts
+    int* wall_count = nullptr;   // [4 * substeps] their counts (spheres, boxes)
+    int* version = nullptr;      // [n] items each body has done in the current block of sweeps
+    int* listed = nullptr;       // [n] on the current wall list
+    unsigned* body_colours = nullptr;  // [n] rounds each body has a pair in
+    int schedule = 0;
     unsigned long long* trace = nullptr;  // phase end times of the last traced step
     int trace_cap = 0, tracing = 0;
     int *colour = nullptr, *inc_count = nullptr, *inc_start = nullptr, *inc_fill = nullptr, *inc_list = nullptr;
-    int *round_count = nullptr, *round_start = nullptr, *round_fill = nullptr;
+    int *round_count = nullptr, *round_start = nullptr, *round_fill = nullptr;  // by (round, kind) bucket
+    int* bucket_start = nullptr;
     Counters* counters = nullptr;
     Totals* totals = nullptr;
     Totals* host_totals = nullptr;  // pinned
@@ -507,8 +516,18 @@ __global__ void __launch_bounds__(THREADS) k_colour(const int* __restrict__ touc
     }
 }
 
+__device__ __forceinline__ int pair_kind(float shapeA, float shapeB, int count) {
+    const bool sa = shapeA > 0.5f, sb = shapeB > 0.5f;
+    if (sa && sb) return 0;
+    if (sa || sb) return 1;
+    return 1 + min(max(count, 1), 4);
+}
+
 __global__ void k_round_count(const int* __restrict__ touching_n, const int* __restrict__ colour,
-                              int* __restrict__ round_count, Counters* counters) {
+                              int* __restrict__ round_count, Counters* counters, const int* __restrict__ ta,
+                              const int* __restrict__ tb, unsigned* __restrict__ body_colours,
+                              const int* __restrict__ tcand, const float4* __restrict__ head,
+                              const float4* __restrict__ half) {
     const int total = *touching_n;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         int c = colour[t];
@@ -516,9 +535,15 @@ __global__ void k_round_count(const int* __restrict__ touching_n, const int* __r
             atomicCAS(&counters->status, ST_OK, ST_ROUNDS);
             c = MOST_ROUNDS;
         }
-        atomicAdd(&round_count[c], 1);
-        if (c < MOST_ROUNDS) atomicMax(&counters->rounds, c + 1);
-        else atomicAdd(&counters->unplaced, 1);
+        const int kind = pair_kind(half[ta[t]].w, half[tb[t]].w, (int)head[tcand[t]].w);
+        atomicAdd(&round_count[c * PAIR_KINDS + kind], 1);
+        if (c < MOST_ROUNDS) {
+            atomicMax(&counters->rounds, c + 1);
+            atomicOr(&body_colours[ta[t]], 1u << c);
+            atomicOr(&body_colours[tb[t]], 1u << c);
+        } else {
+            atomicAdd(&counters->unplaced, 1);
+        }
     }
 }
 
@@ -526,19 +551,28 @@ __global__ void k_round_count(const int* __restrict__ touching_n, const int* __r
 // carried impulses next to it, so a solve phase reads one contiguous record per pair. Within a round the order is
 // the atomic fill's: the pairs of a round share no body, so their order does not change any result.
 __global__ void k_order(const int* __restrict__ touching_n, const int* __restrict__ colour,
-                        const int* __restrict__ round_start, int* __restrict__ round_fill, const int* __restrict__ ta,
+                        const int* __restrict__ bucket_start, int* __restrict__ round_fill, const int* __restrict__ ta,
                         const int* __restrict__ tcand, const Manifolds m, const float4* __restrict__ imp_t,
-                        const float4* __restrict__ impr_t, PairGen now) {
+                        const float4* __restrict__ impr_t, PairGen now,
+                        const unsigned* __restrict__ body_colours, const float4* __restrict__ half) {
     const int total = *touching_n;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         int c = colour[t];
         if (c < 0 || c > MOST_ROUNDS) c = MOST_ROUNDS;
-        const int p = round_start[c] + atomicAdd(&round_fill[c], 1);
+        const int kind = pair_kind(half[ta[t]].w, half[now.tb[t]].w, (int)m.head[tcand[t]].w);
+        const int bucket = c * PAIR_KINDS + kind;
+        const int p = bucket_start[bucket] + atomicAdd(&round_fill[bucket], 1);
         now.pos[t] = p;
         const int cd = tcand[t];
         const float4 head = m.head[cd];
         const int count = (int)head.w;
-        now.pair[p] = make_int4(ta[t], now.tb[t], count, t);
+        // For the dependency schedule: each body's rank of this pair among its rounds, and its pair count.
+        const int a = ta[t], b = now.tb[t];
+        const unsigned ma = body_colours[a], mb = body_colours[b];
+        const unsigned below = c < MOST_ROUNDS ? (1u << c) - 1u : 0xffffffffu;
+        const unsigned packed = (unsigned)__popc(ma & below) | (unsigned)__popc(mb & below) << 8 |
+                                (unsigned)__popc(ma) << 16 | (unsigned)__popc(mb) << 24;
+        now.pair[p] = make_int4(a, b, count, (int)packed);
         now.normal[p] = make_float4(head.x, head.y, head.z, m.axis[cd]);
         for (int i = 0; i < count; i++) {
             now.pa[(long)p * MOST_POINTS + i] = m.pa[(long)cd * MOST_POINTS + i];
@@ -547,6 +581,12 @@ __global__ void k_order(const int* __restrict__ touching_n, const int* __restric
             now.impr[(long)p * MOST_POINTS + i] = impr_t[(long)t * MOST_POINTS + i];
         }
     }
+}
+
+// Where each round begins: its first bucket's start.
+__global__ void k_round_starts(const int* __restrict__ bucket_start, int* __restrict__ round_start) {
+    const int r = threadIdx.x;  // bucket_start has BUCKETS + 1 entries: r * PAIR_KINDS <= BUCKETS for r <= 33
+    if (r <= MOST_ROUNDS + 1) round_start[r] = bucket_start[r * PAIR_KINDS];
 }
 
 // ------------------------------------------------------------------------------------------------------------
@@ -559,10 +599,14 @@ struct SolveArgs {
     float4* wroll;
     unsigned long long* wmask;
     int* wall_list;   // bodies that may touch a wall until positions next change, rebuilt twice a substep
-    int* wall_count;  // [2 * substeps] their counts
+    int* wall_count;  // [4 * substeps] their counts: spheres, boxes for each half-substep
     PairGen pairs;
     const int* round_start;
     Counters* counters;
+    int* version;                  // [n] items of each body done in this block of sweeps (dependency schedule)
+    int* listed;                   // [n] 1 where the body is on this half-substep's wall list
+    const unsigned* body_colours;  // [n] the rounds of each body's pairs, one bit each
+    int schedule;                  // 0: a grid barrier after every round; 1: dependency-driven
     int substeps, sweeps, symmetric;
     Params params;
     GridBarrier bar;
@@ -570,12 +614,14 @@ struct SolveArgs {
     int trace_cap;
 };
 
+// Body state a solve phase reads and writes goes through L2 (ld/st .cg): under the dependency schedule one
+// body's consecutive items can run on different SMs.
 __device__ __forceinline__ void load_held(Held& h, const Bodies& b, int s) {
-    h.load(b.pose[s], b.turn[s], __ldg(&b.half[s]), b.vel[s], b.mom[s]);
+    h.load(__ldcg(&b.pose[s]), __ldcg(&b.turn[s]), __ldg(&b.half[s]), __ldcg(&b.vel[s]), __ldcg(&b.mom[s]));
 }
 __device__ __forceinline__ void store_held(const Held& h, const Bodies& b, int s) {
-    b.vel[s] = make_float4(h.velocity[0], h.velocity[1], h.velocity[2], 0.0f);
-    b.mom[s] = make_float4(h.momentum[0], h.momentum[1], h.momentum[2], 0.0f);
+    __stcg(&b.vel[s], make_float4(h.velocity[0], h.velocity[1], h.velocity[2], 0.0f));
+    __stcg(&b.mom[s], make_float4(h.momentum[0], h.momentum[1], h.momentum[2], 0.0f));
 }
 
 __device__ __forceinline__ void list_wall_body(const SolveArgs& A, int s, float4 pose, int slot);
@@ -583,19 +629,22 @@ __device__ __forceinline__ void list_wall_body(const SolveArgs& A, int s, float4
 // Boxes.positions :299-342, and the body listed for the relax sweeps' walls from where it now is.
 __device__ __forceinline__ void phase_positions(const SolveArgs& A, int slot) {
     const int stride = gridDim.x * blockDim.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) A.counters->bar_gen = 0u;  // the dependency schedule's ticket
     const float h = A.params.w[P_H];
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += stride) {
-        float4 p = A.b.pose[s];
+        float4 p = __ldcg(&A.b.pose[s]);
         const float im = p.w;
+        A.version[s] = 0;
+        A.listed[s] = 0;
         if (!(im > 0.0f)) continue;
-        const float4 v = A.b.vel[s];
+        const float4 v = __ldcg(&A.b.vel[s]);
         p.x = p.x + h * v.x;
         p.y = p.y + h * v.y;
         p.z = p.z + h * v.z;
-        A.b.pose[s] = p;
-        const float4 tq = A.b.turn[s];
+        __stcg(&A.b.pose[s], p);
+        const float4 tq = __ldcg(&A.b.turn[s]);
         const float q[4] = {tq.x, tq.y, tq.z, tq.w};
-        const float4 l = A.b.mom[s];
+        const float4 l = __ldcg(&A.b.mom[s]);
         const float momentum[3] = {l.x, l.y, l.z};
         float inverse[3];
         inverse_inertia(__ldg(&A.b.half[s]), im, inverse);
@@ -617,7 +666,7 @@ __device__ __forceinline__ void phase_positions(const SolveArgs& A, int slot) {
             rotateq(mid, scaled, omega_mid);
         }
         turned(q, omega_mid, h, end);
-        A.b.turn[s] = make_float4(end[0], end[1], end[2], end[3]);
+        __stcg(&A.b.turn[s], make_float4(end[0], end[1], end[2], end[3]));
         list_wall_body(A, s, p, slot);
     }
 }
@@ -645,21 +694,29 @@ __device__ __forceinline__ unsigned near_walls(float4 pose, float4 hw, const Par
 // The bodies the walls' sweeps must visit until positions next change: near a wall, or holding a wall impulse.
 // The order of the list does not matter: each body's walls touch that body alone.
 __device__ __forceinline__ void list_wall_body(const SolveArgs& A, int s, float4 pose, int slot) {
-    if (A.wmask[s] != 0ull || near_walls(pose, __ldg(&A.b.half[s]), A.params) != 0u)
-        A.wall_list[atomicAdd(&A.wall_count[slot], 1)] = s;
+    const float4 hw = __ldg(&A.b.half[s]);
+    const bool list = __ldcg(&A.wmask[s]) != 0ull || near_walls(pose, hw, A.params) != 0u;
+    if (list) {  // spheres from the front of the list, boxes from the back: a warp's bodies take the same path
+        if (hw.w > 0.5f) A.wall_list[atomicAdd(&A.wall_count[2 * slot], 1)] = s;
+        else A.wall_list[A.n - 1 - atomicAdd(&A.wall_count[2 * slot + 1], 1)] = s;
+    }
+    A.listed[s] = list ? 1 : 0;
 }
 
 __device__ __forceinline__ void phase_velocities_and_list(const SolveArgs& A, int slot) {
     const int stride = gridDim.x * blockDim.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) A.counters->bar_gen = 0u;  // the dependency schedule's ticket
     const float h = A.params.w[P_H];
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += stride) {
         const float4 pose = A.b.pose[s];
+        A.version[s] = 0;
+        A.listed[s] = 0;
         if (!(pose.w > 0.0f)) continue;
-        float4 v = A.b.vel[s];
+        float4 v = __ldcg(&A.b.vel[s]);
         v.x = v.x + h * A.params.w[P_GX];
         v.y = v.y + h * A.params.w[P_GY];
         v.z = v.z + h * A.params.w[P_GZ];
-        A.b.vel[s] = v;
+        __stcg(&A.b.vel[s], v);
         list_wall_body(A, s, pose, slot);
     }
 }
@@ -671,7 +728,7 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
     const Params& P = A.params;
     const float margin = P.w[P_MARGIN];
     const float extent[3] = {P.w[P_SX], P.w[P_SY], P.w[P_SZ]};
-    unsigned long long mask = A.wmask[s];
+    unsigned long long mask = __ldcg(&A.wmask[s]);
     const float4 pose = make_float4(box.at[0], box.at[1], box.at[2], box.im);
     const float4 hw = make_float4(box.half[0], box.half[1], box.half[2], box.shape);
     const bool sphere = hw.w > 0.5f;
@@ -704,19 +761,19 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
             float4 rec = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             const long at = (long)s * WALL_RECORDS + wall * 8;
             if (need) {
-                rec = held ? A.wall[at] : rec;
+                rec = held ? __ldcg(&A.wall[at]) : rec;
                 contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft);
                 if (sweep != WARM) {
-                    A.wall[at] = rec;
+                    __stcg(&A.wall[at], rec);
                     mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
                 }
                 touched = true;
             }
             if (rolled || (sweep != WARM && nonzero_bits(rec))) {
-                float4 rr = rolled ? A.wroll[(long)s * 6 + wall] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                float4 rr = rolled ? __ldcg(&A.wroll[(long)s * 6 + wall]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 roll<false>(sweep, box, box, box.half[0], rec.x, rr, P.w[P_MU_ROLLING]);
                 if (sweep != WARM) {
-                    A.wroll[(long)s * 6 + wall] = rr;
+                    __stcg(&A.wroll[(long)s * 6 + wall], rr);
                     mask = nonzero_bits(rr) ? (mask | (1ull << rbit)) : (mask & ~(1ull << rbit));
                 }
                 touched = true;
@@ -737,17 +794,17 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
                 const float gap = high ? pick3(extent, axis) - reach : reach;
                 if (!(held || (sweep != WARM && gap < margin))) continue;
                 const long at = (long)s * WALL_RECORDS + bit;
-                float4 rec = held ? A.wall[at] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                float4 rec = held ? __ldcg(&A.wall[at]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft);
                 if (sweep != WARM) {
-                    A.wall[at] = rec;
+                    __stcg(&A.wall[at], rec);
                     mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
                 }
                 touched = true;
             }
         }
     }
-    if (touched) A.wmask[s] = mask;
+    if (touched) __stcg(&A.wmask[s], mask);
     return touched;
 }
 
@@ -755,72 +812,165 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
 // momentum, as the reference's walls kernel loads it).
 __device__ __forceinline__ void phase_walls(const SolveArgs& A, int sweep, bool reverse, int slot) {
     const int stride = gridDim.x * blockDim.x;
-    const int listed = *(volatile int*)&A.wall_count[slot];
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < listed; k += stride) {
-        const int s = A.wall_list[k];
+    const int spheres = *(volatile int*)&A.wall_count[2 * slot], boxes = *(volatile int*)&A.wall_count[2 * slot + 1];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < spheres + boxes; k += stride) {
+        const int s = A.wall_list[k < spheres ? k : A.n - 1 - (k - spheres)];
         Held box;
         load_held(box, A.b, s);
         if (walls_of(A, box, s, sweep, reverse)) store_held(box, A.b, s);
     }
 }
 
-// BoxPairs.solve :64-151: one round of pairs that share no body, each read as one record in round order.
+// BoxPairs.solve :64-151 for the pair at round-order position k: its whole manifold in turn, both bodies loaded
+// once and stored once.
+__device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4, int sweep, bool reverse) {
+    const Params& P = A.params;
+    const float4 head = __ldg(&A.pairs.normal[k]);
+    const int ia = rec4.x, ib = rec4.y, count = rec4.z;
+    Held first, second;
+    load_held(first, A.b, ia);
+    load_held(second, A.b, ib);
+    Soft soft(P, false);
+    if (first.im == 0.0f || second.im == 0.0f) {
+        soft.bias = P.w[P_STATIC_BIAS];
+        soft.mass_scale = P.w[P_STATIC_MASS_SCALE];
+        soft.impulse_scale = P.w[P_STATIC_IMPULSE_SCALE];
+    }
+    const float n[3] = {head.x, head.y, head.z};
+    const bool anySphere = first.sphere() || second.sphere();
+    for (int order = 0; order < MOST_POINTS; order++) {
+        const int slot = reverse ? MOST_POINTS - 1 - order : order;
+        if (!(slot < count)) continue;
+        const long at = k * MOST_POINTS + slot;
+        float rA[3], rB[3];
+        if (first.sphere()) {
+            for (int a = 0; a < 3; a++) rA[a] = first.half[0] * n[a];
+        } else {
+            const float4 qa = __ldg(&A.pairs.pa[at]);
+            const float anchorA[3] = {qa.x, qa.y, qa.z};
+            rotateq(first.q, anchorA, rA);
+        }
+        if (second.sphere()) {
+            for (int a = 0; a < 3; a++) rB[a] = -(second.half[0] * n[a]);
+        } else {
+            const float4 qb = __ldg(&A.pairs.pb[at]);
+            const float anchorB[3] = {qb.x, qb.y, qb.z};
+            rotateq(second.q, anchorB, rB);
+        }
+        float gap = ((second.at[0] + rB[0]) - (first.at[0] + rA[0])) * n[0] +
+                    ((second.at[1] + rB[1]) - (first.at[1] + rA[1])) * n[1];
+        gap = gap + ((second.at[2] + rB[2]) - (first.at[2] + rA[2])) * n[2];
+        float4 rec = __ldcg(&A.pairs.imp[at]);
+        contact<true>(sweep, gap, n, first, rA, second, rB, rec, soft);
+        if (sweep != WARM) __stcg(&A.pairs.imp[at], rec);
+        if (anySphere) {
+            float radius = second.half[0];
+            if (first.sphere()) radius = first.half[0];
+            if (first.sphere() && second.sphere())
+                radius = (first.half[0] * second.half[0]) / (first.half[0] + second.half[0]);
+            float4 rr = __ldcg(&A.pairs.impr[at]);
+            roll<true>(sweep, first, second, radius, rec.x, rr, P.w[P_MU_ROLLING]);
+            if (sweep != WARM) __stcg(&A.pairs.impr[at], rr);
+        }
+    }
+    store_held(first, A.b, ia);
+    store_held(second, A.b, ib);
+}
+
+// One round of pairs that share no body (the barrier schedule).
 __device__ __forceinline__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r) {
     const int stride = gridDim.x * blockDim.x;
-    const Params& P = A.params;
     const int lo = A.round_start[r], hi = A.round_start[r + 1];
-    for (int k = lo + blockIdx.x * blockDim.x + threadIdx.x; k < hi; k += stride) {
-        const int4 rec4 = A.pairs.pair[k];
-        const float4 head = A.pairs.normal[k];
-        const int ia = rec4.x, ib = rec4.y, count = rec4.z;
-        Held first, second;
-        load_held(first, A.b, ia);
-        load_held(second, A.b, ib);
-        Soft soft(P, false);
-        if (first.im == 0.0f || second.im == 0.0f) {
-            soft.bias = P.w[P_STATIC_BIAS];
-            soft.mass_scale = P.w[P_STATIC_MASS_SCALE];
-            soft.impulse_scale = P.w[P_STATIC_IMPULSE_SCALE];
-        }
-        const float n[3] = {head.x, head.y, head.z};
-        const bool anySphere = first.sphere() || second.sphere();
-        for (int order = 0; order < MOST_POINTS; order++) {
-            const int slot = reverse ? MOST_POINTS - 1 - order : order;
-            if (!(slot < count)) continue;
-            const long at = (long)k * MOST_POINTS + slot;
-            const float4 qa = A.pairs.pa[at];
-            const float4 qb = A.pairs.pb[at];
-            const float anchorA[3] = {qa.x, qa.y, qa.z}, anchorB[3] = {qb.x, qb.y, qb.z};
-            float rA[3], rB[3];
-            rotateq(first.q, anchorA, rA);
-            rotateq(second.q, anchorB, rB);
-            if (first.sphere())
-                for (int a = 0; a < 3; a++) rA[a] = first.half[0] * n[a];
-            if (second.sphere())
-                for (int a = 0; a < 3; a++) rB[a] = -(second.half[0] * n[a]);
-            float gap = ((second.at[0] + rB[0]) - (first.at[0] + rA[0])) * n[0] +
-                        ((second.at[1] + rB[1]) - (first.at[1] + rA[1])) * n[1];
-            gap = gap + ((second.at[2] + rB[2]) - (first.at[2] + rA[2])) * n[2];
-            float4 rec = A.pairs.imp[at];
-            contact<true>(sweep, gap, n, first, rA, second, rB, rec, soft);
-            if (sweep != WARM) A.pairs.imp[at] = rec;
-            if (anySphere) {
-                float radius = second.half[0];
-                if (first.sphere()) radius = first.half[0];
-                if (first.sphere() && second.sphere())
-                    radius = (first.half[0] * second.half[0]) / (first.half[0] + second.half[0]);
-                float4 rr = A.pairs.impr[at];
-                roll<true>(sweep, first, second, radius, rec.x, rr, P.w[P_MU_ROLLING]);
-                if (sweep != WARM) A.pairs.impr[at] = rr;
+    for (int k = lo + blockIdx.x * blockDim.x + threadIdx.x; k < hi; k += stride)
+        solve_pair(A, k, __ldg(&A.pairs.pair[k]), sweep, reverse);
+}
+
+// Waits until every listed body has done exactly `want` items of this block. A bounded wait: past the limit it
+// raises the abort and status words and returns false.
+__device__ __forceinline__ bool wait_versions(const SolveArgs& A, int a, int wantA, int b, int wantB) {
+    const volatile int* va = A.version + a;
+    const volatile int* vb = A.version + (b < 0 ? a : b);
+    if (*va == wantA && (b < 0 || *vb == wantB)) { __threadfence(); return true; }
+    const unsigned long long start = global_ns();
+    for (unsigned spins = 1;; spins++) {
+        if (spins > 64) __nanosleep(32);
+        if (*va == wantA && (b < 0 || *vb == wantB)) { __threadfence(); return true; }
+        if ((spins & 63u) == 0u) {
+            if (*(volatile int*)A.bar.abort) return false;
+            if (global_ns() - start > A.bar.limit_ns) {
+                atomicExch(A.bar.abort, 1);
+                atomicCAS(A.bar.status, ST_OK, ST_TIMEOUT);
+                return false;
             }
         }
-        store_held(first, A.b, ia);
-        store_held(second, A.b, ib);
     }
 }
 
+// A block of sweeps under the dependency schedule: every pair of every sweep, and the walls of every listed body,
+// as items in the reference's order (sweep by sweep; within a sweep the rounds, then the walls; backward, the
+// walls, then the rounds last to first). Each body counts the items it has done; an item runs once each of its
+// bodies has done exactly the items that precede it in that body's own sequence of the reference's order:
+//   per sweep a body has deg pair items (one per round it is in, in round order) and, if listed, one walls item.
+// So the per-body order of operations, and every result, is the reference's; only unrelated bodies overlap.
+// Items are handed out in increasing order, so the lowest unfinished item always has all it waits on done and a
+// running warp holding it: the schedule cannot stall while every block is resident (a cooperative launch).
+__device__ __forceinline__ bool block_of_sweeps(const SolveArgs& A, int first_kind, int sweeps, int rounds,
+                                                int slot, int sweep0) {
+    const int placed = A.round_start[rounds];
+    const int spheres = *(volatile int*)&A.wall_count[2 * slot];
+    const int walls = spheres + *(volatile int*)&A.wall_count[2 * slot + 1];
+    const long per = (long)placed + walls;
+    const long total = per * sweeps;
+    // Warps take runs of 32 items from a ticket, in increasing order (the lowest unfinished item is always held
+    // by a running warp).
+    unsigned int* ticket = &A.counters->bar_gen;  // zeroed by the phase before the block
+    for (;;) {
+        long base = 0;
+        if ((threadIdx.x & 31) == 0) base = atomicAdd(ticket, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        const long i = base + (threadIdx.x & 31);
+        if (i >= total) continue;
+        const int w = (int)(i / per);
+        const int j = (int)(i - (long)w * per);
+        const int kind = w == 0 ? first_kind : (first_kind == WARM ? SOLVE : first_kind);
+        const int sw = first_kind == WARM ? w - 1 : w;  // index among the block's SOLVE or RELAX sweeps
+        const bool reverse = kind != WARM && A.symmetric && sw % 2 == 1;
+        const bool is_pair = reverse ? j >= walls : j < placed;
+        if (is_pair) {
+            const long k = reverse ? (long)placed - 1 - (j - walls) : j;
+            const int4 rec4 = __ldg(&A.pairs.pair[k]);
+            const unsigned packed = (unsigned)rec4.w;
+            const int rankA = packed & 255u, rankB = (packed >> 8) & 255u;
+            const int degA = (packed >> 16) & 255u, degB = packed >> 24;
+            const int lA = A.listed[rec4.x], lB = A.listed[rec4.y];
+            const int wantA = w * (degA + lA) + (reverse ? lA + (degA - 1 - rankA) : rankA);
+            const int wantB = w * (degB + lB) + (reverse ? lB + (degB - 1 - rankB) : rankB);
+            if (!wait_versions(A, rec4.x, wantA, rec4.y, wantB)) return false;
+            solve_pair(A, k, rec4, kind, reverse);
+            __threadfence();
+            *(volatile int*)&A.version[rec4.x] = wantA + 1;
+            *(volatile int*)&A.version[rec4.y] = wantB + 1;
+        } else {
+            const int wk = reverse ? j : j - placed;
+            const int s = A.wall_list[wk < spheres ? wk : A.n - 1 - (wk - spheres)];
+            const int deg = __popc(A.body_colours[s]);
+            const int want = w * (deg + 1) + (reverse ? 0 : deg);
+            if (!wait_versions(A, s, want, -1, 0)) return false;
+            Held box;
+            load_held(box, A.b, s);
+            if (walls_of(A, box, s, kind, reverse)) store_held(box, A.b, s);
+            __threadfence();
+            *(volatile int*)&A.version[s] = want + 1;
+        }
+    }
+    (void)sweep0;
+    return true;
+}
+
 // Phase codes of the trace: kind | sweep << 4 | round << 8.
-enum : int { TR_START = 0, TR_VELOCITIES = 1, TR_WALLS = 2, TR_POSITIONS = 3, TR_ROUND = 4, TR_WALL_LIST = 5 };
+enum : int { TR_START = 0, TR_VELOCITIES = 1, TR_WALLS = 2, TR_POSITIONS = 3, TR_ROUND = 4, TR_WALL_LIST = 5,
+            TR_BLOCK = 6 };
 
 struct Tracer {
     unsigned long long* out;
@@ -863,14 +1013,26 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(SolveArgs A) {
         phase_velocities_and_list(A, 2 * sub);
         if (!grid_sync(A.bar, epoch)) return;
         tr.mark(TR_VELOCITIES);
-        if (!sweep_all(A, tr, epoch, WARM, false, rounds, 2 * sub)) return;
-        for (int sw = 0; sw < A.sweeps; sw++)
-            if (!sweep_all(A, tr, epoch, SOLVE, A.symmetric && sw % 2 == 1, rounds, 2 * sub)) return;
+        if (A.schedule == 1) {
+            if (!block_of_sweeps(A, WARM, 1 + A.sweeps, rounds, 2 * sub, 0)) return;
+            if (!grid_sync(A.bar, epoch)) return;
+            tr.mark(TR_BLOCK | SOLVE << 4);
+        } else {
+            if (!sweep_all(A, tr, epoch, WARM, false, rounds, 2 * sub)) return;
+            for (int sw = 0; sw < A.sweeps; sw++)
+                if (!sweep_all(A, tr, epoch, SOLVE, A.symmetric && sw % 2 == 1, rounds, 2 * sub)) return;
+        }
         phase_positions(A, 2 * sub + 1);
         if (!grid_sync(A.bar, epoch)) return;
         tr.mark(TR_POSITIONS);
-        for (int sw = 0; sw < A.sweeps; sw++)
-            if (!sweep_all(A, tr, epoch, RELAX, A.symmetric && sw % 2 == 1, rounds, 2 * sub + 1)) return;
+        if (A.schedule == 1) {
+            if (!block_of_sweeps(A, RELAX, A.sweeps, rounds, 2 * sub + 1, 0)) return;
+            if (!grid_sync(A.bar, epoch)) return;
+            tr.mark(TR_BLOCK | RELAX << 4);
+        } else {
+            for (int sw = 0; sw < A.sweeps; sw++)
+                if (!sweep_all(A, tr, epoch, RELAX, A.symmetric && sw % 2 == 1, rounds, 2 * sub + 1)) return;
+        }
     }
     if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) A.counters->trace_len = tr.len;
 }
@@ -970,7 +1132,7 @@ int enqueue_step(vxr_box_world* w) {
     int rc0 = mark(w, 0);
     if (rc0) return rc0;
     VXR_CUDA(cudaMemsetAsync(w->counters, 0, sizeof(Counters), st));
-    VXR_CUDA(cudaMemsetAsync(w->wall_count, 0, sizeof(int) * 2 * w->substeps, st));
+    VXR_CUDA(cudaMemsetAsync(w->wall_count, 0, sizeof(int) * 4 * w->substeps, st));
     PairGen& now = w->gen[w->cur];
     PairGen& was = w->gen[w->cur ^ 1];
     if (w->has_grid) {
@@ -1020,13 +1182,17 @@ int enqueue_step(vxr_box_world* w) {
             int rc = launch_cooperative(w, (const void*)k_colour, w->colour_blocks, THREADS, args);
             if (rc) return rc;
         }
-        VXR_CUDA(cudaMemsetAsync(w->round_count, 0, sizeof(int) * (MOST_ROUNDS + 1), st));
-        VXR_CUDA(cudaMemsetAsync(w->round_fill, 0, sizeof(int) * (MOST_ROUNDS + 1), st));
-        k_round_count<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_count, w->counters);
-        exclusive_scan(w->round_count, w->round_start, MOST_ROUNDS + 1, w->scan_tiles, st);
-        k_order<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_start, w->round_fill, w->ta,
-                                            w->tcand, w->man, w->imp_t, w->impr_t, now);
-        LAUNCHED(1 + 3 + 1 + 1 + 1 + 3 + 1);  // inc count, scan, inc fill, colour, round count, scan, order
+        VXR_CUDA(cudaMemsetAsync(w->round_count, 0, sizeof(int) * BUCKETS, st));
+        VXR_CUDA(cudaMemsetAsync(w->round_fill, 0, sizeof(int) * BUCKETS, st));
+        VXR_CUDA(cudaMemsetAsync(w->body_colours, 0, sizeof(unsigned) * n, st));
+        k_round_count<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_count, w->counters, w->ta,
+                                                  now.tb, w->body_colours, w->tcand, w->man.head, w->b.half);
+        exclusive_scan(w->round_count, w->bucket_start, BUCKETS, w->scan_tiles, st);
+        k_round_starts<<<1, 64, 0, st>>>(w->bucket_start, w->round_start);
+        k_order<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->bucket_start, w->round_fill, w->ta,
+                                            w->tcand, w->man, w->imp_t, w->impr_t, now,
+                                            w->body_colours, w->b.half);
+        LAUNCHED(1 + 3 + 1 + 1 + 1 + 3 + 1 + 1);  // inc count, scan, inc fill, colour, round count, scan, starts, order
     } else {
         if (int rc = mark(w, 1)) return rc;
         if (int rc = mark(w, 2)) return rc;
@@ -1041,6 +1207,10 @@ int enqueue_step(vxr_box_world* w) {
         A.wmask = w->wmask;
         A.wall_list = w->wall_list;
         A.wall_count = w->wall_count;
+        A.version = w->version;
+        A.listed = w->listed;
+        A.body_colours = w->body_colours;
+        A.schedule = w->schedule;
         A.pairs = now;
         A.round_start = w->round_start;
         A.counters = w->counters;
@@ -1206,6 +1376,7 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     w->substeps = cfg->substeps;
     w->sweeps = cfg->sweeps;
     w->symmetric = cfg->symmetric ? 1 : 0;
+    w->schedule = cfg->schedule == 1 ? 1 : 0;
     w->device = cfg->device;
     w->has_grid = (cfg->bodies > 1 && cfg->grid.nx > 0 && cfg->grid.ny > 0 && cfg->grid.nz > 0 && cfg->grid.cell > 0)
                       ? 1 : 0;
@@ -1252,11 +1423,15 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     rc |= alloc(w, &w->counters, 1);
     rc |= alloc(w, &w->totals, 1);
     rc |= alloc(w, &w->scan_tiles, scan_tiles_for(std::max(n, w->cells)) + 1);
-    rc |= alloc(w, &w->round_count, MOST_ROUNDS + 1);
+    rc |= alloc(w, &w->round_count, BUCKETS);
     rc |= alloc(w, &w->round_start, MOST_ROUNDS + 2);
+    rc |= alloc(w, &w->bucket_start, BUCKETS + 1);
     rc |= alloc(w, &w->wall_list, n);
-    rc |= alloc(w, &w->wall_count, 2 * (size_t)w->substeps);
-    rc |= alloc(w, &w->round_fill, MOST_ROUNDS + 1);
+    rc |= alloc(w, &w->wall_count, 4 * (size_t)w->substeps);
+    rc |= alloc(w, &w->version, n);
+    rc |= alloc(w, &w->listed, n);
+    rc |= alloc(w, &w->body_colours, n);
+    rc |= alloc(w, &w->round_fill, BUCKETS);
     if (w->has_grid) {
         rc |= alloc(w, &w->keys, n);
         rc |= alloc(w, &w->cell_count, w->cells);
@@ -1318,6 +1493,10 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     cudaMemsetAsync(w->shown, 0, sizeof(float) * (size_t)n * SHOWN_STRIDE, st);
     cudaMemsetAsync(w->counters, 0, sizeof(Counters), st);
     cudaMemsetAsync(w->totals, 0, sizeof(Totals), st);
+    cudaMemsetAsync(w->round_start, 0, sizeof(int) * (MOST_ROUNDS + 2), st);
+    cudaMemsetAsync(w->body_colours, 0, sizeof(unsigned) * n, st);
+    cudaMemsetAsync(w->version, 0, sizeof(int) * n, st);
+    cudaMemsetAsync(w->listed, 0, sizeof(int) * n, st);
     if (w->has_grid) {
         for (int g = 0; g < 2; g++) {
             cudaMemsetAsync(w->gen[g].tstart, 0, sizeof(int) * ((size_t)n + 1), st);

@@ -37,7 +37,7 @@ class Grid(ctypes.Structure):
 class BoxConfig(ctypes.Structure):
     _fields_ = [("bodies", ctypes.c_int32), ("substeps", ctypes.c_int32), ("sweeps", ctypes.c_int32),
                 ("symmetric", ctypes.c_int32), ("grid", Grid), ("reach_cells", ctypes.c_int32),
-                ("max_pairs", ctypes.c_int32), ("device", ctypes.c_int32)]
+                ("max_pairs", ctypes.c_int32), ("device", ctypes.c_int32), ("schedule", ctypes.c_int32)]
 
 
 class BoxReport(ctypes.Structure):

@@ -49,7 +49,8 @@ class BoxSimulation:
     """A box/mixed world on one GPU: BoxStep's shape plus BoxSimulation's calls."""
 
     def __init__(self, bodies: int, substeps: int, sweeps: int = B.WALL_PASSES, symmetric: bool = False,
-                 grid: B.Grid | None = None, reach_cells: int = 0, max_pairs: int = 0, device: int = 0):
+                 grid: B.Grid | None = None, reach_cells: int = 0, max_pairs: int = 0, device: int = 0,
+                 schedule: int = 0):
         if bodies < 1 or substeps < 1 or sweeps < 1:
             raise ValueError(f"a step needs bodies, substeps and sweeps, got {bodies}, {substeps} and {sweeps}")
         self.L = lib()
@@ -60,6 +61,7 @@ class BoxSimulation:
         cfg.reach_cells = reach_cells
         cfg.max_pairs = max_pairs
         cfg.device = device
+        cfg.schedule = schedule
         status = ctypes.c_int32(0)
         self.h = self.L.vxr_box_create(ctypes.byref(cfg), ctypes.byref(status))
         if not self.h:
