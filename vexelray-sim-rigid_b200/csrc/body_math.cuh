@@ -38,9 +38,13 @@ __device__ __forceinline__ void cross3(const float* x, const float* y, float* o)
     o[1] = c1;
     o[2] = c2;
 }
-// p turned by q: p + w t + q × t with t = 2 q × p / |q|².
-__device__ __forceinline__ void rotateq(const float* q, const float* p, float* out) {
-    const float twice = 2.0f / ((q[0] * q[0] + q[1] * q[1]) + (q[2] * q[2] + q[3] * q[3]));
+// 2 / |q|², the factor every turn by q (or by its conjugate: the same squares) scales by.
+__device__ __forceinline__ float twice_of(const float* q) {
+    return 2.0f / ((q[0] * q[0] + q[1] * q[1]) + (q[2] * q[2] + q[3] * q[3]));
+}
+
+// p turned by q: p + w t + q × t with t = 2 q × p / |q|², the factor given.
+__device__ __forceinline__ void rotate_by(const float* q, float twice, const float* p, float* out) {
     float t[3];
     cross3(q, p, t);
 #pragma unroll
@@ -54,6 +58,7 @@ __device__ __forceinline__ void rotateq(const float* q, const float* p, float* o
     out[1] = o[1];
     out[2] = o[2];
 }
+__device__ __forceinline__ void rotateq(const float* q, const float* p, float* out) { rotate_by(q, twice_of(q), p, out); }
 __device__ __forceinline__ float sign_of(float x) { return x < 0.0f ? -1.0f : 1.0f; }
 
 // q turned by omega for dt, first order, normalised.
@@ -89,23 +94,25 @@ __device__ __forceinline__ void inverse_inertia(const float4 half, float im, flo
 // updated in registers and stored once.
 struct Held {
     float at[3], q[4], half[3], inverse[3], velocity[3], momentum[3], omega[3];
-    float im, shape;
+    float im, shape, twice;
 
     __device__ __forceinline__ void times_inverse_inertia(const float* x, float* out) const {
         const float c[4] = {-q[0], -q[1], -q[2], q[3]};
         float own[3], scaled[3];
-        rotateq(c, x, own);
+        rotate_by(c, twice, x, own);
 #pragma unroll
         for (int a = 0; a < 3; a++) scaled[a] = inverse[a] * own[a];
-        rotateq(q, scaled, out);
+        rotate_by(q, twice, scaled, out);
     }
-    __device__ __forceinline__ void load(float4 pose, float4 turn, float4 halfw, float4 vel, float4 mom) {
+    // inv: the body's inverse principal moments (inverse_inertia of its half-extents, shape and inverse mass)
+    __device__ __forceinline__ void load(float4 pose, float4 turn, float4 halfw, float4 vel, float4 mom, float4 inv) {
         at[0] = pose.x; at[1] = pose.y; at[2] = pose.z; im = pose.w;
         q[0] = turn.x; q[1] = turn.y; q[2] = turn.z; q[3] = turn.w;
         half[0] = halfw.x; half[1] = halfw.y; half[2] = halfw.z; shape = halfw.w;
         velocity[0] = vel.x; velocity[1] = vel.y; velocity[2] = vel.z;
         momentum[0] = mom.x; momentum[1] = mom.y; momentum[2] = mom.z;
-        inverse_inertia(halfw, im, inverse);
+        inverse[0] = inv.x; inverse[1] = inv.y; inverse[2] = inv.z;
+        twice = twice_of(q);
         times_inverse_inertia(momentum, omega);
     }
     __device__ __forceinline__ bool sphere() const { return shape > 0.5f; }
@@ -199,9 +206,12 @@ __device__ __forceinline__ void apply_angular(Held& first, Held& second, const f
 
 // One contact point, one sweep. rec = (normal impulse, tangential impulse x, y, z), updated in place.
 // Returns whether the record was touched (read and possibly written).
+// k_given: the normal's generalised inverse mass when the caller has it (it depends only on the pose, so it is the
+// same in every sweep of a substep's half); negative: computed here.
 template <bool PAIR>
 __device__ __forceinline__ void contact(int sweep, float gap, const float* n, Held& first, const float* rA,
-                                        Held& second, const float* rB, float4& rec, const Soft& soft) {
+                                        Held& second, const float* rB, float4& rec, const Soft& soft,
+                                        float k_given = -1.0f) {
     const float normal = rec.x;
     const float tangent[3] = {rec.y, rec.z, rec.w};
     const bool holding = normal > 0.0f || dot3(tangent, tangent) > 0.0f;
@@ -215,7 +225,7 @@ __device__ __forceinline__ void contact(int sweep, float gap, const float* n, He
         return;
     }
     if (!(gap < soft.margin || holding)) return;
-    const float k = mass_along<PAIR>(first, rA, second, rB, n);
+    const float k = k_given >= 0.0f ? k_given : mass_along<PAIR>(first, rA, second, rB, n);
     float rel[3];
     relative_velocity<PAIR>(first, rA, second, rB, rel);
     const float closing = dot3(rel, n);

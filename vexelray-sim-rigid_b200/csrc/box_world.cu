@@ -49,6 +49,7 @@ constexpr int BUCKETS = (MOST_ROUNDS + 1) * PAIR_KINDS;
 // Device buffers of a world.
 struct Bodies {
     float4 *pose, *turn, *half, *vel, *mom;  // (x, y, z, im), (qx, qy, qz, qw), (hx, hy, hz, shape), (u, v, w, 0), (L, 0)
+    float4* inv;  // inverse principal moments (Boxes.inverseInertia), fixed once the bodies are loaded
 };
 
 struct Manifolds {  // the narrow phase's output, by candidate pair (the current step's)
@@ -70,6 +71,8 @@ struct PairGen {
     float4* pb;      // [cap * 4] by position: anchor on second
     float4* imp;     // [cap * 4] by position: normal impulse, tangential impulse
     float4* impr;    // [cap * 4] by position: rolling impulse
+    float4* prepA;   // [cap * 4] by position, this half-substep: anchor on first in the world's frame, gap
+    float4* prepB;   // [cap * 4] by position, this half-substep: anchor on second in the world's frame, k normal
 };
 
 struct Counters {  // device-side counts of a step
@@ -617,7 +620,8 @@ struct SolveArgs {
 // Body state a solve phase reads and writes goes through L2 (ld/st .cg): under the dependency schedule one
 // body's consecutive items can run on different SMs.
 __device__ __forceinline__ void load_held(Held& h, const Bodies& b, int s) {
-    h.load(__ldcg(&b.pose[s]), __ldcg(&b.turn[s]), __ldg(&b.half[s]), __ldcg(&b.vel[s]), __ldcg(&b.mom[s]));
+    h.load(__ldcg(&b.pose[s]), __ldcg(&b.turn[s]), __ldg(&b.half[s]), __ldcg(&b.vel[s]), __ldcg(&b.mom[s]),
+           __ldg(&b.inv[s]));
 }
 __device__ __forceinline__ void store_held(const Held& h, const Bodies& b, int s) {
     __stcg(&b.vel[s], make_float4(h.velocity[0], h.velocity[1], h.velocity[2], 0.0f));
@@ -646,24 +650,26 @@ __device__ __forceinline__ void phase_positions(const SolveArgs& A, int slot) {
         const float q[4] = {tq.x, tq.y, tq.z, tq.w};
         const float4 l = __ldcg(&A.b.mom[s]);
         const float momentum[3] = {l.x, l.y, l.z};
-        float inverse[3];
-        inverse_inertia(__ldg(&A.b.half[s]), im, inverse);
+        const float4 inv = __ldg(&A.b.inv[s]);
+        const float inverse[3] = {inv.x, inv.y, inv.z};
         float omega[3], mid[4], omega_mid[3], end[4];
         {
             const float c[4] = {-q[0], -q[1], -q[2], q[3]};
+            const float tw = twice_of(q);
             float own[3], scaled[3];
-            rotateq(c, momentum, own);
+            rotate_by(c, tw, momentum, own);
             for (int a = 0; a < 3; a++) scaled[a] = inverse[a] * own[a];
-            rotateq(q, scaled, omega);
+            rotate_by(q, tw, scaled, omega);
         }
         const float half_h = 0.5f * h;
         turned(q, omega, half_h, mid);
         {
             const float c[4] = {-mid[0], -mid[1], -mid[2], mid[3]};
+            const float tw = twice_of(mid);
             float own[3], scaled[3];
-            rotateq(c, momentum, own);
+            rotate_by(c, tw, momentum, own);
             for (int a = 0; a < 3; a++) scaled[a] = inverse[a] * own[a];
-            rotateq(mid, scaled, omega_mid);
+            rotate_by(mid, tw, scaled, omega_mid);
         }
         turned(q, omega_mid, h, end);
         __stcg(&A.b.turn[s], make_float4(end[0], end[1], end[2], end[3]));
@@ -789,7 +795,7 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
                     const int sgn = (c >> a) & 1;
                     offset[a] = box.half[a] * (2.0f * (float)sgn - 1.0f);
                 }
-                rotateq(box.q, offset, r);
+                rotate_by(box.q, box.twice, offset, r);
                 const float reach = pick3(box.at, axis) + pick3(r, axis);
                 const float gap = high ? pick3(extent, axis) - reach : reach;
                 if (!(held || (sweep != WARM && gap < margin))) continue;
@@ -823,7 +829,10 @@ __device__ __forceinline__ void phase_walls(const SolveArgs& A, int sweep, bool 
 
 // BoxPairs.solve :64-151 for the pair at round-order position k: its whole manifold in turn, both bodies loaded
 // once and stored once.
-__device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4, int sweep, bool reverse) {
+// fill: the first sweep of a substep's half (positions fixed until the next positions phase): each point's anchors
+// in the world's frame, its gap and its normal's generalised inverse mass are worked out and kept; the later
+// sweeps of that half read them back (the same values the reference works out again every sweep).
+__device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4, int sweep, bool reverse, bool fill) {
     const Params& P = A.params;
     const float4 head = __ldg(&A.pairs.normal[k]);
     const int ia = rec4.x, ib = rec4.y, count = rec4.z;
@@ -842,26 +851,35 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
         const int slot = reverse ? MOST_POINTS - 1 - order : order;
         if (!(slot < count)) continue;
         const long at = k * MOST_POINTS + slot;
-        float rA[3], rB[3];
-        if (first.sphere()) {
-            for (int a = 0; a < 3; a++) rA[a] = first.half[0] * n[a];
+        float rA[3], rB[3], gap, kn;
+        if (fill) {
+            if (first.sphere()) {
+                for (int a = 0; a < 3; a++) rA[a] = first.half[0] * n[a];
+            } else {
+                const float4 qa = __ldg(&A.pairs.pa[at]);
+                const float anchorA[3] = {qa.x, qa.y, qa.z};
+                rotate_by(first.q, first.twice, anchorA, rA);
+            }
+            if (second.sphere()) {
+                for (int a = 0; a < 3; a++) rB[a] = -(second.half[0] * n[a]);
+            } else {
+                const float4 qb = __ldg(&A.pairs.pb[at]);
+                const float anchorB[3] = {qb.x, qb.y, qb.z};
+                rotate_by(second.q, second.twice, anchorB, rB);
+            }
+            gap = ((second.at[0] + rB[0]) - (first.at[0] + rA[0])) * n[0] +
+                  ((second.at[1] + rB[1]) - (first.at[1] + rA[1])) * n[1];
+            gap = gap + ((second.at[2] + rB[2]) - (first.at[2] + rA[2])) * n[2];
+            kn = mass_along<true>(first, rA, second, rB, n);
+            __stcg(&A.pairs.prepA[at], make_float4(rA[0], rA[1], rA[2], gap));
+            __stcg(&A.pairs.prepB[at], make_float4(rB[0], rB[1], rB[2], kn));
         } else {
-            const float4 qa = __ldg(&A.pairs.pa[at]);
-            const float anchorA[3] = {qa.x, qa.y, qa.z};
-            rotateq(first.q, anchorA, rA);
+            const float4 pa = __ldcg(&A.pairs.prepA[at]), pb = __ldcg(&A.pairs.prepB[at]);
+            rA[0] = pa.x; rA[1] = pa.y; rA[2] = pa.z; gap = pa.w;
+            rB[0] = pb.x; rB[1] = pb.y; rB[2] = pb.z; kn = pb.w;
         }
-        if (second.sphere()) {
-            for (int a = 0; a < 3; a++) rB[a] = -(second.half[0] * n[a]);
-        } else {
-            const float4 qb = __ldg(&A.pairs.pb[at]);
-            const float anchorB[3] = {qb.x, qb.y, qb.z};
-            rotateq(second.q, anchorB, rB);
-        }
-        float gap = ((second.at[0] + rB[0]) - (first.at[0] + rA[0])) * n[0] +
-                    ((second.at[1] + rB[1]) - (first.at[1] + rA[1])) * n[1];
-        gap = gap + ((second.at[2] + rB[2]) - (first.at[2] + rA[2])) * n[2];
         float4 rec = __ldcg(&A.pairs.imp[at]);
-        contact<true>(sweep, gap, n, first, rA, second, rB, rec, soft);
+        contact<true>(sweep, gap, n, first, rA, second, rB, rec, soft, kn);
         if (sweep != WARM) __stcg(&A.pairs.imp[at], rec);
         if (anySphere) {
             float radius = second.half[0];
@@ -878,11 +896,11 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
 }
 
 // One round of pairs that share no body (the barrier schedule).
-__device__ __forceinline__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r) {
+__device__ __forceinline__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r, bool fill) {
     const int stride = gridDim.x * blockDim.x;
     const int lo = A.round_start[r], hi = A.round_start[r + 1];
     for (int k = lo + blockIdx.x * blockDim.x + threadIdx.x; k < hi; k += stride)
-        solve_pair(A, k, __ldg(&A.pairs.pair[k]), sweep, reverse);
+        solve_pair(A, k, __ldg(&A.pairs.pair[k]), sweep, reverse, fill);
 }
 
 // Waits until every listed body has done exactly `want` items of this block. A bounded wait: past the limit it
@@ -947,7 +965,7 @@ __device__ __forceinline__ bool block_of_sweeps(const SolveArgs& A, int first_ki
             const int wantA = w * (degA + lA) + (reverse ? lA + (degA - 1 - rankA) : rankA);
             const int wantB = w * (degB + lB) + (reverse ? lB + (degB - 1 - rankB) : rankB);
             if (!wait_versions(A, rec4.x, wantA, rec4.y, wantB)) return false;
-            solve_pair(A, k, rec4, kind, reverse);
+            solve_pair(A, k, rec4, kind, reverse, w == 0);
             __threadfence();
             *(volatile int*)&A.version[rec4.x] = wantA + 1;
             *(volatile int*)&A.version[rec4.y] = wantB + 1;
@@ -984,7 +1002,7 @@ struct Tracer {
 // One sweep (BoxStep.sweep :253-267): every round of pairs, then the walls; backward, the walls first and the
 // rounds last to first.
 __device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsigned int& epoch, int kind, bool reverse,
-                                          int rounds, int slot) {
+                                          int rounds, int slot, bool fill) {
     if (reverse) {
         phase_walls(A, kind, true, slot);
         if (!grid_sync(A.bar, epoch)) return false;
@@ -992,7 +1010,7 @@ __device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsign
     }
     for (int order = 0; order < rounds; order++) {
         const int r = reverse ? rounds - 1 - order : order;
-        phase_round(A, kind, reverse, r);
+        phase_round(A, kind, reverse, r, fill);
         if (!grid_sync(A.bar, epoch)) return false;
         tr.mark(TR_ROUND | kind << 4 | r << 8);
     }
@@ -1018,9 +1036,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(SolveArgs A) {
             if (!grid_sync(A.bar, epoch)) return;
             tr.mark(TR_BLOCK | SOLVE << 4);
         } else {
-            if (!sweep_all(A, tr, epoch, WARM, false, rounds, 2 * sub)) return;
+            if (!sweep_all(A, tr, epoch, WARM, false, rounds, 2 * sub, true)) return;
             for (int sw = 0; sw < A.sweeps; sw++)
-                if (!sweep_all(A, tr, epoch, SOLVE, A.symmetric && sw % 2 == 1, rounds, 2 * sub)) return;
+                if (!sweep_all(A, tr, epoch, SOLVE, A.symmetric && sw % 2 == 1, rounds, 2 * sub, false)) return;
         }
         phase_positions(A, 2 * sub + 1);
         if (!grid_sync(A.bar, epoch)) return;
@@ -1031,7 +1049,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(SolveArgs A) {
             tr.mark(TR_BLOCK | RELAX << 4);
         } else {
             for (int sw = 0; sw < A.sweeps; sw++)
-                if (!sweep_all(A, tr, epoch, RELAX, A.symmetric && sw % 2 == 1, rounds, 2 * sub + 1)) return;
+                if (!sweep_all(A, tr, epoch, RELAX, A.symmetric && sw % 2 == 1, rounds, 2 * sub + 1, sw == 0))
+                    return;
         }
     }
     if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) A.counters->trace_len = tr.len;
@@ -1086,6 +1105,16 @@ __global__ void k_activity(int n, const int* __restrict__ inc_count, const unsig
     const bool paired = inc_count != nullptr && inc_count[s] > 0;
     if (paired || m) atomicAdd((unsigned long long*)&out[0], 1ull);
     if (m) atomicAdd((unsigned long long*)&out[1], (unsigned long long)__popcll(m));
+}
+
+// Each body's inverse principal moments, once its half-extents, shape and inverse mass are loaded.
+__global__ void k_inverse_inertia(int n, const float4* __restrict__ pose, const float4* __restrict__ half,
+                                  float4* __restrict__ inv) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    float i3[3];
+    inverse_inertia(half[s], pose[s].w, i3);
+    inv[s] = make_float4(i3[0], i3[1], i3[2], 0.0f);
 }
 
 // ------------------------------------------------------------------------------------------------------------
@@ -1416,6 +1445,7 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     rc |= alloc(w, &w->b.half, n);
     rc |= alloc(w, &w->b.vel, n);
     rc |= alloc(w, &w->b.mom, n);
+    rc |= alloc(w, &w->b.inv, n);
     rc |= alloc(w, &w->wall, (size_t)n * WALL_RECORDS);
     rc |= alloc(w, &w->wroll, (size_t)n * 6);
     rc |= alloc(w, &w->wmask, n);
@@ -1466,6 +1496,13 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
             rc |= alloc(w, &p.pb, (size_t)w->cap * MOST_POINTS);
             rc |= alloc(w, &p.imp, (size_t)w->cap * MOST_POINTS);
             rc |= alloc(w, &p.impr, (size_t)w->cap * MOST_POINTS);
+            if (g == 0) {  // the prepared anchors live for one half-substep: one buffer serves both generations
+                rc |= alloc(w, &p.prepA, (size_t)w->cap * MOST_POINTS);
+                rc |= alloc(w, &p.prepB, (size_t)w->cap * MOST_POINTS);
+            } else {
+                p.prepA = w->gen[0].prepA;
+                p.prepB = w->gen[0].prepB;
+            }
         }
         rc |= alloc(w, &w->colour, w->cap);
         rc |= alloc(w, &w->inc_count, n);
@@ -1542,6 +1579,8 @@ int32_t vxr_box_load_state(vxr_box_world* w, const float* const* f, const int32_
     rc |= upload4(w, w->b.turn, f[9], f[10], f[11], f[12], 1.0f);
     rc |= upload4(w, w->b.half, f[14], f[15], f[16], f[17], 0.0f);
     if (rc) return VXR_ECUDA;
+    k_inverse_inertia<<<blocks_for(w->n, THREADS), THREADS, 0, w->stream>>>(w->n, w->b.pose, w->b.half, w->b.inv);
+    VXR_CUDA(cudaGetLastError());
     if (params) vxr_box_params(w, params);
     return VXR_OK;
 }
