@@ -179,6 +179,27 @@ int32_t vxr_box_activity(vxr_box_world* world, int64_t* out4);
 int32_t vxr_collide(int32_t bodies, const float* const* fields18, const int32_t* params18, int32_t npairs,
                     const int32_t* pairs, float* manifold40);
 
+/* The broad phase with no allocation. No counterpart in the reference: it exists for callers that cannot allocate
+ * device memory while they step bodies — a host that owns all device memory through its own pool, or code that
+ * must not allocate (an allocation synchronises the device) between the launches it is recording or under a
+ * frame deadline. It runs the same bin, stable counting sort, neighbourhood list and compaction as a world's step
+ * (core/box/BoxBroad.java:74-164 is what those replace) and writes the candidate pairs, sorted by (first, second),
+ * to the caller's device arrays first_out and second_out (capacity entries each). All its scratch lives in one array
+ * of about 6 MiB in this library's device memory, which every GPU that loads the library holds until the process
+ * exits; nothing is allocated.
+ *   Limits: at most 16384 bodies and 262144 grid cells a call; beyond them the call returns VXR_ECAPACITY and does
+ *   nothing.
+ *   fields11: device pointers to x y z qx qy qz qw hx hy hz shape (bodies floats each).
+ *   result3: a device array that receives [candidate pairs found (may exceed capacity), partners beyond 32 slots,
+ *   VXR_OK or VXR_ECAPACITY (more pairs than capacity: the first capacity are written)].
+ *   stream: the cudaStream_t to run on (NULL: the default stream); the call does not wait.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) and should come before
+ * any stream capture. Every call shares the array and it keeps the last call's contents: calls whose work overlaps
+ * on the GPU (other streams, other host threads) race, so order them on one stream. */
+int32_t vxr_box_broadphase_static(int32_t bodies, const float* const* fields11, vxr_grid grid, int32_t reach_cells,
+                                  float margin, int32_t* first_out, int32_t* second_out, int32_t capacity,
+                                  int32_t* result3, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1962,3 +1963,134 @@ int32_t vxr_collide(int32_t bodies, const float* const* f, const int32_t* params
 }
 
 }  // extern "C"
+
+// ================================================================================================================
+// The broad phase with no allocation.
+//
+// Some callers cannot allocate device memory while they step bodies: a host that hands the library only memory
+// from its own pool (a Java or game-engine host managing device memory itself), code running where an allocation
+// would synchronise the device or is forbidden (inside a frame's command stream, between the launches a caller is
+// recording into a CUDA graph, or under a real-time deadline). For them, one entry point runs the broad phase (bin,
+// stable counting sort, neighbourhood list and compaction: the same kernels a world's step runs) with all its
+// scratch in one array in this library's device memory, sized below, that every GPU which loads the library holds
+// until the process exits. The caller passes the inputs and the outputs; the library allocates nothing.
+namespace {
+
+constexpr int STATIC_MAX_BODIES = 16384;
+constexpr int STATIC_MAX_CELLS = 262144;
+
+constexpr size_t pad256(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+// regions, in order: pose, turn, half, reach (float4 a body); keys, order_tmp, order, partner (32 a body), found,
+// kept, cand_start (+1); cell_count, cell_fill, cell_start (+1); scan tiles; counters
+constexpr size_t STATIC_F4 = pad256(sizeof(float4) * STATIC_MAX_BODIES);
+constexpr size_t STATIC_N = pad256(sizeof(int) * STATIC_MAX_BODIES);
+constexpr size_t STATIC_N1 = pad256(sizeof(int) * (STATIC_MAX_BODIES + 1));
+constexpr size_t STATIC_PARTNER = pad256(sizeof(int) * STATIC_MAX_BODIES * SLOTS);
+constexpr size_t STATIC_C = pad256(sizeof(int) * STATIC_MAX_CELLS);
+constexpr size_t STATIC_C1 = pad256(sizeof(int) * (STATIC_MAX_CELLS + 1));
+constexpr size_t STATIC_TILES = pad256(sizeof(int) * ((STATIC_MAX_CELLS + SCAN_TILE - 1) / SCAN_TILE + 1));
+constexpr size_t STATIC_COUNTERS = pad256(sizeof(Counters));
+constexpr size_t STATIC_BYTES = 4 * STATIC_F4 + 5 * STATIC_N + STATIC_N1 + STATIC_PARTNER + 2 * STATIC_C + STATIC_C1 +
+                                STATIC_TILES + STATIC_COUNTERS;
+
+}  // namespace
+
+// The scratch of vxr_box_broadphase_static: about 6 MiB. Host code must not use this name as a device address; the
+// address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char vxr_broadphase_scratch[STATIC_BYTES];
+
+namespace {
+
+struct StaticFields {
+    const float *x, *y, *z, *qx, *qy, *qz, *qw, *hx, *hy, *hz, *shape;
+};
+
+__global__ void k_pack_static(int n, StaticFields f, float4* __restrict__ pose, float4* __restrict__ turn,
+                              float4* __restrict__ half) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    pose[s] = make_float4(f.x[s], f.y[s], f.z[s], 0.0f);
+    turn[s] = make_float4(f.qx[s], f.qy[s], f.qz[s], f.qw[s]);
+    half[s] = make_float4(f.hx[s], f.hy[s], f.hz[s], f.shape[s]);
+}
+
+__global__ void k_static_result(int n, int capacity, const int* __restrict__ cand_start, const Counters* counters,
+                                int32_t* __restrict__ result) {
+    const int total = cand_start[n];
+    result[0] = total;
+    result[1] = counters->unlisted;
+    result[2] = total > capacity ? VXR_ECAPACITY : VXR_OK;
+}
+
+std::mutex static_setup_lock;
+unsigned char* static_scratch_of_device[64] = {nullptr};
+
+}  // namespace
+
+extern "C" int32_t vxr_box_broadphase_static(int32_t bodies, const float* const* fields11, vxr_grid grid,
+                                             int32_t reach_cells, float margin, int32_t* first_out,
+                                             int32_t* second_out, int32_t capacity, int32_t* result3,
+                                             void* stream) {
+    if (bodies < 1 || !fields11 || !first_out || !second_out || !result3 || capacity < 0 || !(margin >= 0.0f))
+        return VXR_EINVAL;
+    for (int k = 0; k < 11; k++)
+        if (!fields11[k]) return VXR_EINVAL;
+    if (grid.nx < 1 || grid.ny < 1 || grid.nz < 1 || !(grid.cell > 0.0f)) return VXR_EINVAL;
+    const long cells = (long)grid.nx * grid.ny * grid.nz;
+    if (bodies > STATIC_MAX_BODIES || cells > STATIC_MAX_CELLS) return VXR_ECAPACITY;  // beyond the fixed scratch
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return VXR_ECUDA;
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> hold(static_setup_lock);
+        if (!static_scratch_of_device[device]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, vxr_broadphase_scratch) != cudaSuccess || !p) return VXR_ECUDA;
+            static_scratch_of_device[device] = (unsigned char*)p;
+        }
+        base = static_scratch_of_device[device];
+    }
+    unsigned char* at = base;
+    auto take = [&](size_t bytes) {
+        unsigned char* r = at;
+        at += bytes;
+        return r;
+    };
+    float4* pose = (float4*)take(STATIC_F4);
+    float4* turn = (float4*)take(STATIC_F4);
+    float4* half = (float4*)take(STATIC_F4);
+    float4* reach = (float4*)take(STATIC_F4);
+    int* keys = (int*)take(STATIC_N);
+    int* order_tmp = (int*)take(STATIC_N);
+    int* order = (int*)take(STATIC_N);
+    int* partner = (int*)take(STATIC_PARTNER);
+    int* found = (int*)take(STATIC_N);
+    int* kept = (int*)take(STATIC_N);
+    int* cand_start = (int*)take(STATIC_N1);
+    int* cell_count = (int*)take(STATIC_C);
+    int* cell_fill = (int*)take(STATIC_C);
+    int* cell_start = (int*)take(STATIC_C1);
+    int* tiles = (int*)take(STATIC_TILES);
+    Counters* counters = (Counters*)take(STATIC_COUNTERS);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n = bodies;
+    // What must start at zero (the array keeps the last call's contents): the cell counts and fills, the counters.
+    if (cudaMemsetAsync(cell_count, 0, sizeof(int) * cells, st) != cudaSuccess) return VXR_ECUDA;
+    if (cudaMemsetAsync(cell_fill, 0, sizeof(int) * cells, st) != cudaSuccess) return VXR_ECUDA;
+    if (cudaMemsetAsync(counters, 0, sizeof(Counters), st) != cudaSuccess) return VXR_ECUDA;
+    StaticFields f{fields11[0], fields11[1], fields11[2], fields11[3], fields11[4], fields11[5],
+                   fields11[6], fields11[7], fields11[8], fields11[9], fields11[10]};
+    GridDims g{grid.nx, grid.ny, grid.nz, grid.cell, reach_cells > 0 ? reach_cells : 1};
+    k_pack_static<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, f, pose, turn, half);
+    k_bin<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, g, pose, turn, half, keys, reach, cell_count);
+    exclusive_scan(cell_count, cell_start, (int)cells, tiles, st);
+    k_scatter<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, keys, cell_start, cell_fill, order_tmp);
+    k_stable<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, keys, cell_start, order_tmp, order);
+    k_list<<<blocks_for(n, 128), 128, 0, st>>>(n, g, margin, pose, reach, keys, cell_start, order, partner, found,
+                                              kept, counters);
+    exclusive_scan(kept, cand_start, n, tiles, st);
+    k_candidates<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, capacity, kept, cand_start, partner, first_out,
+                                                            second_out, counters);
+    k_static_result<<<1, 1, 0, st>>>(n, capacity, cand_start, counters, result3);
+    return cudaGetLastError() == cudaSuccess ? VXR_OK : VXR_ECUDA;
+}
