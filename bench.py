@@ -136,10 +136,15 @@ def barrier(pg):
         pg.barrier()
 
 
+ITERATION_CAP = 64
+
+
 def make_world(scene, device, max_pairs=0):
     from vxr.box_simulation import BoxSimulation
-    w = BoxSimulation(scene["bodies"], scene["substeps"], scene["sweeps"], False, scene["grid"], device=device,
-                      max_pairs=max_pairs)
+    # room for the iteration count measurement's sweeps; the steps run the scene's own
+    w = BoxSimulation(scene["bodies"], scene["substeps"], max(scene["sweeps"], ITERATION_CAP), False, scene["grid"],
+                      device=device, max_pairs=max_pairs)
+    w.measure(residual=False, sweeps=scene["sweeps"])
     l = [scene["lx"], scene["ly"], scene["lz"]]
     q = [scene["qx"], scene["qy"], scene["qz"], scene["qw"]]
     h = [scene["hx"], scene["hy"], scene["hz"]]
@@ -206,6 +211,7 @@ def main():
     ap.add_argument("--bodies", type=int, default=BODIES)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-iterations", action="store_true")
     ap.add_argument("--max-pairs", type=int, default=0, help="pair capacity of the world (0: 32 a body)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -265,6 +271,24 @@ def main():
                                       activity["points"], activity["bodies_active"], activity["wall_records"])
     achieved = b_solve / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
 
+    # Iterations to residual: the same world, the pile as the timed steps left it, a substep's solve sweeps run until
+    # a sweep's residual (the largest positional correction it makes at any contact point) is 1e-4 m or less, at most
+    # 64; with the impulses carried from the step before (the reference's warm start) and from zero (none).
+    iters = {"tolerance_m": 1e-4, "cap": ITERATION_CAP, "definition": "solve sweeps a substep runs until its residual "
+             "max_points h k (|dlambda_n| + |dlambda_t|) <= 1e-4 m", "learned": None}
+    if not args.no_iterations:
+        for name, cold in (("plain_warm_start", False), ("plain_cold_start", True)):
+            w.measure(residual=True, cold_start=cold, sweeps=ITERATION_CAP, tolerance=1e-4)
+            used_all = []
+            for _ in range(3):
+                w.step_async(1)
+                w.sync()
+                _, used = w.residuals()
+                used_all.extend(int(u) for u in used[:, 0])
+            iters[name] = float(np.mean(used_all))
+            iters[name + "_reached"] = float(np.mean([u < ITERATION_CAP for u in used_all]))
+        w.measure(residual=False, cold_start=False, sweeps=scene["sweeps"], tolerance=0.0)
+
     e2e = None
     if not args.no_e2e:
         w2 = make_world(scene, local, args.max_pairs)
@@ -303,6 +327,7 @@ def main():
                      "frac": achieved / hbm, "traffic": None, "peak_source": which,
                      "bytes_per_launch": b_solve, "ms_per_launch": solve_ms},
         "gpu_launches": int(launches),
+        "iterations_to_residual": iters,
         "e2e": e2e,
     }
     line["clocks"] = clocks.summary()

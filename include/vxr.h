@@ -154,6 +154,22 @@ int32_t vxr_box_walls(vxr_box_world* world, float* lambda48, float* rub144, floa
 /* How many dependency waves the last step's colouring took. */
 int32_t vxr_box_colour_waves(vxr_box_world* world);
 
+/* Measurement and iteration switches, from the next step on: residual = 1 gathers each sweep's residual (below);
+ * cold_start = 1 starts every step's pair impulses from zero instead of carrying them (BoxPairs.carry,
+ * core/box/BoxPairs.java:191-267) — the plain solver with no warm start, for comparison; sweeps (1 .. the count the
+ * world was created with; 0 = that count) sets the sweeps of the solve and of the relax a substep runs, as the
+ * reference's BoxStep sweeps (core/box/BoxStep.java:86); tolerance > 0 (with residual = 1, barrier schedule) stops a
+ * substep's solve sweeps, and its relax sweeps, once a sweep's residual is at or below it. */
+int32_t vxr_box_measure(vxr_box_world* world, int32_t residual, int32_t cold_start, int32_t sweeps, float tolerance);
+
+/* The last step's per-sweep residuals, substep by substep: the warm sweep, the solve sweeps, the relax sweeps
+ * (substeps * (2 sweeps + 1) values). A sweep's residual is the largest positional correction its updates made at any
+ * contact point, h k (|change of the normal impulse| + |change of the tangential impulse|) in metres, k the point's
+ * generalised inverse mass along the normal: zero when the Gauss-Seidel solve has converged. The reference has no
+ * residual; this is the measure "iterations to residual" counts in. used (may be NULL) receives 2 substeps ints: the
+ * solve and the relax sweeps each substep ran. Returns the count of residuals, or minus a status. */
+int32_t vxr_box_residuals(vxr_box_world* world, float* out, int32_t capacity, int32_t* used);
+
 /* Kernels this world has launched since creation (each step launches the same number). */
 long long vxr_box_launches(vxr_box_world* world);
 

@@ -168,3 +168,44 @@ def test_gpu_pile_of_343_rests():
 
 def test_gpu_pile_of_1000_rests():
     C.case_pile("gpu", side=10, most_energy=1e-5, most_depth=2e-3)
+
+
+def test_gpu_measuring_the_residual_changes_nothing():
+    a = C.pile_scene(7)
+    b = C.pile_scene(7)
+    a.start("oracle", threads=True)
+    b.start("gpu")
+    b.world.measure(residual=True)
+    for _ in range(30):
+        assert tuple(a.world.step(1)) == tuple(b.world.step(1))
+    compare_worlds(a, b)
+    res, used = b.world.residuals()
+    assert res.shape == (b.substeps, 2 * b.passes + 1)
+    assert (res[:, 0] == 0).all()  # the warm sweep moves no impulse
+    assert (used == b.passes).all()
+
+
+def iterations(world, steps, cold, tolerance=1e-4, cap=64):
+    world.measure(residual=True, cold_start=cold, sweeps=cap, tolerance=tolerance)
+    runs = []
+    for _ in range(steps):
+        world.step(1)
+        res, used = world.residuals()
+        for sub in range(used.shape[0]):
+            n = used[sub, 0]
+            assert n <= cap
+            if n < cap:  # it stopped: that sweep's residual met the tolerance
+                assert res[sub, n] <= tolerance
+            runs.append(n)
+    return float(np.mean(runs))
+
+
+def test_gpu_a_warm_start_converges_in_fewer_sweeps_than_a_cold_one():
+    scene = C.pile_scene(7)
+    scene.passes = 64
+    scene.start("gpu")
+    scene.world.measure(residual=True, sweeps=8)
+    scene.advance_seconds(3)  # the pile at rest
+    warm = iterations(scene.world, 5, cold=False)
+    cold = iterations(scene.world, 5, cold=True)
+    assert warm < cold, (warm, cold)

@@ -208,10 +208,13 @@ __device__ __forceinline__ void apply_angular(Held& first, Held& second, const f
 // Returns whether the record was touched (read and possibly written).
 // k_given: the normal's generalised inverse mass when the caller has it (it depends only on the pose, so it is the
 // same in every sweep of a substep's half); negative: computed here.
+// track: where the sweep's residual is gathered (null: not measured). A point's share is the positional correction
+// this sweep's update makes there, h k (|change of the normal impulse| + |change of the tangential impulse|): the
+// solve has converged at the point when it is zero. Measuring changes no result.
 template <bool PAIR>
 __device__ __forceinline__ void contact(int sweep, float gap, const float* n, Held& first, const float* rA,
                                         Held& second, const float* rB, float4& rec, const Soft& soft,
-                                        float k_given = -1.0f) {
+                                        float k_given = -1.0f, unsigned* track = nullptr) {
     const float normal = rec.x;
     const float tangent[3] = {rec.y, rec.z, rec.w};
     const bool holding = normal > 0.0f || dot3(tangent, tangent) > 0.0f;
@@ -270,6 +273,10 @@ __device__ __forceinline__ void contact(int sweep, float gap, const float* n, He
     for (int a = 0; a < 3; a++) rubbed[a] = whole[a] - tangent[a];
     rec = make_float4(total, whole[0], whole[1], whole[2]);
     apply_pair<PAIR>(first, rA, second, rB, rubbed);
+    if (track) {
+        const float moved = soft.h * k * (fabsf(total - normal) + sqrtf(dot3(rubbed, rubbed)));
+        if (moved > 0.0f) atomicMax(track, __float_as_uint(moved));
+    }
 }
 
 // Rolling resistance at one contact with a sphere in it; roll = the accumulated angular impulse (x, y, z).

@@ -143,6 +143,12 @@ struct vxr_box_world {
     int* listed = nullptr;       // [n] on the current wall list
     unsigned* body_colours = nullptr;  // [n] rounds each body has a pair in
     int schedule = 0;
+    int measure = 0;                   // gather each sweep's residual
+    int active_sweeps = 0;             // sweeps a substep runs (at most `sweeps`, the count it was created with)
+    float tolerance = 0.0f;            // > 0: stop a substep's sweeps once the residual is this or less
+    int* used = nullptr;               // [2 substeps] sweeps each half-substep ran
+    int cold = 0;                      // start every step's pair impulses from zero (no carry)
+    unsigned* residual = nullptr;      // [substeps * (2 sweeps + 1)]
     unsigned long long* trace = nullptr;  // phase end times of the last traced step
     int trace_cap = 0, tracing = 0;
     int *colour = nullptr, *inc_count = nullptr, *inc_start = nullptr, *inc_fill = nullptr, *inc_list = nullptr;
@@ -611,6 +617,9 @@ struct SolveArgs {
     int* listed;                   // [n] 1 where the body is on this half-substep's wall list
     const unsigned* body_colours;  // [n] the rounds of each body's pairs, one bit each
     int schedule;                  // 0: a grid barrier after every round; 1: dependency-driven
+    unsigned* residual;            // [substeps * (2 sweeps + 1)] per-sweep residual (f32 bits), null: not measured
+    float tolerance;               // > 0: a substep's solve (relax) sweeps stop once a sweep's residual is this or less
+    int* used;                     // [2 substeps] solve and relax sweeps each substep ran
     int substeps, sweeps, symmetric;
     Params params;
     GridBarrier bar;
@@ -731,7 +740,8 @@ __device__ __forceinline__ void phase_velocities_and_list(const SolveArgs& A, in
 // Boxes.walls :357-416 for one body held in registers: its corners (a sphere: its nearest point) against the six
 // walls. A wall the body is far from, with no impulse held against it, is skipped: its contacts would neither
 // start nor apply. Returns whether anything was applied (the caller then stores the body).
-__device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, int sweep, bool reverse) {
+__device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, int sweep, bool reverse,
+                                         unsigned* track = nullptr) {
     const Params& P = A.params;
     const float margin = P.w[P_MARGIN];
     const float extent[3] = {P.w[P_SX], P.w[P_SY], P.w[P_SZ]};
@@ -769,7 +779,7 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
             const long at = (long)s * WALL_RECORDS + wall * 8;
             if (need) {
                 rec = held ? __ldcg(&A.wall[at]) : rec;
-                contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft);
+                contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft, -1.0f, track);
                 if (sweep != WARM) {
                     __stcg(&A.wall[at], rec);
                     mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
@@ -802,7 +812,7 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
                 if (!(held || (sweep != WARM && gap < margin))) continue;
                 const long at = (long)s * WALL_RECORDS + bit;
                 float4 rec = held ? __ldcg(&A.wall[at]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft);
+                contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft, -1.0f, track);
                 if (sweep != WARM) {
                     __stcg(&A.wall[at], rec);
                     mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
@@ -817,14 +827,15 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
 
 // Boxes.walls :357-416 over the listed bodies, each loaded afresh (its angular velocity from its angular
 // momentum, as the reference's walls kernel loads it).
-__device__ __forceinline__ void phase_walls(const SolveArgs& A, int sweep, bool reverse, int slot) {
+__device__ __forceinline__ void phase_walls(const SolveArgs& A, int sweep, bool reverse, int slot,
+                                            unsigned* track) {
     const int stride = gridDim.x * blockDim.x;
     const int spheres = *(volatile int*)&A.wall_count[2 * slot], boxes = *(volatile int*)&A.wall_count[2 * slot + 1];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < spheres + boxes; k += stride) {
         const int s = A.wall_list[k < spheres ? k : A.n - 1 - (k - spheres)];
         Held box;
         load_held(box, A.b, s);
-        if (walls_of(A, box, s, sweep, reverse)) store_held(box, A.b, s);
+        if (walls_of(A, box, s, sweep, reverse, track)) store_held(box, A.b, s);
     }
 }
 
@@ -833,7 +844,8 @@ __device__ __forceinline__ void phase_walls(const SolveArgs& A, int sweep, bool 
 // fill: the first sweep of a substep's half (positions fixed until the next positions phase): each point's anchors
 // in the world's frame, its gap and its normal's generalised inverse mass are worked out and kept; the later
 // sweeps of that half read them back (the same values the reference works out again every sweep).
-__device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4, int sweep, bool reverse, bool fill) {
+__device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4, int sweep, bool reverse, bool fill,
+                                           unsigned* track) {
     const Params& P = A.params;
     const float4 head = __ldg(&A.pairs.normal[k]);
     const int ia = rec4.x, ib = rec4.y, count = rec4.z;
@@ -880,7 +892,7 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
             rB[0] = pb.x; rB[1] = pb.y; rB[2] = pb.z; kn = pb.w;
         }
         float4 rec = __ldcg(&A.pairs.imp[at]);
-        contact<true>(sweep, gap, n, first, rA, second, rB, rec, soft, kn);
+        contact<true>(sweep, gap, n, first, rA, second, rB, rec, soft, kn, track);
         if (sweep != WARM) __stcg(&A.pairs.imp[at], rec);
         if (anySphere) {
             float radius = second.half[0];
@@ -897,11 +909,12 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
 }
 
 // One round of pairs that share no body (the barrier schedule).
-__device__ __forceinline__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r, bool fill) {
+__device__ __forceinline__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r, bool fill,
+                                            unsigned* track) {
     const int stride = gridDim.x * blockDim.x;
     const int lo = A.round_start[r], hi = A.round_start[r + 1];
     for (int k = lo + blockIdx.x * blockDim.x + threadIdx.x; k < hi; k += stride)
-        solve_pair(A, k, __ldg(&A.pairs.pair[k]), sweep, reverse, fill);
+        solve_pair(A, k, __ldg(&A.pairs.pair[k]), sweep, reverse, fill, track);
 }
 
 // Waits until every listed body has done exactly `want` items of this block. A bounded wait: past the limit it
@@ -966,7 +979,7 @@ __device__ __forceinline__ bool block_of_sweeps(const SolveArgs& A, int first_ki
             const int wantA = w * (degA + lA) + (reverse ? lA + (degA - 1 - rankA) : rankA);
             const int wantB = w * (degB + lB) + (reverse ? lB + (degB - 1 - rankB) : rankB);
             if (!wait_versions(A, rec4.x, wantA, rec4.y, wantB)) return false;
-            solve_pair(A, k, rec4, kind, reverse, w == 0);
+            solve_pair(A, k, rec4, kind, reverse, w == 0, A.residual ? A.residual + sweep0 + w : nullptr);
             __threadfence();
             *(volatile int*)&A.version[rec4.x] = wantA + 1;
             *(volatile int*)&A.version[rec4.y] = wantB + 1;
@@ -978,12 +991,12 @@ __device__ __forceinline__ bool block_of_sweeps(const SolveArgs& A, int first_ki
             if (!wait_versions(A, s, want, -1, 0)) return false;
             Held box;
             load_held(box, A.b, s);
-            if (walls_of(A, box, s, kind, reverse)) store_held(box, A.b, s);
+            if (walls_of(A, box, s, kind, reverse, A.residual ? A.residual + sweep0 + w : nullptr))
+                store_held(box, A.b, s);
             __threadfence();
             *(volatile int*)&A.version[s] = want + 1;
         }
     }
-    (void)sweep0;
     return true;
 }
 
@@ -1003,24 +1016,32 @@ struct Tracer {
 // One sweep (BoxStep.sweep :253-267): every round of pairs, then the walls; backward, the walls first and the
 // rounds last to first.
 __device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsigned int& epoch, int kind, bool reverse,
-                                          int rounds, int slot, bool fill) {
+                                          int rounds, int slot, bool fill, int index) {
+    unsigned* track = A.residual ? A.residual + index : nullptr;
     if (reverse) {
-        phase_walls(A, kind, true, slot);
+        phase_walls(A, kind, true, slot, track);
         if (!grid_sync(A.bar, epoch)) return false;
         tr.mark(TR_WALLS | kind << 4);
     }
     for (int order = 0; order < rounds; order++) {
         const int r = reverse ? rounds - 1 - order : order;
-        phase_round(A, kind, reverse, r, fill);
+        phase_round(A, kind, reverse, r, fill, track);
         if (!grid_sync(A.bar, epoch)) return false;
         tr.mark(TR_ROUND | kind << 4 | r << 8);
     }
     if (!reverse) {
-        phase_walls(A, kind, false, slot);
+        phase_walls(A, kind, false, slot, track);
         if (!grid_sync(A.bar, epoch)) return false;
         tr.mark(TR_WALLS | kind << 4);
     }
     return true;
+}
+
+// Whether a substep's sweeps may stop after sweep `index`: its residual is at or below the tolerance. Every block
+// reads the same word after the grid barrier, so every block decides the same.
+__device__ __forceinline__ bool converged(const SolveArgs& A, int index) {
+    if (!(A.tolerance > 0.0f) || !A.residual) return false;
+    return __uint_as_float(*(volatile unsigned*)&A.residual[index]) <= A.tolerance;
 }
 
 __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(SolveArgs A) {
@@ -1028,30 +1049,50 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(SolveArgs A) {
     Tracer tr{A.trace, A.trace_cap, 0};
     unsigned int epoch = 0;
     tr.mark(TR_START);
+    const int stride = 2 * A.sweeps + 1;  // residual words a substep
     for (int sub = 0; sub < A.substeps; sub++) {
         phase_velocities_and_list(A, 2 * sub);
         if (!grid_sync(A.bar, epoch)) return;
         tr.mark(TR_VELOCITIES);
+        int solved = A.sweeps, relaxed = A.sweeps;
         if (A.schedule == 1) {
-            if (!block_of_sweeps(A, WARM, 1 + A.sweeps, rounds, 2 * sub, 0)) return;
+            if (!block_of_sweeps(A, WARM, 1 + A.sweeps, rounds, 2 * sub, sub * stride)) return;
             if (!grid_sync(A.bar, epoch)) return;
             tr.mark(TR_BLOCK | SOLVE << 4);
         } else {
-            if (!sweep_all(A, tr, epoch, WARM, false, rounds, 2 * sub, true)) return;
-            for (int sw = 0; sw < A.sweeps; sw++)
-                if (!sweep_all(A, tr, epoch, SOLVE, A.symmetric && sw % 2 == 1, rounds, 2 * sub, false)) return;
+            const int base = sub * stride;
+            if (!sweep_all(A, tr, epoch, WARM, false, rounds, 2 * sub, true, base)) return;
+            for (int sw = 0; sw < A.sweeps; sw++) {
+                if (!sweep_all(A, tr, epoch, SOLVE, A.symmetric && sw % 2 == 1, rounds, 2 * sub, false, base + 1 + sw))
+                    return;
+                if (converged(A, base + 1 + sw)) {
+                    solved = sw + 1;
+                    break;
+                }
+            }
         }
         phase_positions(A, 2 * sub + 1);
         if (!grid_sync(A.bar, epoch)) return;
         tr.mark(TR_POSITIONS);
         if (A.schedule == 1) {
-            if (!block_of_sweeps(A, RELAX, A.sweeps, rounds, 2 * sub + 1, 0)) return;
+            if (!block_of_sweeps(A, RELAX, A.sweeps, rounds, 2 * sub + 1, sub * stride + 1 + A.sweeps)) return;
             if (!grid_sync(A.bar, epoch)) return;
             tr.mark(TR_BLOCK | RELAX << 4);
         } else {
-            for (int sw = 0; sw < A.sweeps; sw++)
-                if (!sweep_all(A, tr, epoch, RELAX, A.symmetric && sw % 2 == 1, rounds, 2 * sub + 1, sw == 0))
+            const int base = sub * stride + 1 + A.sweeps;
+            for (int sw = 0; sw < A.sweeps; sw++) {
+                if (!sweep_all(A, tr, epoch, RELAX, A.symmetric && sw % 2 == 1, rounds, 2 * sub + 1, sw == 0,
+                               base + sw))
                     return;
+                if (converged(A, base + sw)) {
+                    relaxed = sw + 1;
+                    break;
+                }
+            }
+        }
+        if (A.used && blockIdx.x == 0 && threadIdx.x == 0) {
+            A.used[2 * sub] = solved;
+            A.used[2 * sub + 1] = relaxed;
         }
     }
     if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) A.counters->trace_len = tr.len;
@@ -1192,8 +1233,13 @@ int enqueue_step(vxr_box_world* w) {
         k_touch_list<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->cand_start, w->cand_b, w->man.head,
                                                                 now.tstart, w->ta, now.tb, w->tcand, w->counters);
         const int tblocks = w->sms * 4;
-        k_carry<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->ta, now.tb, w->tcand, w->man, was, w->b.half,
-                                            w->imp_t, w->impr_t);
+        if (w->cold) {  // the plain solver from nothing: no impulse carried from the step before
+            VXR_CUDA(cudaMemsetAsync(w->imp_t, 0, sizeof(float4) * (size_t)w->cap * MOST_POINTS, st));
+            VXR_CUDA(cudaMemsetAsync(w->impr_t, 0, sizeof(float4) * (size_t)w->cap * MOST_POINTS, st));
+        } else {
+            k_carry<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->ta, now.tb, w->tcand, w->man, was, w->b.half,
+                                                w->imp_t, w->impr_t);
+        }
         LAUNCHED(1 + 1 + 3 + 1 + 1);  // collide, touch count, scan, touch list, carry
         if (int rc = mark(w, 2)) return rc;
         // colouring
@@ -1241,11 +1287,16 @@ int enqueue_step(vxr_box_world* w) {
         A.listed = w->listed;
         A.body_colours = w->body_colours;
         A.schedule = w->schedule;
+        A.residual = w->measure ? w->residual : nullptr;
+        if (w->measure)
+            VXR_CUDA(cudaMemsetAsync(w->residual, 0, sizeof(unsigned) * w->substeps * (2 * w->active_sweeps + 1), st));
         A.pairs = now;
         A.round_start = w->round_start;
         A.counters = w->counters;
         A.substeps = w->substeps;
-        A.sweeps = w->sweeps;
+        A.sweeps = w->active_sweeps;
+        A.tolerance = w->measure ? w->tolerance : 0.0f;
+        A.used = w->used;
         A.symmetric = w->symmetric;
         A.params = w->params;
         A.bar = barrier_of(w);
@@ -1405,6 +1456,7 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     w->n = cfg->bodies;
     w->substeps = cfg->substeps;
     w->sweeps = cfg->sweeps;
+    w->active_sweeps = cfg->sweeps;
     w->symmetric = cfg->symmetric ? 1 : 0;
     w->schedule = cfg->schedule == 1 ? 1 : 0;
     w->device = cfg->device;
@@ -1462,6 +1514,8 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     rc |= alloc(w, &w->version, n);
     rc |= alloc(w, &w->listed, n);
     rc |= alloc(w, &w->body_colours, n);
+    rc |= alloc(w, &w->residual, (size_t)w->substeps * (2 * w->sweeps + 1));
+    rc |= alloc(w, &w->used, 2 * (size_t)w->substeps);
     rc |= alloc(w, &w->round_fill, BUCKETS);
     if (w->has_grid) {
         rc |= alloc(w, &w->keys, n);
@@ -1847,6 +1901,26 @@ int32_t vxr_box_colour_waves(vxr_box_world* w) {
 }
 
 long long vxr_box_launches(vxr_box_world* w) { return w ? w->launches : -1; }
+
+int32_t vxr_box_measure(vxr_box_world* w, int32_t residual, int32_t cold_start, int32_t sweeps, float tolerance) {
+    if (!w || sweeps < 0 || sweeps > w->sweeps || !(tolerance >= 0.0f)) return VXR_EINVAL;
+    w->measure = residual ? 1 : 0;
+    w->cold = cold_start ? 1 : 0;
+    w->active_sweeps = sweeps > 0 ? sweeps : w->sweeps;
+    w->tolerance = tolerance;
+    return VXR_OK;
+}
+
+int32_t vxr_box_residuals(vxr_box_world* w, float* out, int32_t capacity, int32_t* used) {
+    if (!w) return -VXR_EINVAL;
+    const int count = w->substeps * (2 * w->active_sweeps + 1);
+    if (!out && !used) return count;
+    if (out && capacity < count) return -VXR_ECAPACITY;
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    if (out) VXR_CUDA(cudaMemcpy(out, w->residual, sizeof(float) * count, cudaMemcpyDeviceToHost));
+    if (used) VXR_CUDA(cudaMemcpy(used, w->used, sizeof(int) * 2 * w->substeps, cudaMemcpyDeviceToHost));
+    return count;
+}
 
 int32_t vxr_box_profile(vxr_box_world* w, int32_t enable, double* phase_ms4) {
     if (!w) return VXR_EINVAL;

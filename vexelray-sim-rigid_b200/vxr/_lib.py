@@ -21,7 +21,8 @@ SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_c
            "vxr_box_error", "vxr_box_start", "vxr_box_load_state", "vxr_box_params", "vxr_box_step",
            "vxr_box_step_async", "vxr_box_sync", "vxr_box_stream", "vxr_box_state", "vxr_box_read_shown",
            "vxr_box_touching", "vxr_box_candidates", "vxr_box_walls", "vxr_box_colour_waves", "vxr_collide",
-           "vxr_box_launches", "vxr_box_profile", "vxr_box_activity", "vxr_box_trace", "vxr_box_broadphase_static"]
+           "vxr_box_launches", "vxr_box_profile", "vxr_box_activity", "vxr_box_trace", "vxr_box_broadphase_static",
+           "vxr_box_measure", "vxr_box_residuals"]
 
 
 class VxrError(RuntimeError):
@@ -102,6 +103,10 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_activity.restype = i32
         L.vxr_box_trace.argtypes = [vp, i32, vp, i32]
         L.vxr_box_trace.restype = i32
+        L.vxr_box_measure.argtypes = [vp, i32, i32, i32, ctypes.c_float]
+        L.vxr_box_measure.restype = i32
+        L.vxr_box_residuals.argtypes = [vp, vp, i32, vp]
+        L.vxr_box_residuals.restype = i32
         L.vxr_box_broadphase_static.argtypes = [i32, vp, Grid, i32, f32, vp, vp, i32, vp, vp]
         L.vxr_box_broadphase_static.restype = i32
         L.vxr_collide.argtypes = [i32, vp, vp, i32, vp, vp]

@@ -67,6 +67,8 @@ class BoxSimulation:
         if not self.h:
             raise VxrError(status.value, "vxr_box_create failed")
         self.n = bodies
+        self.substeps = substeps
+        self.sweeps = sweeps
         self.grid = grid
         self._last = Report(0, 0, 0, 0, 0)
 
@@ -222,6 +224,24 @@ class BoxSimulation:
         raw = out[:n].astype(np.uint64)
         return np.stack([(raw >> np.uint64(48)).astype(np.int64),
                          (raw & np.uint64((1 << 48) - 1)).astype(np.int64)], axis=1)
+
+    def measure(self, residual: bool = True, cold_start: bool = False, sweeps: int = 0, tolerance: float = 0.0):
+        """Gather each sweep's residual; start pair impulses from zero (no warm start); run `sweeps` sweeps (0: the
+        created count); stop a substep's sweeps once the residual is at or below `tolerance` (0: never)."""
+        self._check(self.L.vxr_box_measure(self.h, int(bool(residual)), int(bool(cold_start)), int(sweeps),
+                                           float(tolerance)))
+        self.active_sweeps = sweeps or self.sweeps
+
+    def residuals(self):
+        """The last step's per-sweep residuals, shape (substeps, 2 sweeps + 1) (warm, solve..., relax...), and the
+        sweeps each half-substep ran, shape (substeps, 2)."""
+        count = self.L.vxr_box_residuals(self.h, None, 0, None)
+        out = np.zeros(count, np.float32)
+        used = np.zeros(2 * self.substeps, np.int32)
+        got = self.L.vxr_box_residuals(self.h, ptr(out), count, ptr(used))
+        if got < 0:
+            raise VxrError(-got, self.error())
+        return out.reshape(self.substeps, -1), used.reshape(self.substeps, 2)
 
     def error(self) -> str:
         return self.L.vxr_box_error(self.h).decode() if self.h else ""
