@@ -216,6 +216,107 @@ int32_t vxr_box_broadphase_static(int32_t bodies, const float* const* fields11, 
                                   float margin, int32_t* first_out, int32_t* second_out, int32_t capacity,
                                   int32_t* result3, void* stream);
 
+/* ---- The sphere package: XPBD spheres (core/sphere/) ------------------------------------------------------------
+ * The reference's SphereSimulation (gui/SphereSimulation.java:33-295) over SphereStep and SphereStepper. A call of
+ * steps is one persistent kernel: every pass of every substep, and Gauss-Seidel's run until done with the
+ * stepper's batch sizing, happen on the device with no host wait between them. */
+
+#define VXR_SPHERE_PARAM_COUNT 13       /* core/sphere/Spheres.java:141 */
+#define VXR_SPHERE_SHOWN_STRIDE 40      /* core/sphere/Spheres.java:1654 */
+#define VXR_SPHERE_FIELDS 24            /* core/sphere/Spheres.java:240-241 */
+#define VXR_MOST_LISTED_SPHERES 46340   /* core/sphere/Spheres.java:787 */
+#define VXR_SPHERE_ONE_BLOCK 8192       /* scenes up to this many spheres run as one block of the GPU */
+/* How a pass solves (SphereStep.Solve, core/sphere/SphereStep.java:37-43). */
+#define VXR_JACOBI 0
+#define VXR_GAUSS_SEIDEL_BY_CONTACT 1   /* run until every contact is solved (SphereStepper) */
+#define VXR_FIXED_ROUNDS 2              /* the same with `rounds` rounds a pass and no friction rounds (step()) */
+
+typedef struct vxr_sphere_world vxr_sphere_world;
+
+/* SphereStep(spheres, substeps, iterations, grid, solve, rounds, contactsPerSphere)
+ * (core/sphere/SphereStep.java:115-131). */
+typedef struct {
+    int32_t spheres;
+    int32_t substeps;
+    int32_t iterations;
+    int32_t solve;                /* VXR_JACOBI, VXR_GAUSS_SEIDEL_BY_CONTACT or VXR_FIXED_ROUNDS */
+    int32_t rounds;               /* VXR_FIXED_ROUNDS: rounds a pass (SphereStep.ROUNDS = 32) */
+    int32_t contacts_per_sphere;  /* list places a sphere; 0 = 6 (SphereStep.CONTACTS_PER_SPHERE) */
+    vxr_grid grid;                /* nx = 0: every pair (Jacobi only) */
+    int32_t device;
+    int32_t blocks;               /* 0: one block up to VXR_SPHERE_ONE_BLOCK spheres, else enough for the list */
+} vxr_sphere_config;
+
+/* SphereStepper.Report(waits, rounds, mostRounds, unlisted) (core/sphere/SphereStepper.java:40-47) of the call's
+ * last step, and the same summed over the call's steps (most rounds: the largest). `waits` counts the batches of
+ * rounds the reference's host would have waited for; here no host wait happens inside a call. */
+typedef struct {
+    int32_t waits, rounds, most_rounds, unlisted;
+    int64_t waits_total, rounds_total;
+    int32_t most_rounds_total;
+    int32_t status;
+    int64_t unlisted_total;
+    int32_t listed;               /* the last substep's list length (contactCount[LISTED]) */
+    int32_t pad;
+} vxr_sphere_report;
+
+/* Spheres.params (core/sphere/Spheres.java:212-228): 13 float words as int bits into out13; VXR_EINVAL where the
+ * reference throws IllegalArgumentException. */
+int32_t vxr_sphere_make_params(double h, double gx, double gy, double gz, double sx, double sy, double sz,
+                               double omega, int32_t averaged, double restitution, double mu_static,
+                               double mu_kinetic, double mu_rolling, int32_t* out13);
+/* SphereGrid.covering(sx, sy, sz, widest) (core/sphere/SphereGrid.java:21-26). */
+int32_t vxr_sphere_make_grid(double sx, double sy, double sz, double widest, vxr_grid* out);
+
+/* new SphereStep(...) + new SphereSimulation(context, step) (gui/SphereSimulation.java:62-97). NULL on failure,
+ * with the reason in *status. */
+vxr_sphere_world* vxr_sphere_create(const vxr_sphere_config* config, int32_t* status);
+/* SphereSimulation.close() (gui/SphereSimulation.java:288-295). */
+void vxr_sphere_destroy(vxr_sphere_world* world);
+const char* vxr_sphere_error(const vxr_sphere_world* world);
+
+/* SphereSimulation.start(x, y, z, u, v, w, r, im, params) (gui/SphereSimulation.java:154-178): every buffer cleared,
+ * these written, every orientation the identity, the picture's before and after both this state; friction on
+ * when the parameters have any (Spheres.rubs). */
+int32_t vxr_sphere_start(vxr_sphere_world* world, const float* x, const float* y, const float* z, const float* u,
+                         const float* v, const float* w, const float* r, const float* im, const int32_t* params13);
+/* The test fixture's start (ctest/sphere/Scene.java:122-158): every buffer cleared, then any of the 24 fields
+ * (Spheres.SPHERE order: x y z u v w r im cx cy cz dx dy dz ax ay az tx ty tz qx qy qz qw; a null entry leaves it
+ * zero, qw one) and the parameters; the picture's buffer zero. */
+int32_t vxr_sphere_load_state(vxr_sphere_world* world, const float* const* fields24, const int32_t* params13);
+/* SphereSimulation.params(int[]) (gui/SphereSimulation.java:181-184): from the next step on. */
+int32_t vxr_sphere_params(vxr_sphere_world* world, const int32_t* params13);
+/* SphereStepper.friction(boolean) (core/sphere/SphereStepper.java:106-112): whether passes run friction rounds. */
+int32_t vxr_sphere_friction(vxr_sphere_world* world, int32_t on);
+
+/* SphereSimulation.stepAndWait() (gui/SphereSimulation.java:196-199): `steps` steps, waiting for them. */
+int32_t vxr_sphere_step(vxr_sphere_world* world, int32_t steps, vxr_sphere_report* report);
+/* SphereSimulation.step() (gui/SphereSimulation.java:191-193): enqueued without waiting; vxr_sphere_sync waits. */
+int32_t vxr_sphere_step_async(vxr_sphere_world* world, int32_t steps);
+int32_t vxr_sphere_sync(vxr_sphere_world* world, vxr_sphere_report* report);
+/* The world's cudaStream_t. */
+void* vxr_sphere_stream(vxr_sphere_world* world);
+
+/* SphereSimulation.state() (gui/SphereSimulation.java:256-260): x y z u v w ax ay az into out9 (null entries
+ * skipped). */
+int32_t vxr_sphere_state(vxr_sphere_world* world, float* const* out9);
+/* Any one of the 24 fields (Scene.floats, ctest/sphere/Scene.java:207-210). */
+int32_t vxr_sphere_field(vxr_sphere_world* world, int32_t field, float* out);
+/* SphereSimulation.readShown() (gui/SphereSimulation.java:266-268): 40 floats a sphere. */
+int32_t vxr_sphere_read_shown(vxr_sphere_world* world, float* out);
+/* The last substep's contact list in list order, for inspection: pairs (lower, higher), the pass that solved each,
+ * and its 7 impulse words (normal, tangential 3, angular 3); *listed receives its length (the first `capacity`
+ * entries are written). */
+int32_t vxr_sphere_contacts(vxr_sphere_world* world, int32_t* ab, int32_t* done, float* impulses7,
+                            int32_t capacity, int32_t* listed);
+/* The walls' impulses, 21 floats a sphere (Spheres.WALL_IMPULSE_WORDS, core/sphere/Spheres.java:952). */
+int32_t vxr_sphere_walls(vxr_sphere_world* world, float* out);
+/* contactCount: listed, missed, longest (core/sphere/Spheres.java:797-804). */
+int32_t vxr_sphere_counts(vxr_sphere_world* world, int32_t* out3);
+/* Blocks the world's kernel runs on, and kernels it has launched. */
+int32_t vxr_sphere_blocks(const vxr_sphere_world* world);
+int64_t vxr_sphere_launches(const vxr_sphere_world* world);
+
 #ifdef __cplusplus
 }
 #endif

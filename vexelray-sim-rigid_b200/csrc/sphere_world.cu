@@ -1,0 +1,1543 @@
+// The sphere package on the GPU: XPBD spheres in a walled box, solved by Jacobi or by Gauss-Seidel over a contact
+// list run until every contact is solved, with warm starts, friction, rolling resistance, walls, restitution and the
+// picture's pressing. The reference builds it as IR kernels, one dispatch each, driven from the host with a wait per
+// batch of rounds (core = vexelray-sim-rigid-core/src/main/java/dev/vexelray/sim/rigid/; core/sphere/Spheres.java,
+// SphereStep.java, SphereStepper.java). Here a whole call of steps is ONE persistent kernel: every pass of every
+// substep runs in order inside it, the until-done loop and its batch sizing included, with a barrier between passes
+// (the block's own barrier when the scene fits one block, a bounded grid barrier when it does not).
+//
+// Each pass keeps the reference's arithmetic in its association order (build with --fmad=false and IEEE division
+// and square root), so a pass computes the reference's f32 values. Two things are made deterministic that the
+// reference leaves to the device: the sort is stable (within a cell, ascending index), and the contact list is
+// made by a count, a scan and a fill in sphere order (the order a serial run of the reference's atomic append
+// gives), so the list, its chains and every later pass are reproducible bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "grid_sync.cuh"
+#include "vxr.h"
+
+namespace vxr {
+namespace sph {
+
+// Spheres.params words (core/sphere/Spheres.java:141-155).
+enum { H = 0, GX, GY, GZ, SX, SY, SZ, OMEGA, AVERAGED, RESTITUTION, MU_STATIC, MU_KINETIC, MU_ROLLING, P_COUNT };
+constexpr float COINCIDENT = 1e-12f;   // Spheres.java:157
+constexpr float LIST_MARGIN = 0.02f;   // Spheres.java:795
+constexpr float INERTIA = 0.4f;        // Spheres.java:247
+constexpr int MOST_KEPT = 32;          // Spheres.java:944
+constexpr int CYCLE = 48, BATCH = 8;   // SphereStep.java:53-59
+constexpr int SHRINK_AFTER = 120;      // SphereStepper.java:53
+constexpr int SHOWN = 40, PRESSED_BEFORE = 8, PRESSED_AFTER = 20, TURNED_BEFORE = 32, TURNED_AFTER = 36;
+constexpr int LISTED = 0, MISSED = 1, LONGEST = 2;
+constexpr int THREADS = 512;
+
+struct SParams {
+    float w[P_COUNT];
+};
+
+// Per-sphere state, seven float4 arrays (112 B a sphere). The inverse mass rides with the constraint moves and the
+// radius with the position, so a parting contact reads two float4 a sphere.
+struct State {
+    float4* pos;   // x y z r
+    float4* disp;  // dx dy dz im: what the constraints moved it this substep, and its inverse mass
+    float4* turn;  // tx ty tz -: what the constraints turned it this substep
+    float4* vel;   // u v w -
+    float4* spin;  // ax ay az -: angular velocity
+    float4* q;     // orientation qx qy qz qw
+    float4* cvel;  // cx cy cz -: Jacobi's move, then the velocity before the substep's velocity pass
+};
+
+// One generation of the contact list: this substep's, or the one kept from the substep before.
+struct ListGen {
+    int2* pair;    // [cap] lower sphere, higher sphere
+    int* done;     // [cap] the pass that solved it
+    int* next;     // [cap] the lower sphere's previous contact, or -1
+    float4* imp;   // [2 cap] (normal, p), (q, -): what it has taken this substep
+    int* head;     // [n] the lower sphere's last contact, or -1
+};
+
+struct Counts {
+    int count[3];     // LISTED, MISSED, LONGEST (Spheres.CONTACT_COUNT_WORDS)
+    int open[2];      // Spheres.OPEN_WORDS
+    int last[4];      // the last step's report: waits, rounds, most rounds, unlisted
+    long long total[4];  // summed over the call (most rounds: the largest)
+    int status;
+    int abort;
+    unsigned int bar_count;
+    unsigned int bar_gen;
+    int cur;          // the generation holding the current list
+    int rounds_at;    // the rounds a pass had run when it was given up (status ST_ROUNDS)
+    int pad[2];
+};
+
+struct Kernel {
+    int n, cap, substeps, iterations, solve, rounds, gridded, nx, ny, nz, cells, friction, steps;
+    float cell;
+    SParams p;
+    State s;
+    float4* wall;      // [6 n]: per axis, (normal, p) and (q, -)
+    float* shown;      // [40 n]
+    int* keys;         // [n]
+    int* order;        // [n]
+    int* cell_count;   // [cells]
+    int* cell_start;   // [cells + 1]
+    int* claims;       // [3 n]
+    int* list_count;   // [n]
+    int* list_start;   // [n + 1]
+    ListGen gen[2];
+    Counts* counts;
+    int* opening;      // [iterations] the rounds each pass's opening batch runs (SphereStepper.opening)
+    int* enough;       // [iterations]
+    GridBarrier bar;
+};
+
+__device__ __forceinline__ float dotf(const float* x, const float* y) {
+    return x[0] * y[0] + (x[1] * y[1] + x[2] * y[2]);
+}
+
+__device__ __forceinline__ void crossf(const float* x, const float* y, float* z) {
+    z[0] = x[1] * y[2] - x[2] * y[1];
+    z[1] = x[2] * y[0] - x[0] * y[2];
+    z[2] = x[0] * y[1] - x[1] * y[0];
+}
+
+__device__ __forceinline__ float get(const float4& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// Spheres.turn :1468-1493: q + 1/2 (angle, 0) (x) q, normalised.
+__device__ __forceinline__ float4 turned(float4 was, const float* angle) {
+    const float a0 = 0.5f * angle[0], a1 = 0.5f * angle[1], a2 = 0.5f * angle[2];
+    float4 now;
+    now.x = was.x + (a0 * was.w + (a1 * was.z - a2 * was.y));
+    now.y = was.y + (a1 * was.w + (a2 * was.x - a0 * was.z));
+    now.z = was.z + (a2 * was.w + (a0 * was.y - a1 * was.x));
+    now.w = was.w - (a0 * was.x + (a1 * was.y + a2 * was.z));
+    const float len2 = (now.x * now.x + now.y * now.y) + (now.z * now.z + now.w * now.w);
+    const float inverse = 1.0f / sqrtf(fmaxf(len2, 1e-30f));
+    return make_float4(now.x * inverse, now.y * inverse, now.z * inverse, now.w * inverse);
+}
+
+// A sphere as a pass holds it: loaded once, worked on in registers, stored once (Spheres.Held :542-569).
+struct Held {
+    int s;
+    float at[3], displaced[3], turned[3];
+    float r, im;
+};
+
+__device__ __forceinline__ Held load(const State& S, int s) {
+    Held h;
+    h.s = s;
+    const float4 p = S.pos[s], d = S.disp[s], t = S.turn[s];
+    h.at[0] = p.x, h.at[1] = p.y, h.at[2] = p.z, h.r = p.w;
+    h.displaced[0] = d.x, h.displaced[1] = d.y, h.displaced[2] = d.z, h.im = d.w;
+    h.turned[0] = t.x, h.turned[1] = t.y, h.turned[2] = t.z;
+    return h;
+}
+
+__device__ __forceinline__ void store(const State& S, const Held& h) {
+    S.pos[h.s] = make_float4(h.at[0], h.at[1], h.at[2], h.r);
+    S.disp[h.s] = make_float4(h.displaced[0], h.displaced[1], h.displaced[2], h.im);
+    S.turn[h.s] = make_float4(h.turned[0], h.turned[1], h.turned[2], 0.0f);
+}
+
+// Spheres.Impulse :490-522: normal, p (3), q (3), two float4 in memory.
+struct Impulse {
+    float normal, p[3], q[3];
+};
+
+__device__ __forceinline__ Impulse load_impulse(const float4* at) {
+    const float4 a = at[0], b = at[1];
+    Impulse t;
+    t.normal = a.x, t.p[0] = a.y, t.p[1] = a.z, t.p[2] = a.w;
+    t.q[0] = b.x, t.q[1] = b.y, t.q[2] = b.z;
+    return t;
+}
+
+__device__ __forceinline__ void store_impulse(float4* at, const Impulse& t) {
+    at[0] = make_float4(t.normal, t.p[0], t.p[1], t.p[2]);
+    at[1] = make_float4(t.q[0], t.q[1], t.q[2], 0.0f);
+}
+
+__device__ __forceinline__ void clear_impulse(Impulse& t) {
+    t.normal = 0.0f;
+    for (int k = 0; k < 3; k++) t.p[k] = t.q[k] = 0.0f;
+}
+
+__device__ __forceinline__ float turns_per_impulse(float wv, float lever, float radius) {
+    return (wv * lever) / (INERTIA * (radius * radius));
+}
+
+__device__ __forceinline__ float rubbing_of(const SParams& P) {
+    return P.w[MU_STATIC] + (P.w[MU_KINETIC] + P.w[MU_ROLLING]);
+}
+
+// Spheres.rub :662-677 (o null: a wall).
+__device__ __forceinline__ void rub(Held& a, float wa, float turnsA, Held* o, float wo, float turnsO, const float* n,
+                                    const float* p) {
+    float np[3];
+    crossf(n, p, np);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float move = wa * p[k];
+        a.at[k] = a.at[k] + move;
+        a.displaced[k] = a.displaced[k] + move;
+        a.turned[k] = a.turned[k] - turnsA * np[k];
+        if (o) {
+            const float back = wo * p[k];
+            o->at[k] = o->at[k] - back;
+            o->displaced[k] = o->displaced[k] - back;
+            o->turned[k] = o->turned[k] - turnsO * np[k];
+        }
+    }
+}
+
+// Spheres.contactTravel :751-766.
+__device__ __forceinline__ void contact_travel(const float4& vel, const float4& spin, const Held& s, float h,
+                                               const float* n, float lever, int side, float* travel) {
+    float turn[3], turnN[3];
+    turn[0] = h * spin.x + s.turned[0];
+    turn[1] = h * spin.y + s.turned[1];
+    turn[2] = h * spin.z + s.turned[2];
+    crossf(turn, n, turnN);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float centre = h * get(vel, k) + s.displaced[k];
+        const float spun = lever * turnN[k];
+        travel[k] = side > 0 ? centre + spun : centre - spun;
+    }
+}
+
+// Spheres.friction :595-654 (o null: a wall).
+__device__ __forceinline__ void friction(const SParams& P, Held& a, const float4& velA, const float4& spinA, float wa,
+                                         float leverA, Held* o, const float4& velO, const float4& spinO, float wo,
+                                         float leverO, const float* n, Impulse& taken) {
+    const float muS = P.w[MU_STATIC], muK = P.w[MU_KINETIC];
+    const float lambdaN = taken.normal;
+    if (!(muS + muK > 0.0f)) return;
+    const float h = P.w[H];
+    const float la = leverA;
+    float slip[3];
+    contact_travel(velA, spinA, a, h, n, la, -1, slip);
+    const float ia = wa;
+    const float leverOverIa = turns_per_impulse(ia, la, a.r);
+    float weight = ia + leverOverIa * la;
+    float leverOverIo = 0.0f, io = 0.0f;
+    if (o) {
+        io = wo;
+        const float lo = leverO;
+        float other[3];
+        contact_travel(velO, spinO, *o, h, n, lo, 1, other);
+#pragma unroll
+        for (int k = 0; k < 3; k++) slip[k] = slip[k] - other[k];
+        leverOverIo = turns_per_impulse(io, lo, o->r);
+        weight = weight + (io + leverOverIo * lo);
+    }
+    const float along = dotf(slip, n);
+    float tangent[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) tangent[k] = slip[k] - along * n[k];
+    if (!(weight > 0.0f)) return;
+    const float takenAlong = dotf(taken.p, n);
+    float before[3], whole[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        before[k] = taken.p[k] - takenAlong * n[k];
+        whole[k] = before[k] - tangent[k] / weight;
+    }
+    const float size2 = dotf(whole, whole);
+    const float holds = muS * lambdaN;
+    if (size2 > holds * holds) {
+        const float cut = fminf(1.0f, (muK * lambdaN) / sqrtf(size2));
+#pragma unroll
+        for (int k = 0; k < 3; k++) whole[k] = whole[k] * cut;
+    }
+    float p[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        p[k] = whole[k] - before[k];
+        taken.p[k] = whole[k];
+    }
+    rub(a, ia, leverOverIa, o, io, leverOverIo, n, p);
+}
+
+// Spheres.roll :699-741 (o null: a wall).
+__device__ __forceinline__ void roll(const SParams& P, Held& a, const float4& spinA, float wa, Held* o,
+                                     const float4& spinO, float wo, float reach, Impulse& taken) {
+    const float muR = P.w[MU_ROLLING];
+    const float h = P.w[H];
+    const float ra = a.r;
+    const float ia = wa / (INERTIA * (ra * ra));
+    float inverse = ia;
+    float io = 0.0f;
+    float against[3];
+    against[0] = h * spinA.x + a.turned[0];
+    against[1] = h * spinA.y + a.turned[1];
+    against[2] = h * spinA.z + a.turned[2];
+    if (o) {
+        const float ro = o->r;
+        io = wo / (INERTIA * (ro * ro));
+        inverse = inverse + io;
+        against[0] = against[0] - (h * spinO.x + o->turned[0]);
+        against[1] = against[1] - (h * spinO.y + o->turned[1]);
+        against[2] = against[2] - (h * spinO.z + o->turned[2]);
+    }
+    if (!(inverse > 0.0f)) return;
+    float whole[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) whole[k] = taken.q[k] - against[k] / inverse;
+    const float size2 = dotf(whole, whole);
+    const float holds = (muR * reach) * taken.normal;
+    if (size2 > holds * holds) {
+        const float cut = fminf(1.0f, holds / sqrtf(size2));
+#pragma unroll
+        for (int k = 0; k < 3; k++) whole[k] = whole[k] * cut;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float change = whole[k] - taken.q[k];
+        taken.q[k] = whole[k];
+        a.turned[k] = a.turned[k] + ia * change;
+        if (o) o->turned[k] = o->turned[k] - io * change;
+    }
+}
+
+// Spheres.warm :448-481.
+__device__ __forceinline__ void warm(Held& a, float wa, Held& o, float wo, const float* d, float d2, float reach,
+                                     Impulse& taken) {
+    const float dist = sqrtf(d2);
+    float n[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) n[k] = d[k] / dist;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float push = taken.normal * n[k];
+        const float ma = push * wa;
+        const float mo = -(push * wo);
+        a.at[k] = a.at[k] + ma;
+        o.at[k] = o.at[k] + mo;
+        a.displaced[k] = a.displaced[k] + ma;
+        o.displaced[k] = o.displaced[k] + mo;
+    }
+    const float along = dotf(taken.p, n);
+#pragma unroll
+    for (int k = 0; k < 3; k++) taken.p[k] = taken.p[k] - along * n[k];
+    const float share = dist / reach;
+    const float ra = a.r, ro = o.r;
+    const float turnsA = turns_per_impulse(wa, share * ra, ra);
+    const float turnsO = turns_per_impulse(wo, share * ro, ro);
+    rub(a, wa, turnsA, &o, wo, turnsO, n, taken.p);
+    const float ia = wa / (INERTIA * (ra * ra));
+    const float io = wo / (INERTIA * (ro * ro));
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        a.turned[k] = a.turned[k] + ia * taken.q[k];
+        o.turned[k] = o.turned[k] - io * taken.q[k];
+    }
+}
+
+// Spheres.contact :369-439: contact c of spheres ai and oi, parting (rubs 0) or rubbing.
+__device__ void contact(const Kernel& K, float4* impulse, int ai, int oi, int pass, int rubs) {
+    const State& S = K.s;
+    Held ha = load(S, ai), ho = load(S, oi);
+    float d[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) d[k] = ha.at[k] - ho.at[k];
+    const float d2 = dotf(d, d);
+    const float reach = ha.r + ho.r;
+    const float wa = ha.im, wo = ho.im;
+    const float wsum = wa + wo;
+    const float listed = reach * (1.0f + LIST_MARGIN);
+    if (!(d2 < listed * listed)) return;
+    if (!(d2 > COINCIDENT)) return;
+    if (!(wsum > 0.0f)) return;
+    Impulse taken = load_impulse(impulse);
+    if (rubs == 0) {
+        if (pass == 1) {
+            if (rubbing_of(K.p) > 0.0f) warm(ha, wa, ho, wo, d, d2, reach, taken);
+            else clear_impulse(taken);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; k++) d[k] = ha.at[k] - ho.at[k];
+        const float dist = sqrtf(fmaxf(dotf(d, d), COINCIDENT));
+        const float depth = fmaxf(-(taken.normal * wsum), K.p.w[OMEGA] * (reach - dist));
+        taken.normal = taken.normal + depth / wsum;
+        const float kk = depth / (dist * wsum);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float step = kk * d[k];
+            const float ma = step * wa;
+            const float mo = -(step * wo);
+            ha.at[k] = ha.at[k] + ma;
+            ho.at[k] = ho.at[k] + mo;
+            ha.displaced[k] = ha.displaced[k] + ma;
+            ho.displaced[k] = ho.displaced[k] + mo;
+        }
+    } else {
+        const float dist = sqrtf(d2);
+        float n[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) n[k] = d[k] / dist;
+        const float share = dist / reach;
+        const float pairRadius = (ha.r * ho.r) / reach;
+        const float4 velA = S.vel[ai], velO = S.vel[oi], spinA = S.spin[ai], spinO = S.spin[oi];
+        roll(K.p, ha, spinA, wa, &ho, spinO, wo, pairRadius, taken);
+        friction(K.p, ha, velA, spinA, wa, share * ha.r, &ho, velO, spinO, wo, share * ho.r, n, taken);
+    }
+    store_impulse(impulse, taken);
+    store(S, ha);
+    store(S, ho);
+}
+
+// Spheres.priority :1166-1168.
+__device__ __forceinline__ int priority(int pair, int g) {
+    return (int)(((unsigned)pair * 0x9E3779B1u + (unsigned)g * 0x632BE5ABu) & 0x7FFFFFFFu);
+}
+
+// Cell of a centre (Spheres.bin :1308-1323).
+__device__ __forceinline__ int cell_key(const Kernel& K, float x, float y, float z) {
+    const int c0 = (int)fmaxf(0.0f, fminf((float)(K.nx - 1), floorf(x / K.cell)));
+    const int c1 = (int)fmaxf(0.0f, fminf((float)(K.ny - 1), floorf(y / K.cell)));
+    const int c2 = (int)fmaxf(0.0f, fminf((float)(K.nz - 1), floorf(z / K.cell)));
+    return c0 + K.nx * (c1 + K.ny * c2);
+}
+
+// Spheres.around :1207-1229: every sphere of s's cell and the 26 around it, each cell in the sort's order; with no
+// grid, every sphere in index order.
+template <typename Visit>
+__device__ __forceinline__ void around(const Kernel& K, int s, Visit visit) {
+    if (!K.gridded) {
+        for (int o = 0; o < K.n; o++) visit(o);
+        return;
+    }
+    const int key = K.keys[s];
+    const int ix = key % K.nx, iy = (key / K.nx) % K.ny, iz = key / (K.nx * K.ny);
+    for (int nn = 0; nn < 27; nn++) {
+        const int jx = ix + (nn % 3 - 1), jy = iy + ((nn / 3) % 3 - 1), jz = iz + (nn / 9 - 1);
+        if (!(jx >= 0 && jx < K.nx && jy >= 0 && jy < K.ny && jz >= 0 && jz < K.nz)) continue;
+        const int cell = jx + K.nx * (jy + K.ny * jz);
+        const int end = K.cell_start[cell + 1];
+        for (int k = K.cell_start[cell]; k < end; k++) visit(K.order[k]);
+    }
+}
+
+// --- per-sphere passes ---------------------------------------------------------------------------------------
+
+// Spheres.predict :269-295.
+__device__ __forceinline__ void predict(const Kernel& K, int s) {
+    const State& S = K.s;
+    if (!(S.disp[s].w > 0.0f)) return;
+    const float h = K.p.w[H];
+    float4 p = S.pos[s], v = S.vel[s];
+    const float4 w = S.spin[s];
+    v.x = v.x + h * K.p.w[GX];
+    p.x = p.x + h * v.x;
+    v.y = v.y + h * K.p.w[GY];
+    p.y = p.y + h * v.y;
+    v.z = v.z + h * K.p.w[GZ];
+    p.z = p.z + h * v.z;
+    S.vel[s] = v;
+    S.pos[s] = p;
+    const float angle[3] = {h * w.x, h * w.y, h * w.z};
+    S.q[s] = turned(S.q[s], angle);
+}
+
+// Spheres.warmWalls :890-939.
+__device__ __forceinline__ void warm_walls(const Kernel& K, int s) {
+    const State& S = K.s;
+    Held held = load(S, s);
+    if (!(held.im > 0.0f)) return;
+    const float r = held.r, wv = held.im;
+    const float turns = turns_per_impulse(wv, r, r);
+    const float rubbing = rubbing_of(K.p);
+#pragma unroll
+    for (int axis = 0; axis < 3; axis++) {
+        float4* rec = K.wall + 6 * (size_t)s + 2 * axis;
+        Impulse taken = load_impulse(rec);
+        const float reach = r * (1.0f + LIST_MARGIN);
+        const float position = held.at[axis];
+        float out = 0.0f;
+        if (position < reach) out = 1.0f;
+        if (position > K.p.w[SX + axis] - reach) out = -1.0f;
+        if (!(rubbing > 0.0f && out != 0.0f)) {
+            clear_impulse(taken);
+        } else {
+            const float push = (taken.normal * wv) * out;
+            held.at[axis] = held.at[axis] + push;
+            held.displaced[axis] = held.displaced[axis] + push;
+            taken.p[axis] = 0.0f;
+            float n[3] = {0.0f, 0.0f, 0.0f};
+            n[axis] = out;
+            rub(held, wv, turns, nullptr, 0.0f, 0.0f, n, taken.p);
+#pragma unroll
+            for (int k = 0; k < 3; k++) held.turned[k] = held.turned[k] + (turns * taken.q[k]) / r;
+        }
+        store_impulse(rec, taken);
+    }
+    store(S, held);
+}
+
+// Spheres.walls :1185-1198 = shift :1351-1418 with friction.
+__device__ __forceinline__ void walls(const Kernel& K, int s) {
+    const State& S = K.s;
+    Held held = load(S, s);
+    if (!(held.im > 0.0f)) return;
+    const float r = held.r;
+    const float4 vel = S.vel[s], spin = S.spin[s];
+    const float4 none = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float c = 0.0f;
+        const float moved = held.at[a] + c;
+        const float high = K.p.w[SX + a] - r;
+        float side = 1.0f;
+        float into = r - moved;
+        if (moved * 2.0f > K.p.w[SX + a]) {
+            side = -1.0f;
+            into = moved - high;
+        }
+        const float wv = held.im;
+        float4* rec = K.wall + 6 * (size_t)s + 2 * a;
+        Impulse taken = load_impulse(rec);
+        float inside = fmaxf(r, fminf(high, moved));
+        float push = fmaxf(into, 0.0f);
+        if (!(into > 0.0f) && taken.normal > 0.0f) {
+            push = fmaxf(into, -(taken.normal * wv));
+            inside = moved + side * push;
+        }
+        taken.normal = taken.normal + push / wv;
+        held.at[a] = inside;
+        held.displaced[a] = held.displaced[a] + (c + (inside - moved));
+        const float reach = r * LIST_MARGIN;
+        float out = 0.0f;
+        if (!(inside > r + reach)) out = 1.0f;
+        if (!(inside < high - reach)) out = -1.0f;
+        if (out != 0.0f) {
+            float n[3] = {0.0f, 0.0f, 0.0f};
+            n[a] = out;
+            roll(K.p, held, spin, wv, nullptr, none, 0.0f, r, taken);
+            friction(K.p, held, vel, spin, wv, r, nullptr, none, none, 0.0f, 0.0f, n, taken);
+        }
+        store_impulse(rec, taken);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float high = K.p.w[SX + a] - r;
+        const float inside = fmaxf(r, fminf(high, held.at[a]));
+        held.displaced[a] = held.displaced[a] + (inside - held.at[a]);
+        held.at[a] = inside;
+    }
+    store(S, held);
+}
+
+// Spheres.solve(grid) :302-347 / Solving :1245-1298: Jacobi's move into cx, cy, cz.
+__device__ __forceinline__ void jacobi_solve(const Kernel& K, int s) {
+    const State& S = K.s;
+    const float4 me = S.pos[s];
+    const float mine[3] = {me.x, me.y, me.z};
+    const float rs = me.w, ws = S.disp[s].w;
+    float sum[3] = {0.0f, 0.0f, 0.0f};
+    float contacts = 0.0f;
+    around(K, s, [&](int o) {
+        if (o == s) return;
+        const float4 other = S.pos[o];
+        float d[3] = {mine[0] - other.x, mine[1] - other.y, mine[2] - other.z};
+        const float d2 = d[0] * d[0] + (d[1] * d[1] + d[2] * d[2]);
+        const float reach = rs + other.w;
+        const float wsum = ws + S.disp[o].w;
+        if (!(d2 < reach * reach)) return;
+        if (!(d2 > COINCIDENT)) return;
+        if (!(wsum > 0.0f)) return;
+        const float dist = sqrtf(d2);
+        const float share = ((reach - dist) * (ws / wsum)) / dist;
+#pragma unroll
+        for (int a = 0; a < 3; a++) sum[a] = sum[a] + share * d[a];
+        contacts = contacts + 1.0f;
+    });
+    const float omega = K.p.w[OMEGA];
+    float scale = omega;
+    if (K.p.w[AVERAGED] > 0.0f) scale = omega / fmaxf(contacts, 1.0f);
+    S.cvel[s] = make_float4(scale * sum[0], scale * sum[1], scale * sum[2], 0.0f);
+}
+
+// Spheres.apply :1326-1342 (shift without friction).
+__device__ __forceinline__ void jacobi_apply(const Kernel& K, int s) {
+    const State& S = K.s;
+    Held held = load(S, s);
+    if (!(held.im > 0.0f)) return;
+    const float r = held.r;
+    const float4 move = S.cvel[s];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float c = get(move, a);
+        const float moved = held.at[a] + c;
+        const float high = K.p.w[SX + a] - r;
+        const float inside = fmaxf(r, fminf(high, moved));
+        held.at[a] = inside;
+        const float push = inside - moved;
+        held.displaced[a] = held.displaced[a] + (c + push);
+    }
+    store(S, held);
+}
+
+// Spheres.velocity :1430-1460.
+__device__ __forceinline__ void velocity(const Kernel& K, int s) {
+    const State& S = K.s;
+    const float perH = 1.0f / K.p.w[H];
+    const float4 was = S.vel[s], d = S.disp[s], t = S.turn[s], w = S.spin[s];
+    S.cvel[s] = make_float4(was.x, was.y, was.z, 0.0f);
+    S.vel[s] = make_float4(was.x + d.x * perH, was.y + d.y * perH, was.z + d.z * perH, was.w);
+    S.disp[s] = make_float4(0.0f, 0.0f, 0.0f, d.w);
+    S.spin[s] = make_float4(w.x + t.x * perH, w.y + t.y * perH, w.z + t.z * perH, w.w);
+    S.turn[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float angle[3] = {t.x, t.y, t.z};
+    S.q[s] = turned(S.q[s], angle);
+}
+
+// Spheres.bounce(grid) :1528-1627: the change into dx, dy, dz.
+__device__ __forceinline__ void bounce(const Kernel& K, int s) {
+    const State& S = K.s;
+    const float e = K.p.w[RESTITUTION];
+    const float4 me = S.pos[s];
+    const float wa = S.disp[s].w;
+    if (!(e > 0.0f && wa > 0.0f)) return;
+    const float h = K.p.w[H];
+    const float gx = K.p.w[GX], gy = K.p.w[GY], gz = K.p.w[GZ];
+    const float resting = (2.0f * h) * sqrtf(gx * gx + (gy * gy + gz * gz));
+    const float ra = me.w;
+    const float mine[3] = {me.x, me.y, me.z};
+    const float4 v4 = S.vel[s], c4 = S.cvel[s];
+    const float vel[3] = {v4.x, v4.y, v4.z}, was[3] = {c4.x, c4.y, c4.z};
+    float sum[3] = {0.0f, 0.0f, 0.0f};
+    around(K, s, [&](int o) {
+        if (o == s) return;
+        const float4 other = S.pos[o];
+        float d[3] = {mine[0] - other.x, mine[1] - other.y, mine[2] - other.z};
+        const float d2 = d[0] * d[0] + (d[1] * d[1] + d[2] * d[2]);
+        const float near = (ra + other.w) * (1.0f + LIST_MARGIN);
+        const float wsum = wa + S.disp[o].w;
+        if (!(d2 < near * near && d2 > COINCIDENT)) return;
+        const float dist = sqrtf(d2);
+        const float4 ov = S.vel[o], oc = S.cvel[o];
+        float closing = 0.0f, parting = 0.0f;
+        const float n0 = d[0] / dist, n1 = d[1] / dist, n2 = d[2] / dist;
+        closing = closing + n0 * (was[0] - oc.x);
+        parting = parting + n0 * (vel[0] - ov.x);
+        closing = closing + n1 * (was[1] - oc.y);
+        parting = parting + n1 * (vel[1] - ov.y);
+        closing = closing + n2 * (was[2] - oc.z);
+        parting = parting + n2 * (vel[2] - ov.z);
+        if (closing < -resting) {
+            const float k = ((-(e * closing) - parting) * wa) / (wsum * dist);
+#pragma unroll
+            for (int a = 0; a < 3; a++) sum[a] = sum[a] + k * d[a];
+        }
+    });
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float reach = ra * (1.0f + LIST_MARGIN);
+        if (mine[a] < reach && was[a] < -resting) sum[a] = sum[a] + (-(e * was[a]) - vel[a]);
+        if (mine[a] > K.p.w[SX + a] - reach && was[a] > resting) sum[a] = sum[a] + (-(e * was[a]) - vel[a]);
+    }
+    S.disp[s] = make_float4(sum[0], sum[1], sum[2], wa);
+}
+
+// Spheres.bounced :1633-1644.
+__device__ __forceinline__ void bounced(const Kernel& K, int s) {
+    const State& S = K.s;
+    const float4 v = S.vel[s], d = S.disp[s];
+    S.vel[s] = make_float4(v.x + d.x, v.y + d.y, v.z + d.z, v.w);
+    S.disp[s] = make_float4(0.0f, 0.0f, 0.0f, d.w);
+}
+
+// Spheres.show(grid) :1697-1794.
+__device__ __forceinline__ void show(const Kernel& K, int s) {
+    const State& S = K.s;
+    float* sh = K.shown + (size_t)s * SHOWN;
+    const float4 me = S.pos[s];
+    const float mine[3] = {me.x, me.y, me.z};
+    const float rs = me.w;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        sh[a] = sh[4 + a];
+        sh[4 + a] = mine[a];
+    }
+    sh[3] = rs;
+    for (int k = 0; k < 12; k++) sh[PRESSED_BEFORE + k] = sh[PRESSED_AFTER + k];
+    const float4 q = S.q[s];
+    for (int k = 0; k < 4; k++) sh[TURNED_BEFORE + k] = sh[TURNED_AFTER + k];
+    sh[TURNED_AFTER + 0] = q.x;
+    sh[TURNED_AFTER + 1] = q.y;
+    sh[TURNED_AFTER + 2] = q.z;
+    sh[TURNED_AFTER + 3] = q.w;
+    float flat[6] = {0, 0, 0, 0, 0, 0}, lean[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float low = rs - mine[a];
+        const float high = (mine[a] + rs) - K.p.w[SX + a];
+        if (low > 0.0f) {
+            const float share = low / rs;
+            flat[a] = flat[a] + share;
+            lean[a] = lean[a] + -1.0f * share;
+        }
+        if (high > 0.0f) {
+            const float share = high / rs;
+            flat[a] = flat[a] + share;
+            lean[a] = lean[a] + 1.0f * share;
+        }
+    }
+    around(K, s, [&](int o) {
+        if (o == s) return;
+        const float4 other = S.pos[o];
+        float d[3] = {other.x - mine[0], other.y - mine[1], other.z - mine[2]};
+        const float d2 = dotf(d, d);
+        const float reach = rs + other.w;
+        if (!(d2 < reach * reach && d2 > COINCIDENT)) return;
+        const float dist = sqrtf(d2);
+        const float share = (reach - dist) / reach;
+        const float g = share / d2;
+        const float along = share / dist;
+        flat[0] = flat[0] + g * (d[0] * d[0]);
+        flat[1] = flat[1] + g * (d[1] * d[1]);
+        flat[2] = flat[2] + g * (d[2] * d[2]);
+        flat[3] = flat[3] + g * (d[0] * d[1]);
+        flat[4] = flat[4] + g * (d[0] * d[2]);
+        flat[5] = flat[5] + g * (d[1] * d[2]);
+#pragma unroll
+        for (int a = 0; a < 3; a++) lean[a] = lean[a] + along * d[a];
+    });
+    float* after = sh + PRESSED_AFTER;
+    for (int k = 0; k < 6; k++) after[k] = flat[k];
+    for (int a = 0; a < 3; a++) after[6 + a] = lean[a];
+    after[9] = (flat[0] + flat[1]) + flat[2];
+    after[10] = sqrtf(dotf(lean, lean));
+}
+
+// --- the contact list ----------------------------------------------------------------------------------------
+
+// listContacts' first half: how many spheres of higher index are near sphere a (Spheres.listContacts :961-1022).
+__device__ __forceinline__ int count_near(const Kernel& K, int a) {
+    const float4 me = K.s.pos[a];
+    int found = 0;
+    around(K, a, [&](int o) {
+        if (!(o > a)) return;
+        const float4 other = K.s.pos[o];
+        const float d0 = me.x - other.x, d1 = me.y - other.y, d2v = me.z - other.z;
+        const float d2 = d0 * d0 + (d1 * d1 + d2v * d2v);
+        const float near = (me.w + other.w) * (1.0f + LIST_MARGIN);
+        if (d2 < near * near) found++;
+    });
+    return found;
+}
+
+// listContacts' second half: sphere a's contacts written at the places the scan gave it, chained, each with the
+// impulses the pair took in the substep before (found by walking a's kept chain, at most MOST_KEPT places).
+__device__ __forceinline__ void fill_near(const Kernel& K, const ListGen& L, const ListGen& kept, int a) {
+    const float4 me = K.s.pos[a];
+    const int first = K.list_start[a];
+    int slot = first;
+    int last = -1;
+    around(K, a, [&](int o) {
+        if (!(o > a)) return;
+        const float4 other = K.s.pos[o];
+        const float d0 = me.x - other.x, d1 = me.y - other.y, d2v = me.z - other.z;
+        const float d2 = d0 * d0 + (d1 * d1 + d2v * d2v);
+        const float near = (me.w + other.w) * (1.0f + LIST_MARGIN);
+        if (!(d2 < near * near)) return;
+        const int at = slot++;
+        if (!(at < K.cap)) return;
+        L.pair[at] = make_int2(a, o);
+        L.done[at] = 0;
+        L.next[at] = last;
+        last = at;
+        float4 w0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), w1 = w0;
+        int j = kept.head[a];
+        int walked = 0;
+        while (j >= 0 && walked < MOST_KEPT) {
+            if (kept.pair[j].y == o) {
+                w0 = kept.imp[2 * (size_t)j];
+                w1 = kept.imp[2 * (size_t)j + 1];
+                walked = MOST_KEPT;
+            }
+            j = kept.next[j];
+            walked++;
+        }
+        L.imp[2 * (size_t)at] = w0;
+        L.imp[2 * (size_t)at + 1] = w1;
+    });
+    L.head[a] = last;
+}
+
+// Spheres.contactRound :1076-1133, one dispatch over the list. The winners of a dispatch share no sphere (each
+// sphere's claim is held by one priority), so they solve in parallel with the result of any serial order.
+__device__ __forceinline__ void contact_round(const Kernel& K, const ListGen& L, int listed, int checks, int claims,
+                                              int pass, int dispatch, int mark, int check_dispatch, int rubs,
+                                              const int* checked, int* claimed, int* cleared, int gtid, int gsize) {
+    if (gtid == 0) K.counts->open[1 - mark] = 0;
+    for (int c = gtid; c < listed; c += gsize) {
+        if (L.done[c] == pass) continue;
+        const int2 ab = L.pair[c];
+        const int pair = ab.x * K.n + ab.y;
+        int won = 0;
+        if (checks > 0) {
+            const int last = priority(pair, check_dispatch);
+            if (checked[ab.x] == last && checked[ab.y] == last) won = 1;
+        }
+        if (won) {
+            contact(K, L.imp + 2 * (size_t)c, ab.x, ab.y, pass, rubs);
+            L.done[c] = pass;
+        } else {
+            cleared[ab.x] = 0;
+            cleared[ab.y] = 0;
+            if (claims > 0) {
+                K.counts->open[mark] = 1;
+                const int mine = priority(pair, dispatch);
+                atomicMax(&claimed[ab.x], mine);
+                atomicMax(&claimed[ab.y], mine);
+            } else {
+                atomicAdd(&K.counts->count[MISSED], 1);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ int position(int k) { return k == 0 ? 0 : 1 + (k - 1) % CYCLE; }
+
+// Exclusive scan of in[0..m) into out[0..m], out[m] the total, by the threads of one block.
+__device__ void block_scan(const int* in, int* out, int m) {
+    __shared__ int warp_sums[32];
+    const int per = (m + blockDim.x - 1) / blockDim.x;
+    const int begin = min(m, (int)threadIdx.x * per), end = min(m, begin + per);
+    int sum = 0;
+    for (int i = begin; i < end; i++) sum += in[i];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int v = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        warp_sums[lane] = v;
+    }
+    __syncthreads();
+    int run = (warp > 0 ? warp_sums[warp - 1] : 0) + x - sum;
+    for (int i = begin; i < end; i++) {
+        const int v = in[i];
+        out[i] = run;
+        run += v;
+    }
+    if (threadIdx.x == blockDim.x - 1) out[m] = warp_sums[(blockDim.x >> 5) - 1];
+    __syncthreads();
+}
+
+__device__ __forceinline__ int read_int(const int* p) { return *(const volatile int*)p; }
+
+// The barrier between passes: the block's own when the kernel is one block, else the bounded grid barrier.
+#define SYNC()                                                    \
+    do {                                                          \
+        if (gridDim.x == 1) {                                     \
+            __syncthreads();                                      \
+        } else if (!grid_sync(K.bar, epoch)) {                    \
+            return;                                               \
+        }                                                         \
+    } while (0)
+
+// `steps` whole steps (SphereStep's pass list :184-196; SphereStepper.step :66-103 when run until done).
+__global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gsize = gridDim.x * blockDim.x;
+    const int n = K.n;
+    unsigned int epoch = 0;
+    int cur = read_int(&K.counts->cur);
+    const bool gs = K.solve != 0;
+    const int limit = K.cap + 2 * CYCLE;
+    for (int step = 0; step < K.steps; step++) {
+        if (gtid == 0) {
+            for (int k = 0; k < 4; k++) K.counts->last[k] = 0;
+        }
+        for (int sub = 0; sub < K.substeps; sub++) {
+            // predict; the cell of each centre, counted; the walls' warm start; every claim cleared
+            for (int s = gtid; s < n; s += gsize) {
+                if (sub > 0) bounced(K, s);
+                predict(K, s);
+                if (K.gridded) {
+                    const float4 p = K.s.pos[s];
+                    const int key = cell_key(K, p.x, p.y, p.z);
+                    K.keys[s] = key;
+                    atomicAdd(&K.cell_count[key], 1);
+                }
+                if (gs) {
+                    warm_walls(K, s);
+                    K.claims[s] = 0;
+                    K.claims[n + s] = 0;
+                    K.claims[2 * n + s] = 0;
+                }
+            }
+            if (gs && gtid == 0) {
+                Counts* c = K.counts;
+                c->count[LONGEST] = max(c->count[LONGEST], c->count[LISTED]);
+            }
+            SYNC();
+            if (K.gridded) {
+                if (blockIdx.x == 0) block_scan(K.cell_count, K.cell_start, K.cells);
+                SYNC();
+                // a place in its cell for each sphere; the counts return to zero for the next substep
+                for (int s = gtid; s < n; s += gsize) {
+                    const int key = K.keys[s];
+                    K.order[K.cell_start[key] + atomicSub(&K.cell_count[key], 1) - 1] = s;
+                }
+                SYNC();
+                // within a cell, ascending index: the stable counting sort's order
+                for (int c = gtid; c < K.cells; c += gsize) {
+                    const int begin = K.cell_start[c], end = K.cell_start[c + 1];
+                    for (int i = begin + 1; i < end; i++) {
+                        const int v = K.order[i];
+                        int j = i - 1;
+                        while (j >= begin && K.order[j] > v) {
+                            K.order[j + 1] = K.order[j];
+                            j--;
+                        }
+                        K.order[j + 1] = v;
+                    }
+                }
+                SYNC();
+            }
+            int listed = 0;
+            if (gs) {
+                for (int a = gtid; a < n; a += gsize) K.list_count[a] = count_near(K, a);
+                SYNC();
+                if (blockIdx.x == 0) {
+                    block_scan(K.list_count, K.list_start, n);
+                    if (threadIdx.x == 0) K.counts->count[LISTED] = K.list_start[n];
+                }
+                SYNC();
+                cur ^= 1;
+                const ListGen L = K.gen[cur], kept = K.gen[cur ^ 1];
+                for (int a = gtid; a < n; a += gsize) fill_near(K, L, kept, a);
+                SYNC();
+                listed = min(read_int(&K.counts->count[LISTED]), K.cap);
+            }
+            const ListGen L = K.gen[cur];
+            for (int it = 0; it < K.iterations; it++) {
+                if (K.solve == 0) {
+                    for (int s = gtid; s < n; s += gsize) jacobi_solve(K, s);
+                    SYNC();
+                    for (int s = gtid; s < n; s += gsize) jacobi_apply(K, s);
+                    SYNC();
+                    continue;
+                }
+                if (K.solve == 2) {
+                    // rounds 0..R on dispatches counted over the substep's passes (SphereStep.byContact :216-262)
+                    for (int k = 0; k <= K.rounds; k++) {
+                        const int g = it * (K.rounds + 1) + k;
+                        contact_round(K, L, listed, k == 0 ? 0 : 1, k == K.rounds ? 0 : 1, it + 1, g, g % 2, g - 1,
+                                      0, K.claims + ((g + 2) % 3) * n, K.claims + (g % 3) * n,
+                                      K.claims + ((g + 1) % 3) * n, gtid, gsize);
+                        SYNC();
+                    }
+                    for (int s = gtid; s < n; s += gsize) walls(K, s);
+                    SYNC();
+                    continue;
+                }
+                // until done: the opening batch, then BATCH more while the last round left a contact open
+                int k = read_int(&K.opening[it]);
+                int waits = 0;
+                int from = 0;
+                for (;;) {
+                    for (int j = from; j < k; j++) {
+                        const int p = position(j);
+                        contact_round(K, L, listed, p == 0 ? 0 : 1, 1, it + 1, it * CYCLE + p % CYCLE, p % 2,
+                                      it * CYCLE + max(p - 1, 0) % CYCLE, 0, K.claims + ((p + 2) % 3) * n,
+                                      K.claims + (p % 3) * n, K.claims + ((p + 1) % 3) * n, gtid, gsize);
+                        SYNC();
+                    }
+                    waits++;
+                    const int open = read_int(&K.counts->open[position(k - 1) % 2]);
+                    SYNC();
+                    if (open == 0) break;
+                    if (k > limit) {
+                        if (gtid == 0) {
+                            K.counts->rounds_at = k;
+                            atomicCAS(&K.counts->status, ST_OK, ST_ROUNDS);
+                        }
+                        return;
+                    }
+                    from = k;
+                    k += BATCH;
+                }
+                if (K.friction) {
+                    // the same dispatches again, rubbing (SphereStep.rubs :271-278)
+                    for (int j = 0; j < k; j++) {
+                        const int p = position(j);
+                        contact_round(K, L, listed, p == 0 ? 0 : 1, 1, K.iterations + it + 1,
+                                      it * CYCLE + p % CYCLE, p % 2, it * CYCLE + max(p - 1, 0) % CYCLE, 1,
+                                      K.claims + ((p + 2) % 3) * n, K.claims + (p % 3) * n,
+                                      K.claims + ((p + 1) % 3) * n, gtid, gsize);
+                        SYNC();
+                    }
+                }
+                for (int s = gtid; s < n; s += gsize) walls(K, s);
+                if (gtid == 0) {
+                    Counts* c = K.counts;
+                    const int unlisted = max(0, c->count[LISTED] - K.cap);
+                    c->last[0] += waits;
+                    c->last[1] += k;
+                    c->last[2] = max(c->last[2], k);
+                    c->last[3] += unlisted;
+                    c->total[0] += waits;
+                    c->total[1] += k;
+                    c->total[2] = max(c->total[2], (long long)k);
+                    c->total[3] += unlisted;
+                    // SphereStepper.adapt :118-126
+                    if (k > K.opening[it]) {
+                        K.opening[it] = min(k, CYCLE);
+                        K.enough[it] = 0;
+                    } else if (++K.enough[it] >= SHRINK_AFTER && K.opening[it] > BATCH) {
+                        K.opening[it] -= BATCH;
+                        K.enough[it] = 0;
+                    }
+                }
+                SYNC();
+            }
+            for (int s = gtid; s < n; s += gsize) velocity(K, s);
+            SYNC();
+            for (int s = gtid; s < n; s += gsize) bounce(K, s);
+            SYNC();
+        }
+        // the last substep's restitution added, then the picture's buffer
+        for (int s = gtid; s < n; s += gsize) {
+            bounced(K, s);
+            show(K, s);
+        }
+        SYNC();
+    }
+    if (gtid == 0) K.counts->cur = cur;
+}
+
+}  // namespace sph
+}  // namespace vxr
+
+using namespace vxr;
+using namespace vxr::sph;
+
+struct vxr_sphere_world {
+    int n = 0, substeps = 1, iterations = 1, solve = 0, rounds = 32, cap = 0;
+    int gridded = 0, nx = 1, ny = 1, nz = 1, cells = 1;
+    float cell = 1.0f;
+    int device = 0, sms = 148, blocks = 1, friction = 1;
+    cudaStream_t stream = nullptr;
+    SParams params{};
+    std::string error;
+    State s{};
+    float4* wall = nullptr;
+    float* shown = nullptr;
+    int *keys = nullptr, *order = nullptr, *cell_count = nullptr, *cell_start = nullptr;
+    int *claims = nullptr, *list_count = nullptr, *list_start = nullptr;
+    ListGen gen[2]{};
+    Counts* counts = nullptr;
+    Counts* host_counts = nullptr;  // pinned
+    int *opening = nullptr, *enough = nullptr;
+    float* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    std::vector<void*> allocations;
+    long long launches = 0;
+    int pending = 0;  // a call of steps is in flight
+};
+
+namespace {
+
+int sfail(vxr_sphere_world* w, int code, const std::string& why) {
+    if (w) w->error = why;
+    return code;
+}
+
+#define SPH_CUDA(call)                                                                           \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) return sfail(w, VXR_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+int salloc(vxr_sphere_world* w, T** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) return sfail(w, VXR_ECUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    w->allocations.push_back(q);
+    *p = (T*)q;
+    return VXR_OK;
+}
+
+int32_t f32bits(double v) {
+    const float f = (float)v;
+    int32_t b;
+    std::memcpy(&b, &f, 4);
+    return b;
+}
+
+float* staging(vxr_sphere_world* w, size_t bytes) {
+    if (w->pinned_bytes < bytes) {
+        if (w->pinned) cudaFreeHost(w->pinned);
+        w->pinned = nullptr;
+        w->pinned_bytes = 0;
+        if (cudaMallocHost(&w->pinned, bytes) != cudaSuccess) return nullptr;
+        w->pinned_bytes = bytes;
+    }
+    return w->pinned;
+}
+
+// The 24 fields of the reference (Spheres.SPHERE :240-241) as (array, component) of the float4 layout.
+struct FieldAt {
+    int array;  // 0 pos 1 disp 2 turn 3 vel 4 spin 5 q 6 cvel
+    int comp;
+};
+const FieldAt FIELD_AT[24] = {{0, 0}, {0, 1}, {0, 2}, {3, 0}, {3, 1}, {3, 2}, {0, 3}, {1, 3},
+                              {6, 0}, {6, 1}, {6, 2}, {1, 0}, {1, 1}, {1, 2}, {4, 0}, {4, 1},
+                              {4, 2}, {2, 0}, {2, 1}, {2, 2}, {5, 0}, {5, 1}, {5, 2}, {5, 3}};
+
+float4* array_of(vxr_sphere_world* w, int k) {
+    float4* arrays[7] = {w->s.pos, w->s.disp, w->s.turn, w->s.vel, w->s.spin, w->s.q, w->s.cvel};
+    return arrays[k];
+}
+
+// Writes the fields given (null: zero; qw: one), every other buffer cleared, as the reference's runner.clear()
+// and constants leave them (SphereSimulation.start, gui/SphereSimulation.java:154-178).
+int write_state(vxr_sphere_world* w, const float* const* fields24, const float* shown) {
+    const int n = w->n;
+    const size_t bytes = sizeof(float4) * (size_t)n * 7;
+    float4* host = (float4*)staging(w, bytes);
+    if (!host) return sfail(w, VXR_ECUDA, "pinned staging");
+    std::memset(host, 0, bytes);
+    for (int s = 0; s < n; s++) host[5 * (size_t)n + s].w = 1.0f;  // qw
+    for (int f = 0; f < 24; f++) {
+        if (!fields24 || !fields24[f]) continue;
+        const FieldAt at = FIELD_AT[f];
+        float* base = (float*)(host + (size_t)at.array * n);
+        for (int s = 0; s < n; s++) base[4 * (size_t)s + at.comp] = fields24[f][s];
+    }
+    cudaStream_t st = w->stream;
+    for (int a = 0; a < 7; a++)
+        SPH_CUDA(cudaMemcpyAsync(array_of(w, a), host + (size_t)a * n, sizeof(float4) * n, cudaMemcpyHostToDevice, st));
+    SPH_CUDA(cudaStreamSynchronize(st));
+    SPH_CUDA(cudaMemsetAsync(w->wall, 0, sizeof(float4) * 6 * (size_t)n, st));
+    if (shown)
+        SPH_CUDA(cudaMemcpyAsync(w->shown, shown, sizeof(float) * SHOWN * (size_t)n, cudaMemcpyHostToDevice, st));
+    else
+        SPH_CUDA(cudaMemsetAsync(w->shown, 0, sizeof(float) * SHOWN * (size_t)n, st));
+    SPH_CUDA(cudaMemsetAsync(w->claims, 0, sizeof(int) * 3 * (size_t)n, st));
+    if (w->gridded) SPH_CUDA(cudaMemsetAsync(w->cell_count, 0, sizeof(int) * (size_t)w->cells, st));
+    if (w->solve != 0) {
+        for (int g = 0; g < 2; g++) {
+            SPH_CUDA(cudaMemsetAsync(w->gen[g].head, 0xFF, sizeof(int) * (size_t)n, st));
+            SPH_CUDA(cudaMemsetAsync(w->gen[g].done, 0, sizeof(int) * (size_t)w->cap, st));
+        }
+    }
+    SPH_CUDA(cudaMemsetAsync(w->counts, 0, sizeof(Counts), st));
+    SPH_CUDA(cudaStreamSynchronize(st));
+    return VXR_OK;
+}
+
+int launch_steps(vxr_sphere_world* w, int steps) {
+    Kernel K;
+    K.n = w->n;
+    K.cap = w->cap;
+    K.substeps = w->substeps;
+    K.iterations = w->iterations;
+    K.solve = w->solve;
+    K.rounds = w->rounds;
+    K.gridded = w->gridded;
+    K.nx = w->nx;
+    K.ny = w->ny;
+    K.nz = w->nz;
+    K.cells = w->cells;
+    K.friction = w->friction;
+    K.steps = steps;
+    K.cell = w->cell;
+    K.p = w->params;
+    K.s = w->s;
+    K.wall = w->wall;
+    K.shown = w->shown;
+    K.keys = w->keys;
+    K.order = w->order;
+    K.cell_count = w->cell_count;
+    K.cell_start = w->cell_start;
+    K.claims = w->claims;
+    K.list_count = w->list_count;
+    K.list_start = w->list_start;
+    K.gen[0] = w->gen[0];
+    K.gen[1] = w->gen[1];
+    K.counts = w->counts;
+    K.opening = w->opening;
+    K.enough = w->enough;
+    K.bar.count = &w->counts->bar_count;
+    K.bar.generation = &w->counts->bar_gen;
+    K.bar.abort = &w->counts->abort;
+    K.bar.status = &w->counts->status;
+    K.bar.limit_ns = 2000000000ull;  // 2 s: far above any barrier's honest wait
+    cudaStream_t st = w->stream;
+    // the barrier's counter, the status and the call's totals start at zero; the list, its counts and the
+    // generation carry over
+    SPH_CUDA(cudaMemsetAsync(&w->counts->total, 0, sizeof(long long) * 4, st));
+    SPH_CUDA(cudaMemsetAsync(&w->counts->status, 0, sizeof(int) * 4, st));
+    void* args[] = {&K};
+    cudaError_t e;
+    if (w->blocks == 1)
+        e = cudaLaunchKernel((const void*)k_sphere_steps, dim3(1), dim3(THREADS), args, 0, st);
+    else
+        e = cudaLaunchCooperativeKernel((const void*)k_sphere_steps, dim3(w->blocks), dim3(THREADS), args, 0, st);
+    if (e != cudaSuccess) return sfail(w, VXR_ECUDA, std::string("sphere step launch: ") + cudaGetErrorString(e));
+    w->launches++;
+    SPH_CUDA(cudaMemcpyAsync(w->host_counts, w->counts, sizeof(Counts), cudaMemcpyDeviceToHost, st));
+    w->pending = 1;
+    return VXR_OK;
+}
+
+int finish(vxr_sphere_world* w, vxr_sphere_report* report) {
+    if (!w->pending) {
+        if (report) std::memset(report, 0, sizeof(*report));
+        return VXR_OK;
+    }
+    w->pending = 0;
+    SPH_CUDA(cudaStreamSynchronize(w->stream));
+    const Counts& c = *w->host_counts;
+    if (report) {
+        report->waits = c.last[0];
+        report->rounds = c.last[1];
+        report->most_rounds = c.last[2];
+        report->unlisted = c.last[3];
+        report->waits_total = c.total[0];
+        report->rounds_total = c.total[1];
+        report->most_rounds_total = (int32_t)c.total[2];
+        report->unlisted_total = c.total[3];
+        report->status = c.status;
+        report->listed = c.count[LISTED];
+    }
+    if (c.status == ST_ROUNDS)
+        return sfail(w, VXR_EROUNDS, "a pass is still open after " + std::to_string(c.rounds_at) +
+                                         " rounds, on a list of " + std::to_string(c.count[LISTED]));
+    if (c.status == ST_TIMEOUT) return sfail(w, VXR_ETIMEOUT, "a grid barrier's wait ran out; the step stopped");
+    if (c.status != ST_OK) return sfail(w, VXR_ECUDA, "device status " + std::to_string(c.status));
+    return VXR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t vxr_sphere_make_params(double h, double gx, double gy, double gz, double sx, double sy, double sz,
+                               double omega, int32_t averaged, double restitution, double mu_static,
+                               double mu_kinetic, double mu_rolling, int32_t* out) {
+    if (!out) return VXR_EINVAL;
+    for (double mu : {mu_static, mu_kinetic, mu_rolling})
+        if (!(mu >= 0) || std::isinf(mu)) return VXR_EINVAL;
+    if (!(restitution >= 0) || !(restitution <= 1)) return VXR_EINVAL;
+    if (!(h > 0) || !(sx > 0) || !(sy > 0) || !(sz > 0) || !(omega > 0) || !(omega <= 1)) return VXR_EINVAL;
+    const double v[13] = {h, gx, gy, gz, sx, sy, sz, omega, averaged ? 1.0 : 0.0, restitution, mu_static,
+                          mu_kinetic, mu_rolling};
+    for (int k = 0; k < 13; k++) out[k] = f32bits(v[k]);
+    return VXR_OK;
+}
+
+int32_t vxr_sphere_make_grid(double sx, double sy, double sz, double widest, vxr_grid* out) {
+    if (!out || !(widest > 0)) return VXR_EINVAL;
+    out->nx = std::max(1, (int)std::ceil(sx / widest));
+    out->ny = std::max(1, (int)std::ceil(sy / widest));
+    out->nz = std::max(1, (int)std::ceil(sz / widest));
+    out->cell = (float)widest;
+    return VXR_OK;
+}
+
+void vxr_sphere_destroy(vxr_sphere_world* w) {
+    if (!w) return;
+    if (w->stream) cudaStreamSynchronize(w->stream);
+    for (void* p : w->allocations) cudaFree(p);
+    if (w->pinned) cudaFreeHost(w->pinned);
+    if (w->host_counts) cudaFreeHost(w->host_counts);
+    if (w->stream) cudaStreamDestroy(w->stream);
+    delete w;
+}
+
+vxr_sphere_world* vxr_sphere_create(const vxr_sphere_config* cfg, int32_t* status) {
+    auto set = [&](int32_t s) {
+        if (status) *status = s;
+    };
+    if (!cfg || cfg->spheres < 1 || cfg->substeps < 1 || cfg->iterations < 1 || cfg->solve < 0 || cfg->solve > 2) {
+        set(VXR_EINVAL);
+        return nullptr;
+    }
+    const bool gridded = cfg->grid.nx > 0 && cfg->grid.ny > 0 && cfg->grid.nz > 0 && cfg->grid.cell > 0;
+    const int per = cfg->contacts_per_sphere > 0 ? cfg->contacts_per_sphere : 6;
+    // Gauss-Seidel needs the grid and orders at most MOST_LISTED_SPHERES (SphereStep.java:115-131)
+    if ((cfg->solve != 0 && !gridded) || (cfg->solve != 0 && cfg->spheres > VXR_MOST_LISTED_SPHERES) ||
+        (cfg->solve == 2 && cfg->rounds < 1) || (long)cfg->spheres * per > (1L << 30)) {
+        set(VXR_EINVAL);
+        return nullptr;
+    }
+    vxr_sphere_world* w = new vxr_sphere_world();
+    w->n = cfg->spheres;
+    w->substeps = cfg->substeps;
+    w->iterations = cfg->iterations;
+    w->solve = cfg->solve;
+    w->rounds = cfg->solve == 2 ? cfg->rounds : 0;
+    w->cap = w->n * per;
+    w->device = cfg->device;
+    w->gridded = gridded ? 1 : 0;
+    if (gridded) {
+        const long cells = (long)cfg->grid.nx * cfg->grid.ny * cfg->grid.nz;
+        if (cells > (1L << 28)) {
+            set(VXR_EINVAL);
+            delete w;
+            return nullptr;
+        }
+        w->nx = cfg->grid.nx;
+        w->ny = cfg->grid.ny;
+        w->nz = cfg->grid.nz;
+        w->cell = cfg->grid.cell;
+        w->cells = (int)cells;
+    }
+    auto bad = [&](int rc) {
+        set(rc);
+        vxr_sphere_destroy(w);
+        return (vxr_sphere_world*)nullptr;
+    };
+    if (cudaSetDevice(w->device) != cudaSuccess) return bad(VXR_ECUDA);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, w->device) != cudaSuccess) return bad(VXR_ECUDA);
+    w->sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(VXR_ECUDA);
+    const int n = w->n;
+    int rc = 0;
+    rc |= salloc(w, &w->s.pos, n);
+    rc |= salloc(w, &w->s.disp, n);
+    rc |= salloc(w, &w->s.turn, n);
+    rc |= salloc(w, &w->s.vel, n);
+    rc |= salloc(w, &w->s.spin, n);
+    rc |= salloc(w, &w->s.q, n);
+    rc |= salloc(w, &w->s.cvel, n);
+    rc |= salloc(w, &w->wall, 6 * (size_t)n);
+    rc |= salloc(w, &w->shown, SHOWN * (size_t)n);
+    rc |= salloc(w, &w->claims, 3 * (size_t)n);
+    rc |= salloc(w, &w->counts, 1);
+    rc |= salloc(w, &w->opening, w->iterations);
+    rc |= salloc(w, &w->enough, w->iterations);
+    if (gridded) {
+        rc |= salloc(w, &w->keys, n);
+        rc |= salloc(w, &w->order, n);
+        rc |= salloc(w, &w->cell_count, w->cells);
+        rc |= salloc(w, &w->cell_start, (size_t)w->cells + 1);
+    }
+    if (w->solve != 0) {
+        rc |= salloc(w, &w->list_count, n);
+        rc |= salloc(w, &w->list_start, (size_t)n + 1);
+        for (int g = 0; g < 2; g++) {
+            rc |= salloc(w, &w->gen[g].pair, w->cap);
+            rc |= salloc(w, &w->gen[g].done, w->cap);
+            rc |= salloc(w, &w->gen[g].next, w->cap);
+            rc |= salloc(w, &w->gen[g].imp, 2 * (size_t)w->cap);
+            rc |= salloc(w, &w->gen[g].head, n);
+        }
+    }
+    if (rc) return bad(VXR_ECUDA);
+    if (cudaMallocHost(&w->host_counts, sizeof(Counts)) != cudaSuccess) return bad(VXR_ECUDA);
+    // One block while the scene is small enough that a block's barrier beats a grid's; otherwise every SM.
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sphere_steps, THREADS, 0);
+    const int most = std::max(1, per_sm) * w->sms;
+    const long work = std::max<long>(n, w->solve != 0 ? 3L * n : n);
+    int blocks = cfg->blocks > 0 ? cfg->blocks : (n <= VXR_SPHERE_ONE_BLOCK ? 1 : (int)((work + THREADS - 1) / THREADS));
+    w->blocks = std::max(1, std::min(blocks, most));
+    // the stepper's batch sizing starts at BATCH a pass (SphereStepper.java:59-64)
+    std::vector<int> batch(w->iterations, BATCH);
+    if (cudaMemcpy(w->opening, batch.data(), sizeof(int) * w->iterations, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bad(VXR_ECUDA);
+    if (cudaMemset(w->enough, 0, sizeof(int) * w->iterations) != cudaSuccess) return bad(VXR_ECUDA);
+    if (write_state(w, nullptr, nullptr) != VXR_OK) return bad(VXR_ECUDA);
+    set(VXR_OK);
+    return w;
+}
+
+const char* vxr_sphere_error(const vxr_sphere_world* w) { return w ? w->error.c_str() : "no world"; }
+
+static int rubs_of(const int32_t* params) {
+    float f[13];
+    std::memcpy(f, params, sizeof(f));
+    return (f[MU_STATIC] + f[MU_KINETIC]) + f[MU_ROLLING] > 0.0f ? 1 : 0;
+}
+
+int32_t vxr_sphere_start(vxr_sphere_world* w, const float* x, const float* y, const float* z, const float* u,
+                         const float* v, const float* wv, const float* r, const float* im, const int32_t* params) {
+    if (!w || !x || !y || !z || !u || !v || !wv || !r || !im || !params) return sfail(w, VXR_EINVAL, "null argument");
+    if (w->pending) finish(w, nullptr);
+    const float* fields[24] = {x, y, z, u, v, wv, r, im};
+    std::vector<float> shown((size_t)w->n * SHOWN, 0.0f);
+    for (int s = 0; s < w->n; s++) {
+        float* b = shown.data() + (size_t)s * SHOWN;
+        b[0] = b[4] = x[s];
+        b[1] = b[5] = y[s];
+        b[2] = b[6] = z[s];
+        b[3] = r[s];
+        b[TURNED_BEFORE + 3] = b[TURNED_AFTER + 3] = 1.0f;
+    }
+    std::memcpy(w->params.w, params, sizeof(float) * P_COUNT);
+    w->friction = rubs_of(params);
+    return write_state(w, fields, shown.data());
+}
+
+int32_t vxr_sphere_load_state(vxr_sphere_world* w, const float* const* fields24, const int32_t* params) {
+    if (!w || !fields24 || !params) return sfail(w, VXR_EINVAL, "null argument");
+    if (w->pending) finish(w, nullptr);
+    std::memcpy(w->params.w, params, sizeof(float) * P_COUNT);
+    w->friction = rubs_of(params);
+    return write_state(w, fields24, nullptr);
+}
+
+int32_t vxr_sphere_params(vxr_sphere_world* w, const int32_t* params) {
+    if (!w || !params) return sfail(w, VXR_EINVAL, "null argument");
+    std::memcpy(w->params.w, params, sizeof(float) * P_COUNT);
+    w->friction = rubs_of(params);
+    return VXR_OK;
+}
+
+int32_t vxr_sphere_friction(vxr_sphere_world* w, int32_t on) {
+    if (!w) return VXR_EINVAL;
+    w->friction = on ? 1 : 0;
+    return VXR_OK;
+}
+
+int32_t vxr_sphere_step_async(vxr_sphere_world* w, int32_t steps) {
+    if (!w || steps < 0) return sfail(w, VXR_EINVAL, "steps must be at least 0");
+    if (w->pending) {
+        const int rc = finish(w, nullptr);
+        if (rc != VXR_OK) return rc;
+    }
+    if (steps == 0) return VXR_OK;
+    if (cudaSetDevice(w->device) != cudaSuccess) return sfail(w, VXR_ECUDA, "cudaSetDevice");
+    return launch_steps(w, steps);
+}
+
+int32_t vxr_sphere_sync(vxr_sphere_world* w, vxr_sphere_report* report) {
+    if (!w) return VXR_EINVAL;
+    return finish(w, report);
+}
+
+int32_t vxr_sphere_step(vxr_sphere_world* w, int32_t steps, vxr_sphere_report* report) {
+    const int rc = vxr_sphere_step_async(w, steps);
+    if (rc != VXR_OK) return rc;
+    return finish(w, report);
+}
+
+void* vxr_sphere_stream(vxr_sphere_world* w) { return w ? (void*)w->stream : nullptr; }
+
+int32_t vxr_sphere_field(vxr_sphere_world* w, int32_t field, float* out) {
+    if (!w || !out || field < 0 || field >= 24) return sfail(w, VXR_EINVAL, "field is 0 to 23");
+    if (w->pending) {
+        const int rc = finish(w, nullptr);
+        if (rc != VXR_OK) return rc;
+    }
+    const FieldAt at = FIELD_AT[field];
+    const int n = w->n;
+    float4* host = (float4*)staging(w, sizeof(float4) * n);
+    if (!host) return sfail(w, VXR_ECUDA, "pinned staging");
+    SPH_CUDA(cudaMemcpyAsync(host, array_of(w, at.array), sizeof(float4) * n, cudaMemcpyDeviceToHost, w->stream));
+    SPH_CUDA(cudaStreamSynchronize(w->stream));
+    const float* f = (const float*)host;
+    for (int s = 0; s < n; s++) out[s] = f[4 * (size_t)s + at.comp];
+    return VXR_OK;
+}
+
+int32_t vxr_sphere_state(vxr_sphere_world* w, float* const* out9) {
+    if (!w || !out9) return sfail(w, VXR_EINVAL, "null argument");
+    const int fields[9] = {0, 1, 2, 3, 4, 5, 14, 15, 16};  // x y z u v w ax ay az
+    for (int k = 0; k < 9; k++) {
+        if (!out9[k]) continue;
+        const int rc = vxr_sphere_field(w, fields[k], out9[k]);
+        if (rc != VXR_OK) return rc;
+    }
+    return VXR_OK;
+}
+
+int32_t vxr_sphere_read_shown(vxr_sphere_world* w, float* out) {
+    if (!w || !out) return sfail(w, VXR_EINVAL, "null argument");
+    if (w->pending) {
+        const int rc = finish(w, nullptr);
+        if (rc != VXR_OK) return rc;
+    }
+    SPH_CUDA(cudaMemcpy(out, w->shown, sizeof(float) * SHOWN * (size_t)w->n, cudaMemcpyDeviceToHost));
+    return VXR_OK;
+}
+
+int32_t vxr_sphere_contacts(vxr_sphere_world* w, int32_t* ab, int32_t* done, float* impulses, int32_t capacity,
+                            int32_t* listed) {
+    if (!w || !listed) return sfail(w, VXR_EINVAL, "null argument");
+    if (w->pending) {
+        const int rc = finish(w, nullptr);
+        if (rc != VXR_OK) return rc;
+    }
+    Counts c;
+    SPH_CUDA(cudaMemcpy(&c, w->counts, sizeof(Counts), cudaMemcpyDeviceToHost));
+    const int k = w->solve == 0 ? 0 : std::min(c.count[LISTED], w->cap);
+    *listed = k;
+    const int m = std::min(k, std::max(0, capacity));
+    if (m == 0) return VXR_OK;
+    const ListGen& L = w->gen[c.cur];
+    if (ab) SPH_CUDA(cudaMemcpy(ab, L.pair, sizeof(int2) * m, cudaMemcpyDeviceToHost));
+    if (done) SPH_CUDA(cudaMemcpy(done, L.done, sizeof(int) * m, cudaMemcpyDeviceToHost));
+    if (impulses) {
+        std::vector<float4> tmp(2 * (size_t)m);
+        SPH_CUDA(cudaMemcpy(tmp.data(), L.imp, sizeof(float4) * 2 * m, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < m; i++) {
+            const float4 a = tmp[2 * i], b = tmp[2 * i + 1];
+            float* o = impulses + 7 * (size_t)i;
+            o[0] = a.x, o[1] = a.y, o[2] = a.z, o[3] = a.w, o[4] = b.x, o[5] = b.y, o[6] = b.z;
+        }
+    }
+    return VXR_OK;
+}
+
+int32_t vxr_sphere_walls(vxr_sphere_world* w, float* out) {
+    if (!w || !out) return sfail(w, VXR_EINVAL, "null argument");
+    if (w->pending) {
+        const int rc = finish(w, nullptr);
+        if (rc != VXR_OK) return rc;
+    }
+    std::vector<float4> tmp(6 * (size_t)w->n);
+    SPH_CUDA(cudaMemcpy(tmp.data(), w->wall, sizeof(float4) * tmp.size(), cudaMemcpyDeviceToHost));
+    for (int s = 0; s < w->n; s++)
+        for (int a = 0; a < 3; a++) {
+            const float4 p = tmp[6 * (size_t)s + 2 * a], q = tmp[6 * (size_t)s + 2 * a + 1];
+            float* o = out + 21 * (size_t)s + 7 * a;
+            o[0] = p.x, o[1] = p.y, o[2] = p.z, o[3] = p.w, o[4] = q.x, o[5] = q.y, o[6] = q.z;
+        }
+    return VXR_OK;
+}
+
+int32_t vxr_sphere_counts(vxr_sphere_world* w, int32_t* out3) {
+    if (!w || !out3) return sfail(w, VXR_EINVAL, "null argument");
+    if (w->pending) {
+        const int rc = finish(w, nullptr);
+        if (rc != VXR_OK) return rc;
+    }
+    Counts c;
+    SPH_CUDA(cudaMemcpy(&c, w->counts, sizeof(Counts), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 3; k++) out3[k] = c.count[k];
+    return VXR_OK;
+}
+
+int32_t vxr_sphere_blocks(const vxr_sphere_world* w) { return w ? w->blocks : 0; }
+
+int64_t vxr_sphere_launches(const vxr_sphere_world* w) { return w ? w->launches : 0; }
+
+}  // extern "C"

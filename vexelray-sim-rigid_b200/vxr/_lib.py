@@ -22,7 +22,12 @@ SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_c
            "vxr_box_step_async", "vxr_box_sync", "vxr_box_stream", "vxr_box_state", "vxr_box_read_shown",
            "vxr_box_touching", "vxr_box_candidates", "vxr_box_walls", "vxr_box_colour_waves", "vxr_collide",
            "vxr_box_launches", "vxr_box_profile", "vxr_box_activity", "vxr_box_trace", "vxr_box_broadphase_static",
-           "vxr_box_measure", "vxr_box_residuals"]
+           "vxr_box_measure", "vxr_box_residuals",
+           "vxr_sphere_make_params", "vxr_sphere_make_grid", "vxr_sphere_create", "vxr_sphere_destroy",
+           "vxr_sphere_error", "vxr_sphere_start", "vxr_sphere_load_state", "vxr_sphere_params", "vxr_sphere_friction",
+           "vxr_sphere_step", "vxr_sphere_step_async", "vxr_sphere_sync", "vxr_sphere_stream", "vxr_sphere_state",
+           "vxr_sphere_field", "vxr_sphere_read_shown", "vxr_sphere_contacts", "vxr_sphere_walls",
+           "vxr_sphere_counts", "vxr_sphere_blocks", "vxr_sphere_launches"]
 
 
 class VxrError(RuntimeError):
@@ -46,6 +51,19 @@ class BoxReport(ctypes.Structure):
                 ("unplaced", ctypes.c_int32), ("unlisted", ctypes.c_int32), ("most_rounds", ctypes.c_int32),
                 ("unplaced_total", ctypes.c_int64), ("unlisted_total", ctypes.c_int64), ("status", ctypes.c_int32),
                 ("steps", ctypes.c_int32)]
+
+
+class SphereConfig(ctypes.Structure):
+    _fields_ = [("spheres", ctypes.c_int32), ("substeps", ctypes.c_int32), ("iterations", ctypes.c_int32),
+                ("solve", ctypes.c_int32), ("rounds", ctypes.c_int32), ("contacts_per_sphere", ctypes.c_int32),
+                ("grid", Grid), ("device", ctypes.c_int32), ("blocks", ctypes.c_int32)]
+
+
+class SphereReport(ctypes.Structure):
+    _fields_ = [("waits", ctypes.c_int32), ("rounds", ctypes.c_int32), ("most_rounds", ctypes.c_int32),
+                ("unlisted", ctypes.c_int32), ("waits_total", ctypes.c_int64), ("rounds_total", ctypes.c_int64),
+                ("most_rounds_total", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("unlisted_total", ctypes.c_int64), ("listed", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
 _lib = None
@@ -111,6 +129,47 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_broadphase_static.restype = i32
         L.vxr_collide.argtypes = [i32, vp, vp, i32, vp, vp]
         L.vxr_collide.restype = i32
+        L.vxr_sphere_make_params.argtypes = [f64] * 8 + [i32] + [f64] * 4 + [vp]
+        L.vxr_sphere_make_params.restype = i32
+        L.vxr_sphere_make_grid.argtypes = [f64] * 4 + [ctypes.POINTER(Grid)]
+        L.vxr_sphere_make_grid.restype = i32
+        L.vxr_sphere_create.argtypes = [ctypes.POINTER(SphereConfig), ctypes.POINTER(i32)]
+        L.vxr_sphere_create.restype = vp
+        L.vxr_sphere_destroy.argtypes = [vp]
+        L.vxr_sphere_error.argtypes = [vp]
+        L.vxr_sphere_error.restype = ctypes.c_char_p
+        L.vxr_sphere_start.argtypes = [vp] + [vp] * 8 + [vp]
+        L.vxr_sphere_start.restype = i32
+        L.vxr_sphere_load_state.argtypes = [vp, vp, vp]
+        L.vxr_sphere_load_state.restype = i32
+        L.vxr_sphere_params.argtypes = [vp, vp]
+        L.vxr_sphere_params.restype = i32
+        L.vxr_sphere_friction.argtypes = [vp, i32]
+        L.vxr_sphere_friction.restype = i32
+        L.vxr_sphere_step.argtypes = [vp, i32, ctypes.POINTER(SphereReport)]
+        L.vxr_sphere_step.restype = i32
+        L.vxr_sphere_step_async.argtypes = [vp, i32]
+        L.vxr_sphere_step_async.restype = i32
+        L.vxr_sphere_sync.argtypes = [vp, ctypes.POINTER(SphereReport)]
+        L.vxr_sphere_sync.restype = i32
+        L.vxr_sphere_stream.argtypes = [vp]
+        L.vxr_sphere_stream.restype = vp
+        L.vxr_sphere_state.argtypes = [vp, vp]
+        L.vxr_sphere_state.restype = i32
+        L.vxr_sphere_field.argtypes = [vp, i32, vp]
+        L.vxr_sphere_field.restype = i32
+        L.vxr_sphere_read_shown.argtypes = [vp, vp]
+        L.vxr_sphere_read_shown.restype = i32
+        L.vxr_sphere_contacts.argtypes = [vp, vp, vp, vp, i32, ctypes.POINTER(i32)]
+        L.vxr_sphere_contacts.restype = i32
+        L.vxr_sphere_walls.argtypes = [vp, vp]
+        L.vxr_sphere_walls.restype = i32
+        L.vxr_sphere_counts.argtypes = [vp, vp]
+        L.vxr_sphere_counts.restype = i32
+        L.vxr_sphere_blocks.argtypes = [vp]
+        L.vxr_sphere_blocks.restype = i32
+        L.vxr_sphere_launches.argtypes = [vp]
+        L.vxr_sphere_launches.restype = ctypes.c_longlong
         _lib = L
     return _lib
 

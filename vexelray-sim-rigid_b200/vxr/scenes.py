@@ -82,5 +82,38 @@ def sub_volume(bodies_full: int, fraction: float, seed: int = 1) -> dict:
     return large_mixed(int(round(bodies_full * fraction)), seed=seed, volume=(128.0 * side, 64.0, 128.0 * side))
 
 
+def sphere_lattice(seed: int = 1, nx: int = 16, ny: int = 8, nz: int = 8, spacing: float = 1.2,
+                   jitter: float = 0.05, radius: float = 0.5, density: float = 1000.0, box: float = 20.0,
+                   height: float = 40.0) -> dict:
+    """The plain sphere scene: 16 x 8 x 8 = 1,024 spheres of radius 0.5 m and density 1000 kg/m^3 on a lattice at
+    1.2 m, each jittered by a seeded uniform +-0.05 m per axis, at rest, dropping into an open 20 x 20 m box of
+    static planes (the reference's walled box with its lid far above: `height`). dt 1/60 s with 4 substeps and 8
+    iterations of Gauss-Seidel over the contact list, mu 0.5, restitution 0.2, grid cells 1.0 m; 600 steps.
+
+    Lattice columns run along x (16, centred in the box's width), layers along y from 1 m up, rows along z (8,
+    centred in its depth)."""
+    from . import spheres as S
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n = nx * ny * nz
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    x0 = (box - (nx - 1) * spacing) / 2
+    z0 = (box - (nz - 1) * spacing) / 2
+    x = x0 + spacing * i.reshape(-1) + rng.uniform(-jitter, jitter, n)
+    y = 1.0 + spacing * j.reshape(-1) + rng.uniform(-jitter, jitter, n)
+    z = z0 + spacing * k.reshape(-1) + rng.uniform(-jitter, jitter, n)
+    mass = density * 4.0 / 3.0 * math.pi * radius ** 3
+    f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)  # noqa: E731
+    dt, substeps = 1 / 60, 4
+    return {
+        "x": f32(x), "y": f32(y), "z": f32(z), "u": np.zeros(n, np.float32), "v": np.zeros(n, np.float32),
+        "w": np.zeros(n, np.float32), "r": np.full(n, radius, np.float32), "im": np.full(n, 1 / mass, np.float32),
+        "spheres": n, "walls": (box, height, box), "dt": dt, "substeps": substeps, "iterations": 8,
+        "grid": S.covering(box, height, box, 2 * radius),
+        "params": S.params(dt / substeps, 0.0, -9.81, 0.0, box, height, box, 1.0, True, 0.2, 0.5, 0.5, 0.0),
+        "steps": 600,
+        "name": f"sphere lattice {nx}x{ny}x{nz} = {n} spheres, r {radius} m, seed {seed}",
+    }
+
+
 def fields(scene: dict) -> list:
     return [scene[k] for k in FIELDS]
