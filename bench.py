@@ -181,9 +181,151 @@ def cpu_baseline(steps_timed: int = 24, warm: int = 2, fraction: float = 1 / 16)
                       f"{warm + steps_timed - 1} of the drop, {dt:.1f} s, OpenMP C++ oracle"}
 
 
+SPHERE_WORKLOAD = ("sphere lattice: 1,024 spheres r 0.5 m rho 1000 on a 16x8x8 lattice at 1.2 m, jitter U(+-0.05) "
+                   "m, at rest, into an open 20x20 m box; dt 1/60 s, 4 substeps, 8 Gauss-Seidel iterations run until "
+                   "done, mu 0.5, e 0.2, grid cell 1.0 m")
+
+
+def sphere_step_bytes(n, substeps, iterations, listed, rounds):
+    """Bytes one sphere step must move: per substep, the state (112 B a sphere) read and written by each of the
+    per-sphere passes (predict and bin, warm walls, list, velocity, restitution, the walls of every pass); the list
+    made (pair, links and 7 impulse words, 48 B a place); per round every open place read (pair and mark, 12 B); and
+    per pass and phase every contact solved once (both spheres' state read, 160 B, and written, 96 B, and its
+    impulses read and written, 64 B). `rounds` is the step's rounds over every pass (parting; rubbing runs as many)."""
+    per_sphere = 224 * (5 + iterations)
+    per_substep = n * per_sphere + 48 * listed + 2 * iterations * listed * (160 + 96 + 64)
+    return substeps * per_substep + 2 * rounds * listed * 12
+
+
+def sphere_cpu_baseline(scene, warm, steps):
+    """The oracle (serial C++ restatement) on the same scene: steps warm..warm+steps-1, timed on the host."""
+    from oracle.sphere import OracleSphereWorld
+    from vxr import spheres as S
+    w = OracleSphereWorld(scene["spheres"], scene["substeps"], scene["iterations"], S.GAUSS_SEIDEL_BY_CONTACT,
+                          scene["grid"])
+    for k in ("x", "y", "z", "u", "v", "w", "r", "im"):
+        w.set_field(k, scene[k])
+    w.set_shown(S.shown_at_start(scene["x"], scene["y"], scene["z"], scene["r"]))
+    w.set_params(scene["params"], S.rubs(scene["params"]))
+    w.step(warm)
+    t0 = time.perf_counter()
+    w.step(steps)
+    dt = time.perf_counter() - t0
+    w.close()
+    return {"value": scene["spheres"] * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"the whole scene, steps {warm}..{warm + steps - 1}, {dt:.1f} s, serial C++ oracle"}
+
+
+def run_spheres(args):
+    """The plain sphere scene on the sphere package: one persistent kernel a step."""
+    world_size, rank, local, pg = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from vxr import scenes
+    from vxr import spheres as S
+    from vxr.sphere_simulation import SphereSimulation
+    scene = scenes.sphere_lattice(seed=1 + rank)
+    n = scene["spheres"]
+
+    def make():
+        sim = SphereSimulation(n, scene["substeps"], scene["iterations"], scene["grid"], S.GAUSS_SEIDEL_BY_CONTACT,
+                               device=local)
+        sim.start(scene["x"], scene["y"], scene["z"], scene["u"], scene["v"], scene["w"], scene["r"], scene["im"],
+                  scene["params"])
+        return sim
+
+    sim = make()
+    stream = torch.cuda.ExternalStream(sim.stream())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    sim.step_and_wait(args.warmup)
+    launches0 = sim.launches()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    rounds, listed = [], []
+    barrier(pg)
+    torch.cuda.synchronize()
+    with Clocks(local) as clocks:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                starts[k].record(stream)
+            sim.step_async(1)
+            with torch.cuda.stream(stream):
+                ends[k].record(stream)
+            rep = sim.sync()
+            rounds.append(rep.rounds)
+            listed.append(int(sim.counts()[S.LISTED]))
+    torch.cuda.synchronize()
+    barrier(pg)
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    launches = sim.launches() - launches0
+    total_ms = float(sum(step_ms))
+    slowest_ms = all_max(pg, total_ms)
+    bodies_all = all_sum(pg, float(n))
+    value = bodies_all * args.steps / (slowest_ms / 1e3)
+    hbm, which = peaks()
+    b = [sphere_step_bytes(n, scene["substeps"], scene["iterations"], min(l, 6 * n), r)
+         for l, r in zip(listed, rounds)]
+    achieved = sum(b) / (total_ms / 1e3) / 1e9
+    sim.close()
+
+    e2e = None
+    if not args.no_e2e:
+        sim2 = make()
+        for _ in range(args.warmup):
+            sim2.step_and_wait(1)
+            sim2.state()
+        barrier(pg)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            sim2.params(scene["params"])
+            sim2.step_and_wait(1)
+            sim2.state()
+        e2e_s = all_max(pg, time.perf_counter() - t0)
+        sim2.close()
+        e2e = {"value": bodies_all * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 13 * 4,
+               "d2h_bytes_per_step": 9 * 4 * n}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": slowest_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": SPHERE_WORKLOAD, "spheres": n, "dt": scene["dt"], "substeps": scene["substeps"],
+                   "iterations": scene["iterations"], "timed_steps": f"{args.warmup}..{args.warmup + args.steps - 1}",
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": "replicas" if world_size > 1 else "single"},
+        "rounds_per_step": {"mean": float(np.mean(rounds)), "max": int(np.max(rounds))},
+        "listed_last": listed[-1],
+        "roofline": {"bound": "hbm", "kernel": "k_sphere_steps", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "peak_source": which,
+                     "bytes_per_launch": float(np.mean(b)), "ms_per_launch": total_ms / args.steps},
+        "gpu_launches": int(launches),
+        "iterations_to_residual": None,
+        "e2e": e2e,
+    }
+    line["clocks"] = clocks.summary()
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = sphere_cpu_baseline(scene, args.warmup, args.steps)
+    if pg is not None:
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def run_reference(args):
     world, rank, local, pg = dist_setup()
     if rank != 0:
+        return 0
+    if args.workload == "sphere-lattice":
+        from vxr import scenes
+        scene = scenes.sphere_lattice()
+        base = sphere_cpu_baseline(scene, min(args.warmup, 3), args.steps)
+        line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": min(args.warmup, 3), "ms_per_step": None, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": SPHERE_WORKLOAD, "spheres": scene["spheres"]}, "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
         return 0
     steps = min(args.steps, 24)
     warm = min(args.warmup, 3)
@@ -213,11 +355,14 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-iterations", action="store_true")
     ap.add_argument("--max-pairs", type=int, default=0, help="pair capacity of the world (0: 32 a body)")
+    ap.add_argument("--workload", default="large-mixed", choices=["large-mixed", "sphere-lattice"])
     args = ap.parse_args()
-    if args.impl == "reference":
-        return run_reference(args)
     if args.warmup < 3:
         args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.workload == "sphere-lattice":
+        return run_spheres(args)
 
     world_size, rank, local, pg = dist_setup()
     import torch
