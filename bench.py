@@ -312,9 +312,170 @@ def run_spheres(args):
     return 0
 
 
+BATCH_WORKLOAD = ("batched scenes: 512 independent scenes, bodies log-U[64,4096] each (70% spheres / 30% boxes, the "
+                  "large mixed scene's size distributions), per-scene gravity tilt U(+-5 deg) and mu U[0.3,0.8], "
+                  "dt 1/60 s, 4 substeps, 10 sweeps; one world, steps replayed from a captured CUDA graph")
+
+
+def batch_subset(b, scenes_idx):
+    """The scenes `scenes_idx` of a batch, as a batch of their own."""
+    from vxr import scenes
+    parts = [b["parts"][k] for k in scenes_idx]
+    out = {name: np.concatenate([p[name] for p in parts]) for name in scenes.FIELDS}
+    out.update({"counts": np.asarray([b["counts"][k] for k in scenes_idx], np.int32),
+                "grids": [b["grids"][k] for k in scenes_idx], "walls": [b["walls"][k] for k in scenes_idx],
+                "params": b["params"][list(scenes_idx)], "parts": parts, "substeps": b["substeps"],
+                "sweeps": b["sweeps"], "scenes": len(parts)})
+    out["bodies"] = int(out["counts"].sum())
+    return out
+
+
+def batch_cpu_baseline(b, warm=2, steps=24, scenes_wanted=16):
+    """The OpenMP oracle on a bounded sample of the batch: its first scenes, each a world of its own."""
+    from oracle.box import OracleBoxWorld, lib as orc_lib
+    from vxr import scenes
+    picked = list(range(min(scenes_wanted, len(b["parts"]))))
+    worlds = []
+    for k in picked:
+        part = b["parts"][k]
+        w = OracleBoxWorld(part["bodies"], part["substeps"], part["sweeps"], False, part["grid"], threads=True)
+        for name in scenes.FIELDS:
+            w.set_field(name, part[name])
+        w.set_params(b["params"][k])
+        w.step(warm)
+        worlds.append(w)
+    t0 = time.perf_counter()
+    for w in worlds:
+        w.step(steps)
+    dt = time.perf_counter() - t0
+    bodies = sum(b["parts"][k]["bodies"] for k in picked)
+    for w in worlds:
+        w.close()
+    return {"value": bodies * steps / dt, "unit": UNIT, "cores": int(orc_lib(True).orc_threads()), "kind": "port",
+            "sample": f"the first {len(picked)} scenes ({bodies} bodies), steps {warm}..{warm + steps - 1}, {dt:.1f} s, "
+                      "OpenMP C++ oracle, scene after scene"}
+
+
+def run_batched(args):
+    """Batched scenes: one world of every scene (this rank's share), stepped by CUDA graph replays."""
+    world_size, rank, local, pg = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from vxr import autotune, scenes
+    from vxr.box_simulation import BatchSimulation
+    full = scenes.batched(seed=1)
+    mine = [k for k in range(full["scenes"]) if k % world_size == rank]  # scenes shared out across the ranks
+    b = batch_subset(full, mine) if world_size > 1 else full
+    tune = autotune.tune_batch(b, local)
+    grids = autotune.scaled_grids(b, tune["cell_scale"])
+
+    def make():
+        sim = BatchSimulation(b["counts"], grids, b["substeps"], b["sweeps"], device=local,
+                              schedule=tune["schedule"], solve_blocks_per_sm=tune["solve_blocks_per_sm"])
+        sim.load_state([b[k] for k in scenes.FIELDS], None)
+        sim.scene_params(b["params"])
+        return sim
+
+    sim = make()
+    stream = torch.cuda.ExternalStream(sim.stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    sim.step_and_wait(args.warmup)
+    sim.step_graph(1)  # capture the graph outside the timed region
+    sim.sync()
+    pairs = max(1, args.steps // 2)
+    launches0 = sim.launches()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(pairs)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(pairs)]
+    barrier(pg)
+    torch.cuda.synchronize()
+    with Clocks(local) as clocks:
+        for k in range(pairs):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                starts[k].record(stream)
+            sim.step_graph(1)
+            with torch.cuda.stream(stream):
+                ends[k].record(stream)
+            if k % 10 == 9:
+                sim.sync()
+        rep = sim.sync()
+    torch.cuda.synchronize()
+    barrier(pg)
+    launches = sim.launches() - launches0
+    total_ms = float(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+    steps = 2 * pairs
+    slowest_ms = all_max(pg, total_ms)
+    bodies_all = all_sum(pg, float(b["bodies"]))
+    value = bodies_all * steps / (slowest_ms / 1e3)
+    # the solve kernel's share, from a short profiled run of plain steps after the timed region
+    sim.profile(True)
+    sim.step_and_wait(10)
+    phases = sim.profile(False)
+    activity = sim.activity()
+    solve_ms = phases[3] / 10
+    hbm, which = peaks()
+    b_solve = algorithmic_solve_bytes(b["bodies"], b["substeps"], b["sweeps"], activity["touching"],
+                                      activity["points"], activity["bodies_active"], activity["wall_records"])
+    achieved = b_solve / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
+    sim.close()
+    e2e = None
+    if not args.no_e2e:
+        sim2 = make()
+        for _ in range(args.warmup):
+            sim2.step_and_wait(1)
+            sim2.state()
+        barrier(pg)
+        e2e_steps = min(args.steps, 100)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            sim2.scene_params(b["params"])
+            sim2.step_and_wait(1)
+            sim2.state()
+        e2e_s = all_max(pg, time.perf_counter() - t0)
+        sim2.close()
+        e2e = {"value": bodies_all * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 18 * 4 * b["scenes"],
+               "d2h_bytes_per_step": 13 * 4 * b["bodies"], "steps": e2e_steps}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": slowest_ms / steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "scenes": b["scenes"], "bodies": b["bodies"],
+                   "timed_steps": f"{args.warmup + 2}..{args.warmup + 1 + steps}, as {pairs} replays of a two-step graph",
+                   "l2": "flushed (256 MiB write) before every replay",
+                   "autotuned": {k: tune[k] for k in ("cell_scale", "solve_blocks_per_sm", "schedule", "cached")},
+                   "parallelism": f"scenes shared out over {world_size} ranks" if world_size > 1 else "single"},
+        "phase_ms_per_step": {"broad": phases[0] / 10, "narrow": phases[1] / 10, "colour": phases[2] / 10,
+                              "solve": solve_ms},
+        "last_step": {"touching": rep.touching, "points": rep.points, "rounds": rep.rounds, **activity},
+        "roofline": {"bound": "hbm", "kernel": "k_solve", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "peak_source": which, "bytes_per_launch": b_solve,
+                     "ms_per_launch": solve_ms},
+        "gpu_launches": int(launches),
+        "e2e": e2e,
+    }
+    line["clocks"] = clocks.summary()
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = batch_cpu_baseline(b)
+    if pg is not None:
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def run_reference(args):
     world, rank, local, pg = dist_setup()
     if rank != 0:
+        return 0
+    if args.workload == "batched-scenes":
+        from vxr import scenes
+        base = batch_cpu_baseline(scenes.batched(seed=1), warm=min(args.warmup, 3), steps=min(args.steps, 24))
+        line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world,
+                "steps": min(args.steps, 24), "warmup": min(args.warmup, 3), "ms_per_step": None,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": {"workload": BATCH_WORKLOAD}, "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
         return 0
     if args.workload == "sphere-lattice":
         from vxr import scenes
@@ -355,7 +516,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-iterations", action="store_true")
     ap.add_argument("--max-pairs", type=int, default=0, help="pair capacity of the world (0: 32 a body)")
-    ap.add_argument("--workload", default="large-mixed", choices=["large-mixed", "sphere-lattice"])
+    ap.add_argument("--workload", default="large-mixed", choices=["large-mixed", "sphere-lattice", "batched-scenes"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -363,6 +524,8 @@ def main():
         return run_reference(args)
     if args.workload == "sphere-lattice":
         return run_spheres(args)
+    if args.workload == "batched-scenes":
+        return run_batched(args)
 
     world_size, rank, local, pg = dist_setup()
     import torch

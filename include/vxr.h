@@ -61,6 +61,7 @@ typedef struct {
     int32_t schedule;    /* 0: a grid-wide barrier after every round (default); 1: dependency-driven, each pair or
                             wall item waiting only for its own bodies. Both keep the reference's per-body order of
                             operations and give the same results. */
+    int32_t solve_blocks_per_sm; /* blocks of the solve kernel an SM runs; 0 = as many as fit (the autotuner's knob) */
 } vxr_box_config;
 
 /* What a step took: core/box/BoxStepper.java:308-311 (Report), plus the totals over a vxr_box_step call. */
@@ -215,6 +216,33 @@ int32_t vxr_collide(int32_t bodies, const float* const* fields18, const int32_t*
 int32_t vxr_box_broadphase_static(int32_t bodies, const float* const* fields11, vxr_grid grid, int32_t reach_cells,
                                   float margin, int32_t* first_out, int32_t* second_out, int32_t capacity,
                                   int32_t* result3, void* stream);
+
+/* ---- Batched scenes -----------------------------------------------------------------------------------------------
+ * Many independent scenes stepped as one world: no reference counterpart (the reference runs one BoxStep a scene,
+ * core/box/BoxStep.java:117-198). Bodies are numbered scene after scene; each scene has its own grid (cells in one
+ * key space, end to end, so no body meets another scene's) and its own gravity, walls and friction. The substep,
+ * margin, softness and push are one for the batch. Every scene's step is the one a world of that scene alone would
+ * take, bit for bit: greedy colouring gives each scene's pairs the rounds they get alone. */
+typedef struct {
+    int32_t scenes;
+    const int32_t* bodies;   /* [scenes] bodies of each scene */
+    const vxr_grid* grids;   /* [scenes] each scene's grid (vxr_box_make_grid over its own walls) */
+    int32_t substeps, sweeps, symmetric, max_pairs, device, schedule, solve_blocks_per_sm;
+} vxr_batch_config;
+
+vxr_box_world* vxr_box_create_batch(const vxr_batch_config* config, int32_t* status);
+/* Each scene's 18 parameter words ([scenes * 18], as vxr_box_make_params makes them); VXR_EINVAL where a scene's
+ * substep, margin, softness or push differs from scene 0's. Needed before a batch's first step. vxr_box_params on a
+ * batch gives every scene the same words. */
+int32_t vxr_box_scene_params(vxr_box_world* world, const int32_t* params);
+/* The batch's scene count (0 for a single scene); first_body (scenes + 1 entries, may be null) receives each
+ * scene's first body and the total. */
+int32_t vxr_box_scenes(const vxr_box_world* world, int32_t* first_body);
+
+/* `pairs` x 2 steps as replays of one CUDA graph holding two whole steps, enqueued without waiting (vxr_box_sync
+ * waits and reports). The first call captures the graph; changing the parameters, the measuring switches or the
+ * state captures it again at the next call. Profiling and tracing must be off. */
+int32_t vxr_box_step_graph(vxr_box_world* world, int32_t pairs);
 
 /* ---- The sphere package: XPBD spheres (core/sphere/) ------------------------------------------------------------
  * The reference's SphereSimulation (gui/SphereSimulation.java:33-295) over SphereStep and SphereStepper. A call of

@@ -167,6 +167,19 @@ struct vxr_box_world {
     int events_used = 0;
     double phase_ms[4] = {0, 0, 0, 0};
     long long* activity = nullptr;  // device scratch for vxr_box_activity
+    // batched scenes (vxr_box_create_batch): each scene's parameter words and grid, each body's scene
+    int scenes = 0;
+    int scene_params_set = 0;
+    Params* scene_params = nullptr;  // [scenes]
+    int* body_scene = nullptr;       // [n]
+    int4* scene_grid = nullptr;      // [scenes] nx, ny, nz, first key
+    float* scene_cell = nullptr;     // [scenes]
+    std::vector<int> scene_first;    // [scenes + 1] first body of each scene
+    // a captured pair of steps (vxr_box_step_graph)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    long long graph_launches = 0;  // kernels in the captured pair of steps
+    int capturing = 0;
 };
 
 namespace {
@@ -207,19 +220,41 @@ struct GridDims {
     int reach;  // neighbourhood half-width in cells
 };
 
+// Batched scenes: each body's scene, and each scene's grid (nx, ny, nz, first key) and cell side. The scenes' grids
+// lie end to end in one key space, so a body's neighbourhood never leaves its own scene. Null for a single scene.
+struct SceneGrids {
+    const int* body_scene;
+    const int4* grid;
+    const float* cell;
+};
+
+// The grid a body is binned and searched in: the world's, or its scene's (with that scene's first key).
+__device__ __forceinline__ void grid_of(const GridDims& g, const SceneGrids& sg, int s, int& nx, int& ny, int& nz,
+                                        int& base, float& cell) {
+    nx = g.nx, ny = g.ny, nz = g.nz, base = 0, cell = g.cell;
+    if (sg.body_scene) {
+        const int sc = sg.body_scene[s];
+        const int4 d = sg.grid[sc];
+        nx = d.x, ny = d.y, nz = d.z, base = d.w, cell = sg.cell[sc];
+    }
+}
+
 // bin :74-89, and reach :196-227 for the list.
-__global__ void k_bin(int n, GridDims g, const float4* __restrict__ pose, const float4* __restrict__ turn,
-                      const float4* __restrict__ half, int* __restrict__ keys, float4* __restrict__ reach,
-                      int* __restrict__ cell_count) {
+__global__ void k_bin(int n, GridDims g, SceneGrids sg, const float4* __restrict__ pose,
+                      const float4* __restrict__ turn, const float4* __restrict__ half, int* __restrict__ keys,
+                      float4* __restrict__ reach, int* __restrict__ cell_count) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const float4 p = pose[s];
     const float at[3] = {p.x, p.y, p.z};
-    const int cells[3] = {g.nx, g.ny, g.nz};
+    int gx, gy, gz, base;
+    float cell;
+    grid_of(g, sg, s, gx, gy, gz, base, cell);
+    const int cells[3] = {gx, gy, gz};
     int c[3];
 #pragma unroll
-    for (int a = 0; a < 3; a++) c[a] = (int)fmaxf(0.0f, fminf((float)(cells[a] - 1), floorf(at[a] / g.cell)));
-    const int key = c[0] + cells[0] * (c[1] + cells[1] * c[2]);
+    for (int a = 0; a < 3; a++) c[a] = (int)fmaxf(0.0f, fminf((float)(cells[a] - 1), floorf(at[a] / cell)));
+    const int key = base + (c[0] + cells[0] * (c[1] + cells[1] * c[2]));
     keys[s] = key;
     atomicAdd(&cell_count[key], 1);
     const float4 q = turn[s];
@@ -259,7 +294,7 @@ __global__ void k_stable(int n, const int* __restrict__ keys, const int* __restr
 // list :103-164 with around :230-252: the higher-numbered bodies near s, the first 32 found kept in ascending
 // order, and how many were found. With reach > 1 (cells narrower than the reference's rule) the neighbourhood
 // widens to (2 reach + 1)^3 cells; at reach 1 it is the reference's 27, visited in its order.
-__global__ void k_list(int n, GridDims g, float margin, const float4* __restrict__ pose,
+__global__ void k_list(int n, GridDims g, SceneGrids sg, float margin, const float4* __restrict__ pose,
                        const float4* __restrict__ reach, const int* __restrict__ keys,
                        const int* __restrict__ cell_start, const int* __restrict__ order, int* __restrict__ partner,
                        int* __restrict__ found_out, int* __restrict__ kept_out, Counters* counters) {
@@ -271,16 +306,19 @@ __global__ void k_list(int n, GridDims g, float margin, const float4* __restrict
     const float rch[3] = {rs.x, rs.y, rs.z};
     int slot[SLOTS];
     int found = 0;
-    const int key = keys[s];
-    const int ix = key % g.nx, iy = (key / g.nx) % g.ny, iz = key / (g.nx * g.ny);
+    int gx, gy, gz, base;
+    float cell_side;
+    grid_of(g, sg, s, gx, gy, gz, base, cell_side);
+    const int key = keys[s] - base;
+    const int ix = key % gx, iy = (key / gx) % gy, iz = key / (gx * gy);
     const int side = 2 * g.reach + 1;
     const int around = side * side * side;
     for (int nn = 0; nn < around; nn++) {
         const int jx = ix + (nn % side - g.reach);
         const int jy = iy + ((nn / side) % side - g.reach);
         const int jz = iz + (nn / (side * side) - g.reach);
-        if (!(jx >= 0 && jx < g.nx && jy >= 0 && jy < g.ny && jz >= 0 && jz < g.nz)) continue;
-        const int cell = jx + g.nx * (jy + g.ny * jz);
+        if (!(jx >= 0 && jx < gx && jy >= 0 && jy < gy && jz >= 0 && jz < gz)) continue;
+        const int cell = base + (jx + gx * (jy + gy * jz));
         const int end = cell_start[cell + 1];
         for (int k = cell_start[cell]; k < end; k++) {
             const int o = order[k];
@@ -622,6 +660,8 @@ struct SolveArgs {
     int* used;                     // [2 substeps] solve and relax sweeps each substep ran
     int substeps, sweeps, symmetric;
     Params params;
+    const Params* scene_params;  // batched scenes: each scene's words (gravity, walls, friction differ); else null
+    const int* body_scene;       // [n] each body's scene; else null
     GridBarrier bar;
     unsigned long long* trace;  // null: not traced
     int trace_cap;
@@ -690,14 +730,20 @@ __device__ __forceinline__ void phase_positions(const SolveArgs& A, int slot) {
 // v[i] for a runtime i without indexing a local array (which would move the array to local memory).
 __device__ __forceinline__ float pick3(const float* v, int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
 
+// A body's scene in a batch, or -1 in a single scene; and a parameter word of that scene (the world's words for
+// -1). In a batch the substep, margin, softness and push are one for every scene; gravity, walls and friction are
+// the scene's own.
+__device__ __forceinline__ int scene_of(const SolveArgs& A, int s) { return A.body_scene ? __ldg(&A.body_scene[s]) : -1; }
+__device__ __forceinline__ float word_of(const SolveArgs& A, int sc, int i) {
+    return sc < 0 ? A.params.w[i] : __ldg(&A.scene_params[sc].w[i]);
+}
+
 // Which walls a body may touch: bit w set where the body's bounding sphere comes within the margin of wall w
 // (a bound that holds through f32 rounding: every corner's gap to a wall not in the set exceeds the margin).
-__device__ __forceinline__ unsigned near_walls(float4 pose, float4 hw, const Params& P) {
-    const float margin = P.w[P_MARGIN];
+__device__ __forceinline__ unsigned near_walls(float4 pose, float4 hw, float margin, const float* extent) {
     const float r = hw.w > 0.5f ? hw.x : sqrtf((hw.x * hw.x + hw.y * hw.y) + hw.z * hw.z);
     const float bound = r * 1.01f + 1e-3f + margin;
     const float at[3] = {pose.x, pose.y, pose.z};
-    const float extent[3] = {P.w[P_SX], P.w[P_SY], P.w[P_SZ]};
     unsigned near = 0u;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -711,7 +757,9 @@ __device__ __forceinline__ unsigned near_walls(float4 pose, float4 hw, const Par
 // The order of the list does not matter: each body's walls touch that body alone.
 __device__ __forceinline__ void list_wall_body(const SolveArgs& A, int s, float4 pose, int slot) {
     const float4 hw = __ldg(&A.b.half[s]);
-    const bool list = __ldcg(&A.wmask[s]) != 0ull || near_walls(pose, hw, A.params) != 0u;
+    const int sc = scene_of(A, s);
+    const float extent[3] = {word_of(A, sc, P_SX), word_of(A, sc, P_SY), word_of(A, sc, P_SZ)};
+    const bool list = __ldcg(&A.wmask[s]) != 0ull || near_walls(pose, hw, A.params.w[P_MARGIN], extent) != 0u;
     if (list) {  // spheres from the front of the list, boxes from the back: a warp's bodies take the same path
         if (hw.w > 0.5f) A.wall_list[atomicAdd(&A.wall_count[2 * slot], 1)] = s;
         else A.wall_list[A.n - 1 - atomicAdd(&A.wall_count[2 * slot + 1], 1)] = s;
@@ -729,9 +777,10 @@ __device__ __forceinline__ void phase_velocities_and_list(const SolveArgs& A, in
         A.listed[s] = 0;
         if (!(pose.w > 0.0f)) continue;
         float4 v = __ldcg(&A.b.vel[s]);
-        v.x = v.x + h * A.params.w[P_GX];
-        v.y = v.y + h * A.params.w[P_GY];
-        v.z = v.z + h * A.params.w[P_GZ];
+        const int sc = scene_of(A, s);
+        v.x = v.x + h * word_of(A, sc, P_GX);
+        v.y = v.y + h * word_of(A, sc, P_GY);
+        v.z = v.z + h * word_of(A, sc, P_GZ);
         __stcg(&A.b.vel[s], v);
         list_wall_body(A, s, pose, slot);
     }
@@ -744,12 +793,14 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
                                          unsigned* track = nullptr) {
     const Params& P = A.params;
     const float margin = P.w[P_MARGIN];
-    const float extent[3] = {P.w[P_SX], P.w[P_SY], P.w[P_SZ]};
+    const int sc = scene_of(A, s);
+    const float extent[3] = {word_of(A, sc, P_SX), word_of(A, sc, P_SY), word_of(A, sc, P_SZ)};
+    const float mu_rolling = word_of(A, sc, P_MU_ROLLING);
     unsigned long long mask = __ldcg(&A.wmask[s]);
     const float4 pose = make_float4(box.at[0], box.at[1], box.at[2], box.im);
     const float4 hw = make_float4(box.half[0], box.half[1], box.half[2], box.shape);
     const bool sphere = hw.w > 0.5f;
-    const unsigned near = sweep == WARM ? 0u : near_walls(pose, hw, P);
+    const unsigned near = sweep == WARM ? 0u : near_walls(pose, hw, margin, extent);
     unsigned held_walls = 0u;
 #pragma unroll
     for (int wl = 0; wl < 6; wl++) {
@@ -758,7 +809,11 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
     }
     const unsigned visit = near | held_walls;
     if (visit == 0u) return false;
-    const Soft soft(P, true);
+    Soft soft(P, true);
+    if (sc >= 0) {
+        soft.mu_static = word_of(A, sc, P_MU_STATIC);
+        soft.mu_kinetic = word_of(A, sc, P_MU_KINETIC);
+    }
     bool touched = false;
     for (int order = 0; order < 6; order++) {
         const int wall = reverse ? 5 - order : order;
@@ -788,7 +843,7 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
             }
             if (rolled || (sweep != WARM && nonzero_bits(rec))) {
                 float4 rr = rolled ? __ldcg(&A.wroll[(long)s * 6 + wall]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                roll<false>(sweep, box, box, box.half[0], rec.x, rr, P.w[P_MU_ROLLING]);
+                roll<false>(sweep, box, box, box.half[0], rec.x, rr, mu_rolling);
                 if (sweep != WARM) {
                     __stcg(&A.wroll[(long)s * 6 + wall], rr);
                     mask = nonzero_bits(rr) ? (mask | (1ull << rbit)) : (mask & ~(1ull << rbit));
@@ -858,6 +913,13 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
         soft.mass_scale = P.w[P_STATIC_MASS_SCALE];
         soft.impulse_scale = P.w[P_STATIC_IMPULSE_SCALE];
     }
+    const int sc = scene_of(A, ia);
+    float mu_rolling = P.w[P_MU_ROLLING];
+    if (sc >= 0) {
+        soft.mu_static = word_of(A, sc, P_MU_STATIC);
+        soft.mu_kinetic = word_of(A, sc, P_MU_KINETIC);
+        mu_rolling = word_of(A, sc, P_MU_ROLLING);
+    }
     const float n[3] = {head.x, head.y, head.z};
     const bool anySphere = first.sphere() || second.sphere();
     for (int order = 0; order < MOST_POINTS; order++) {
@@ -900,7 +962,7 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
             if (first.sphere() && second.sphere())
                 radius = (first.half[0] * second.half[0]) / (first.half[0] + second.half[0]);
             float4 rr = __ldcg(&A.pairs.impr[at]);
-            roll<true>(sweep, first, second, radius, rec.x, rr, P.w[P_MU_ROLLING]);
+            roll<true>(sweep, first, second, radius, rec.x, rr, mu_rolling);
             if (sweep != WARM) __stcg(&A.pairs.impr[at], rr);
         }
     }
@@ -1165,7 +1227,21 @@ __global__ void k_inverse_inertia(int n, const float4* __restrict__ pose, const 
 int blocks_for(long n, int threads) { return (int)std::max<long>(1, (n + threads - 1) / threads); }
 
 int launch_cooperative(vxr_box_world* w, const void* fn, int blocks, int threads, void** args) {
-    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, 0, w->stream);
+    cudaError_t e;
+    if (w->capturing) {  // the form a stream capture records as a cooperative kernel node
+        cudaLaunchConfig_t c = {};
+        c.gridDim = dim3(blocks);
+        c.blockDim = dim3(threads);
+        c.stream = w->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        c.attrs = attr;
+        c.numAttrs = 1;
+        e = cudaLaunchKernelExC(&c, fn, args);
+    } else {
+        e = cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads), args, 0, w->stream);
+    }
     if (e != cudaSuccess) return fail(w, std::string("cooperative launch: ") + cudaGetErrorString(e));
     return VXR_OK;
 }
@@ -1200,6 +1276,10 @@ int mark(vxr_box_world* w, int which) {
 int enqueue_step(vxr_box_world* w) {
     cudaStream_t st = w->stream;
     const int n = w->n;
+    if (w->scenes > 0 && !w->scene_params_set) {
+        w->error = "a batch of scenes needs its scenes' parameters (vxr_box_scene_params) before a step";
+        return VXR_EINVAL;
+    }
     int rc0 = mark(w, 0);
     if (rc0) return rc0;
     VXR_CUDA(cudaMemsetAsync(w->counters, 0, sizeof(Counters), st));
@@ -1211,13 +1291,14 @@ int enqueue_step(vxr_box_world* w) {
         const float margin = w->params.w[P_MARGIN];
         VXR_CUDA(cudaMemsetAsync(w->cell_count, 0, sizeof(int) * w->cells, st));
         VXR_CUDA(cudaMemsetAsync(w->cell_fill, 0, sizeof(int) * w->cells, st));
-        k_bin<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, g, w->b.pose, w->b.turn, w->b.half, w->keys, w->reach,
+        const SceneGrids sg{w->body_scene, w->scene_grid, w->scene_cell};
+        k_bin<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, g, sg, w->b.pose, w->b.turn, w->b.half, w->keys, w->reach,
                                                          w->cell_count);
         exclusive_scan(w->cell_count, w->cell_start, w->cells, w->scan_tiles, st);
         k_scatter<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->keys, w->cell_start, w->cell_fill,
                                                              w->order_tmp);
         k_stable<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->keys, w->cell_start, w->order_tmp, w->order);
-        k_list<<<blocks_for(n, 128), 128, 0, st>>>(n, g, margin, w->b.pose, w->reach, w->keys, w->cell_start,
+        k_list<<<blocks_for(n, 128), 128, 0, st>>>(n, g, sg, margin, w->b.pose, w->reach, w->keys, w->cell_start,
                                                   w->order, w->partner, w->found, w->kept, w->counters);
         exclusive_scan(w->kept, w->cand_start, n, w->scan_tiles, st);
         k_candidates<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->kept, w->cand_start, w->partner,
@@ -1299,6 +1380,8 @@ int enqueue_step(vxr_box_world* w) {
         A.used = w->used;
         A.symmetric = w->symmetric;
         A.params = w->params;
+        A.scene_params = w->scene_params;
+        A.body_scene = w->body_scene;
         A.bar = barrier_of(w);
         A.trace = w->tracing ? w->trace : nullptr;
         A.trace_cap = w->trace_cap;
@@ -1316,6 +1399,14 @@ int enqueue_step(vxr_box_world* w) {
     return VXR_OK;
 }
 
+// Forgets a captured pair of steps: what it baked in (parameters, the pair generation, switches) has changed.
+void drop_graph(vxr_box_world* w) {
+    if (w->graph_exec) cudaGraphExecDestroy(w->graph_exec);
+    if (w->graph) cudaGraphDestroy(w->graph);
+    w->graph_exec = nullptr;
+    w->graph = nullptr;
+}
+
 // Every impulse, wall record and pair list back to zero, as the reference's runner.clear() leaves them.
 int clear_dynamic(vxr_box_world* w) {
     cudaStream_t st = w->stream;
@@ -1328,6 +1419,7 @@ int clear_dynamic(vxr_box_world* w) {
     if (w->has_grid)
         for (int g = 0; g < 2; g++) VXR_CUDA(cudaMemsetAsync(w->gen[g].tstart, 0, sizeof(int) * ((size_t)n + 1), st));
     w->cur = 0;
+    drop_graph(w);
     return VXR_OK;
 }
 
@@ -1570,7 +1662,9 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     // Occupancy of the cooperative kernels: every block must be resident at once.
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve, SOLVE_THREADS, 0);
-    w->solve_blocks = std::max(1, per_sm) * w->sms;
+    per_sm = std::max(1, per_sm);
+    if (cfg->solve_blocks_per_sm > 0) per_sm = std::min(per_sm, (int)cfg->solve_blocks_per_sm);
+    w->solve_blocks = per_sm * w->sms;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_colour, THREADS, 0);
     w->colour_blocks = std::max(1, per_sm) * w->sms;
     // Everything starts at zero, as the reference's buffers do; every orientation the identity.
@@ -1603,6 +1697,7 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
 void vxr_box_destroy(vxr_box_world* w) {
     if (!w) return;
     if (w->stream) cudaStreamSynchronize(w->stream);
+    drop_graph(w);
     for (void* p : w->allocations) cudaFree(p);
     if (w->pinned) cudaFreeHost(w->pinned);
     if (w->host_totals) cudaFreeHost(w->host_totals);
@@ -1617,7 +1712,161 @@ const char* vxr_box_error(const vxr_box_world* w) { return w ? w->error.c_str() 
 
 int32_t vxr_box_params(vxr_box_world* w, const int32_t* params) {
     if (!w || !params) return VXR_EINVAL;
+    if (w->scenes > 0) {  // a batch: the same words for every scene
+        std::vector<int32_t> all((size_t)w->scenes * P_COUNT);
+        for (int sc = 0; sc < w->scenes; sc++) std::memcpy(&all[(size_t)sc * P_COUNT], params, sizeof(int32_t) * P_COUNT);
+        return vxr_box_scene_params(w, all.data());
+    }
+    drop_graph(w);
     std::memcpy(w->params.w, params, sizeof(float) * P_COUNT);
+    return VXR_OK;
+}
+
+int32_t vxr_box_scene_params(vxr_box_world* w, const int32_t* params) {
+    if (!w || !params) return VXR_EINVAL;
+    if (w->scenes == 0) {
+        w->error = "not a batch of scenes";
+        return VXR_EINVAL;
+    }
+    // the words every scene shares: the substep, the margin, the softness and the push
+    const int shared[] = {P_H, P_MARGIN, P_BIAS, P_MASS_SCALE, P_IMPULSE_SCALE, P_STATIC_BIAS, P_STATIC_MASS_SCALE,
+                          P_STATIC_IMPULSE_SCALE, P_PUSH};
+    for (int sc = 1; sc < w->scenes; sc++)
+        for (int k : shared)
+            if (params[(size_t)sc * P_COUNT + k] != params[k]) {
+                w->error = "scene " + std::to_string(sc) + " differs from scene 0 in word " + std::to_string(k) +
+                           " (the substep, margin, softness and push are one for a batch)";
+                return VXR_EINVAL;
+            }
+    drop_graph(w);
+    std::memcpy(w->params.w, params, sizeof(float) * P_COUNT);
+    VXR_CUDA(cudaMemcpyAsync(w->scene_params, params, sizeof(Params) * w->scenes, cudaMemcpyHostToDevice, w->stream));
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    w->scene_params_set = 1;
+    return VXR_OK;
+}
+
+vxr_box_world* vxr_box_create_batch(const vxr_batch_config* cfg, int32_t* status) {
+    auto set = [&](int32_t s) {
+        if (status) *status = s;
+    };
+    if (!cfg || cfg->scenes < 1 || !cfg->bodies || !cfg->grids) {
+        set(VXR_EINVAL);
+        return nullptr;
+    }
+    long total = 0, cells = 0;
+    for (int sc = 0; sc < cfg->scenes; sc++) {
+        const vxr_grid g = cfg->grids[sc];
+        if (cfg->bodies[sc] < 1 || g.nx < 1 || g.ny < 1 || g.nz < 1 || !(g.cell > 0)) {
+            set(VXR_EINVAL);
+            return nullptr;
+        }
+        total += cfg->bodies[sc];
+        cells += (long)g.nx * g.ny * g.nz;
+    }
+    if (total < 2 || total > (1L << 28) || cells > (1L << 30)) {
+        set(VXR_EINVAL);
+        return nullptr;
+    }
+    vxr_box_config c = {};
+    c.bodies = (int32_t)total;
+    c.substeps = cfg->substeps;
+    c.sweeps = cfg->sweeps;
+    c.symmetric = cfg->symmetric;
+    c.grid.nx = (int32_t)cells;  // one key space for every scene's grid, end to end
+    c.grid.ny = 1;
+    c.grid.nz = 1;
+    c.grid.cell = 1.0f;
+    c.reach_cells = 1;
+    c.max_pairs = cfg->max_pairs;
+    c.device = cfg->device;
+    c.schedule = cfg->schedule;
+    c.solve_blocks_per_sm = cfg->solve_blocks_per_sm;
+    vxr_box_world* w = vxr_box_create(&c, status);
+    if (!w) return nullptr;
+    const int scenes = cfg->scenes;
+    w->scenes = scenes;
+    int rc = 0;
+    rc |= alloc(w, &w->scene_params, scenes);
+    rc |= alloc(w, &w->body_scene, w->n);
+    rc |= alloc(w, &w->scene_grid, scenes);
+    rc |= alloc(w, &w->scene_cell, scenes);
+    if (rc) {
+        set(VXR_ECUDA);
+        vxr_box_destroy(w);
+        return nullptr;
+    }
+    std::vector<int> body_scene(w->n);
+    std::vector<int4> grid(scenes);
+    std::vector<float> cell(scenes);
+    w->scene_first.assign(scenes + 1, 0);
+    int first = 0, base = 0;
+    for (int sc = 0; sc < scenes; sc++) {
+        const vxr_grid g = cfg->grids[sc];
+        w->scene_first[sc] = first;
+        for (int k = 0; k < cfg->bodies[sc]; k++) body_scene[first + k] = sc;
+        first += cfg->bodies[sc];
+        grid[sc] = make_int4(g.nx, g.ny, g.nz, base);
+        cell[sc] = g.cell;
+        base += g.nx * g.ny * g.nz;
+    }
+    w->scene_first[scenes] = first;
+    if (cudaMemcpy(w->body_scene, body_scene.data(), sizeof(int) * w->n, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(w->scene_grid, grid.data(), sizeof(int4) * scenes, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(w->scene_cell, cell.data(), sizeof(float) * scenes, cudaMemcpyHostToDevice) != cudaSuccess) {
+        set(VXR_ECUDA);
+        vxr_box_destroy(w);
+        return nullptr;
+    }
+    set(VXR_OK);
+    return w;
+}
+
+int32_t vxr_box_scenes(const vxr_box_world* w, int32_t* first_body) {
+    if (!w) return -VXR_EINVAL;
+    if (first_body)
+        for (int sc = 0; sc <= w->scenes && w->scenes > 0; sc++) first_body[sc] = w->scene_first[sc];
+    return w->scenes;
+}
+
+int32_t vxr_box_step_graph(vxr_box_world* w, int32_t pairs) {
+    if (!w || pairs < 0) return VXR_EINVAL;
+    if (w->profile || w->tracing) {
+        w->error = "a captured step records no profile or trace: switch them off first";
+        return VXR_EINVAL;
+    }
+    cudaSetDevice(w->device);
+    if (!w->graph_exec) {
+        const long long before = w->launches;
+        VXR_CUDA(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
+        w->capturing = 1;
+        int rc = enqueue_step(w);
+        if (rc == VXR_OK) rc = enqueue_step(w);  // two steps: the pair generations come back to where they were
+        w->capturing = 0;
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(w->stream, &g);
+        w->launches = before;
+        if (rc != VXR_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            if (rc == VXR_OK) w->error = std::string("stream capture: ") + cudaGetErrorString(e);
+            return rc != VXR_OK ? rc : VXR_ECUDA;
+        }
+        w->graph = g;
+        VXR_CUDA(cudaGraphInstantiate(&w->graph_exec, g, 0));
+        size_t nodes = 0;
+        cudaGraphGetNodes(g, nullptr, &nodes);
+        w->graph_launches = 0;
+        std::vector<cudaGraphNode_t> all(nodes);
+        if (nodes) cudaGraphGetNodes(g, all.data(), &nodes);
+        for (cudaGraphNode_t node : all) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(node, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) w->graph_launches++;
+        }
+    }
+    for (int k = 0; k < pairs; k++) {
+        VXR_CUDA(cudaGraphLaunch(w->graph_exec, w->stream));
+        w->launches += w->graph_launches;
+    }
     return VXR_OK;
 }
 
@@ -1830,6 +2079,7 @@ int32_t vxr_box_touching(vxr_box_world* w, int32_t* first, int32_t* second, int3
 
 int32_t vxr_box_trace(vxr_box_world* w, int32_t enable, int64_t* out, int32_t capacity) {
     if (!w) return -VXR_EINVAL;
+    if (enable) drop_graph(w);
     int len = 0;
     if (out && w->trace) {
         Counters c;
@@ -1904,6 +2154,7 @@ long long vxr_box_launches(vxr_box_world* w) { return w ? w->launches : -1; }
 
 int32_t vxr_box_measure(vxr_box_world* w, int32_t residual, int32_t cold_start, int32_t sweeps, float tolerance) {
     if (!w || sweeps < 0 || sweeps > w->sweeps || !(tolerance >= 0.0f)) return VXR_EINVAL;
+    drop_graph(w);
     w->measure = residual ? 1 : 0;
     w->cold = cold_start ? 1 : 0;
     w->active_sweeps = sweeps > 0 ? sweeps : w->sweeps;
@@ -1924,6 +2175,7 @@ int32_t vxr_box_residuals(vxr_box_world* w, float* out, int32_t capacity, int32_
 
 int32_t vxr_box_profile(vxr_box_world* w, int32_t enable, double* phase_ms4) {
     if (!w) return VXR_EINVAL;
+    if (enable) drop_graph(w);
     if (phase_ms4)
         for (int k = 0; k < 4; k++) phase_ms4[k] = w->phase_ms[k];
     for (int k = 0; k < 4; k++) w->phase_ms[k] = 0.0;
@@ -2156,11 +2408,12 @@ extern "C" int32_t vxr_box_broadphase_static(int32_t bodies, const float* const*
                    fields11[6], fields11[7], fields11[8], fields11[9], fields11[10]};
     GridDims g{grid.nx, grid.ny, grid.nz, grid.cell, reach_cells > 0 ? reach_cells : 1};
     k_pack_static<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, f, pose, turn, half);
-    k_bin<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, g, pose, turn, half, keys, reach, cell_count);
+    const SceneGrids none{nullptr, nullptr, nullptr};
+    k_bin<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, g, none, pose, turn, half, keys, reach, cell_count);
     exclusive_scan(cell_count, cell_start, (int)cells, tiles, st);
     k_scatter<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, keys, cell_start, cell_fill, order_tmp);
     k_stable<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, keys, cell_start, order_tmp, order);
-    k_list<<<blocks_for(n, 128), 128, 0, st>>>(n, g, margin, pose, reach, keys, cell_start, order, partner, found,
+    k_list<<<blocks_for(n, 128), 128, 0, st>>>(n, g, none, margin, pose, reach, keys, cell_start, order, partner, found,
                                               kept, counters);
     exclusive_scan(kept, cand_start, n, tiles, st);
     k_candidates<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, capacity, kept, cand_start, partner, first_out,

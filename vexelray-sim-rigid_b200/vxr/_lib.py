@@ -22,7 +22,8 @@ SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_c
            "vxr_box_step_async", "vxr_box_sync", "vxr_box_stream", "vxr_box_state", "vxr_box_read_shown",
            "vxr_box_touching", "vxr_box_candidates", "vxr_box_walls", "vxr_box_colour_waves", "vxr_collide",
            "vxr_box_launches", "vxr_box_profile", "vxr_box_activity", "vxr_box_trace", "vxr_box_broadphase_static",
-           "vxr_box_measure", "vxr_box_residuals",
+           "vxr_box_measure", "vxr_box_residuals", "vxr_box_create_batch", "vxr_box_scene_params",
+           "vxr_box_scenes", "vxr_box_step_graph",
            "vxr_sphere_make_params", "vxr_sphere_make_grid", "vxr_sphere_create", "vxr_sphere_destroy",
            "vxr_sphere_error", "vxr_sphere_start", "vxr_sphere_load_state", "vxr_sphere_params", "vxr_sphere_friction",
            "vxr_sphere_step", "vxr_sphere_step_async", "vxr_sphere_sync", "vxr_sphere_stream", "vxr_sphere_state",
@@ -43,7 +44,15 @@ class Grid(ctypes.Structure):
 class BoxConfig(ctypes.Structure):
     _fields_ = [("bodies", ctypes.c_int32), ("substeps", ctypes.c_int32), ("sweeps", ctypes.c_int32),
                 ("symmetric", ctypes.c_int32), ("grid", Grid), ("reach_cells", ctypes.c_int32),
-                ("max_pairs", ctypes.c_int32), ("device", ctypes.c_int32), ("schedule", ctypes.c_int32)]
+                ("max_pairs", ctypes.c_int32), ("device", ctypes.c_int32), ("schedule", ctypes.c_int32),
+                ("solve_blocks_per_sm", ctypes.c_int32)]
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("scenes", ctypes.c_int32), ("bodies", ctypes.c_void_p), ("grids", ctypes.c_void_p),
+                ("substeps", ctypes.c_int32), ("sweeps", ctypes.c_int32), ("symmetric", ctypes.c_int32),
+                ("max_pairs", ctypes.c_int32), ("device", ctypes.c_int32), ("schedule", ctypes.c_int32),
+                ("solve_blocks_per_sm", ctypes.c_int32)]
 
 
 class BoxReport(ctypes.Structure):
@@ -129,6 +138,14 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_broadphase_static.restype = i32
         L.vxr_collide.argtypes = [i32, vp, vp, i32, vp, vp]
         L.vxr_collide.restype = i32
+        L.vxr_box_create_batch.argtypes = [ctypes.POINTER(BatchConfig), ctypes.POINTER(i32)]
+        L.vxr_box_create_batch.restype = vp
+        L.vxr_box_scene_params.argtypes = [vp, vp]
+        L.vxr_box_scene_params.restype = i32
+        L.vxr_box_scenes.argtypes = [vp, vp]
+        L.vxr_box_scenes.restype = i32
+        L.vxr_box_step_graph.argtypes = [vp, i32]
+        L.vxr_box_step_graph.restype = i32
         L.vxr_sphere_make_params.argtypes = [f64] * 8 + [i32] + [f64] * 4 + [vp]
         L.vxr_sphere_make_params.restype = i32
         L.vxr_sphere_make_grid.argtypes = [f64] * 4 + [ctypes.POINTER(Grid)]

@@ -13,7 +13,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import boxes as B
-from ._lib import BoxConfig, BoxReport, Grid, VxrError, lib, ptr, ptr_array
+from ._lib import BatchConfig, BoxConfig, BoxReport, Grid, VxrError, lib, ptr, ptr_array
 
 STATE_FIELDS = ["x", "y", "z", "u", "v", "w", "lx", "ly", "lz", "qx", "qy", "qz", "qw"]
 ALL_FIELDS = STATE_FIELDS + ["im", "hx", "hy", "hz", "shape"]
@@ -50,7 +50,13 @@ class BoxSimulation:
 
     def __init__(self, bodies: int, substeps: int, sweeps: int = B.WALL_PASSES, symmetric: bool = False,
                  grid: B.Grid | None = None, reach_cells: int = 0, max_pairs: int = 0, device: int = 0,
-                 schedule: int = 0):
+                 schedule: int = 0, solve_blocks_per_sm: int = 0, _handle=None):
+        if _handle is not None:  # made by BatchSimulation
+            self.L = lib()
+            self.h = _handle
+            self.n, self.substeps, self.sweeps, self.grid = bodies, substeps, sweeps, grid
+            self._last = Report(0, 0, 0, 0, 0)
+            return
         if bodies < 1 or substeps < 1 or sweeps < 1:
             raise ValueError(f"a step needs bodies, substeps and sweeps, got {bodies}, {substeps} and {sweeps}")
         self.L = lib()
@@ -62,6 +68,7 @@ class BoxSimulation:
         cfg.max_pairs = max_pairs
         cfg.device = device
         cfg.schedule = schedule
+        cfg.solve_blocks_per_sm = solve_blocks_per_sm
         status = ctypes.c_int32(0)
         self.h = self.L.vxr_box_create(ctypes.byref(cfg), ctypes.byref(status))
         if not self.h:
@@ -97,6 +104,16 @@ class BoxSimulation:
         pb = np.ascontiguousarray(params, dtype=np.int32)
         self._check(self.L.vxr_box_load_state(self.h, ptr_array(f), ptr(pb)))
 
+    def load_state(self, fields18, params=None):
+        """Starts from the 18 fields x y z u v w lx ly lz qx qy qz qw im hx hy hz shape; params None keeps the
+        world's (a batch takes its scenes' words with BatchSimulation.scene_params)."""
+        f = [np.ascontiguousarray(a, dtype=np.float32) for a in fields18]
+        for a in f:
+            if a.shape != (self.n,):
+                raise ValueError(f"every field holds {self.n} floats")
+        pb = None if params is None else np.ascontiguousarray(params, dtype=np.int32)
+        self._check(self.L.vxr_box_load_state(self.h, ptr_array(f), ptr(pb)))
+
     def params(self, params):
         pb = np.ascontiguousarray(params, dtype=np.int32)
         self._check(self.L.vxr_box_params(self.h, ptr(pb)))
@@ -111,6 +128,10 @@ class BoxSimulation:
 
     def step(self, steps: int = 1) -> Report:
         return self.step_and_wait(steps)
+
+    def step_graph(self, pairs: int = 1) -> None:
+        """pairs x 2 steps as replays of one captured CUDA graph of two whole steps, not waited for (sync waits)."""
+        self._check(self.L.vxr_box_step_graph(self.h, pairs))
 
     def step_async(self, steps: int = 1):
         self._check(self.L.vxr_box_step_async(self.h, steps))
@@ -262,3 +283,34 @@ def collide_pairs(fields18, param_bits, pairs) -> np.ndarray:
     if rc:
         raise VxrError(rc, "vxr_collide failed")
     return out
+
+
+class BatchSimulation(BoxSimulation):
+    """Many independent scenes stepped as one world (vxr_box_create_batch): bodies numbered scene after scene, each
+    scene with its own grid, gravity, walls and friction. Every BoxSimulation call applies to the whole batch; the
+    state arrays hold every scene's bodies in order (``first`` gives each scene's first body)."""
+
+    def __init__(self, bodies_per_scene, grids, substeps: int, sweeps: int, symmetric: bool = False,
+                 max_pairs: int = 0, device: int = 0, schedule: int = 0, solve_blocks_per_sm: int = 0):
+        counts = np.ascontiguousarray(bodies_per_scene, dtype=np.int32)
+        table = (Grid * len(grids))(*[Grid(g.nx, g.ny, g.nz, g.cell) for g in grids])
+        cfg = BatchConfig()
+        cfg.scenes = len(counts)
+        cfg.bodies = counts.ctypes.data
+        cfg.grids = ctypes.cast(table, ctypes.c_void_p)
+        cfg.substeps, cfg.sweeps, cfg.symmetric = substeps, sweeps, int(bool(symmetric))
+        cfg.max_pairs, cfg.device, cfg.schedule, cfg.solve_blocks_per_sm = max_pairs, device, schedule, solve_blocks_per_sm
+        status = ctypes.c_int32(0)
+        h = lib().vxr_box_create_batch(ctypes.byref(cfg), ctypes.byref(status))
+        if not h:
+            raise VxrError(status.value, "vxr_box_create_batch failed")
+        super().__init__(int(counts.sum()), substeps, sweeps, symmetric, None, _handle=h)
+        self.scenes = len(counts)
+        first = np.zeros(self.scenes + 1, np.int32)
+        lib().vxr_box_scenes(self.h, ptr(first))
+        self.first = first
+
+    def scene_params(self, params) -> None:
+        """Each scene's 18 words, shape (scenes, 18)."""
+        p = np.ascontiguousarray(params, dtype=np.int32).reshape(self.scenes, 18)
+        self._check(self.L.vxr_box_scene_params(self.h, ptr(p)))

@@ -82,6 +82,44 @@ def sub_volume(bodies_full: int, fraction: float, seed: int = 1) -> dict:
     return large_mixed(int(round(bodies_full * fraction)), seed=seed, volume=(128.0 * side, 64.0, 128.0 * side))
 
 
+def batched(scenes: int = 512, seed: int = 1, smallest: int = 64, largest: int = 4096, sphere_share: float = 0.7,
+            dt: float = 1 / 60, substeps: int = 4, sweeps: int = 10, margin: float = 0.005,
+            mu_rolling: float = 0.1) -> dict:
+    """Independent scenes for one batched world: each scene's body count log-uniform in 64-4096, a 70/30
+    sphere/box mix with the large mixed scene's size, orientation, velocity and density distributions, its own
+    gravity tilted by up to 5 degrees about a random horizontal axis, and its own mu in 0.3-0.8 (static = kinetic).
+    dt 1/60 s, 4 substeps; the configuration names no sweep count, so the large mixed scene's 10 are used.
+
+    Each scene drops at the large mixed scene's body density (0.25 a cubic metre) into its own walled box a x a x a
+    with a = (8 N)^(1/3) (bodies start in the lower half). Returns the concatenated fields (scene after scene), each
+    scene's count, grid and 18 parameter words."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    counts = np.round(np.exp(rng.uniform(math.log(smallest), math.log(largest), scenes))).astype(np.int32)
+    parts, grids, words, walls = [], [], [], []
+    for k in range(scenes):
+        n = int(counts[k])
+        a = (8.0 * n) ** (1.0 / 3.0)
+        sc = large_mixed(n, seed=int(rng.integers(1 << 31)), volume=(a, a / 2, a), sphere_share=sphere_share,
+                         dt=dt, substeps=substeps, sweeps=sweeps, margin=margin, mu_rolling=mu_rolling, height=a)
+        tilt = math.radians(rng.uniform(-5.0, 5.0))
+        about = rng.uniform(0.0, 2.0 * math.pi)
+        g = (9.81 * math.sin(tilt) * math.cos(about), -9.81 * math.cos(tilt), 9.81 * math.sin(tilt) * math.sin(about))
+        mu = float(rng.uniform(0.3, 0.8))
+        sx, sy, sz = sc["walls"]
+        words.append(B.params(dt / substeps, g[0], g[1], g[2], sx, sy, sz, mu, mu, margin, mu_rolling))
+        grids.append(sc["grid"])
+        walls.append((sx, sy, sz))
+        parts.append(sc)
+    out = {name: np.concatenate([p[name] for p in parts]) for name in FIELDS}
+    out.update({
+        "scenes": scenes, "counts": counts, "bodies": int(counts.sum()), "grids": grids,
+        "params": np.stack(words), "walls": walls, "dt": dt, "substeps": substeps, "sweeps": sweeps,
+        "margin": margin, "parts": parts,
+        "name": f"{scenes} batched scenes, {int(counts.sum())} bodies ({sphere_share:.0%} spheres), seed {seed}",
+    })
+    return out
+
+
 def sphere_lattice(seed: int = 1, nx: int = 16, ny: int = 8, nz: int = 8, spacing: float = 1.2,
                    jitter: float = 0.05, radius: float = 0.5, density: float = 1000.0, box: float = 20.0,
                    height: float = 40.0) -> dict:
