@@ -244,6 +244,45 @@ int32_t vxr_box_scenes(const vxr_box_world* world, int32_t* first_body);
  * state captures it again at the next call. Profiling and tracing must be off. */
 int32_t vxr_box_step_graph(vxr_box_world* world, int32_t pairs);
 
+/* ---- The learned warm start's network ---------------------------------------------------------------------------
+ * No reference counterpart: the reference warm-starts a contact with the impulses it took last step
+ * (core/box/BoxPairs.java:191-267). This is a 16 -> 64 -> 64 -> 2 multilayer perceptron with SiLU activations, BF16
+ * weights and activations, FP32 accumulation, run and trained by this library's tcgen05 kernels; it predicts a
+ * contact's starting normal and friction impulse from 16 local features (vxr_box_features gives them). Parameters are
+ * FP32 masters in the order w1 [16][64], b1 [64], w2 [64][64], b2 [64], w3 [64][2], b3 [2]. */
+#define VXR_MLP_PARAMS 5378
+typedef struct vxr_mlp vxr_mlp;
+/* A network with He-initialised weights from `seed`, on `device`. */
+vxr_mlp* vxr_mlp_create(int32_t device, uint64_t seed, int32_t* status);
+void vxr_mlp_destroy(vxr_mlp* net);
+const char* vxr_mlp_error(const vxr_mlp* net);
+/* Parameters and the inputs' normalisation (x - mean) * inv_std; any pointer may be null (kept). Setting the
+ * parameters restarts Adam. */
+int32_t vxr_mlp_set(vxr_mlp* net, const float* params, const float* mean16, const float* inv_std16);
+int32_t vxr_mlp_get(vxr_mlp* net, float* params, float* mean16, float* inv_std16);
+/* Forward over `rows` host rows of 16 features: out2 receives (normal, friction) a row. */
+int32_t vxr_mlp_forward(vxr_mlp* net, const float* features, int32_t rows, float* out2);
+/* The gradients of the loss sum over rows |y - t|^2 / rows at the current parameters (no update), and the loss. */
+int32_t vxr_mlp_gradients(vxr_mlp* net, const float* features, const float* targets, int32_t rows, float* grads,
+                          float* loss);
+/* Adam (beta 0.9, 0.999, eps 1e-8) at learning rate lr over `epochs` shuffled passes of minibatches of `batch`
+ * rows; the normalisation is set from the training features first. epoch_loss (may be null) receives each epoch's
+ * mean minibatch loss. */
+int32_t vxr_mlp_train(vxr_mlp* net, const float* features, const float* targets, int32_t rows, int32_t epochs,
+                      int32_t batch, float lr, uint64_t seed, float* epoch_loss);
+
+/* The learned warm start in a box world. mode 0: off (the reference's carried impulses); 1: each step gathers 16
+ * features a contact point at its start and the impulses its solve reached (vxr_box_features reads them); 2: each
+ * step starts every contact point from `net`'s predicted normal and friction impulse instead of the carried ones.
+ * Features: gap, relative normal and tangential speed, the two inverse masses, the two inverse inertias along the
+ * normal, the carried normal and friction impulse, the two bodies' touching pair counts, the feature kind one-hot
+ * (face of first, face of second, edge, sphere) and the normal's vertical component; impulses (carried, targets and
+ * predictions) in units of the pair's effective mass x |g| x h. */
+int32_t vxr_box_learned(vxr_box_world* world, vxr_mlp* net, int32_t mode);
+/* The last step's gathered rows, one a contact point: features16 (rows x 16) and targets2 (rows x 2), the first
+ * `capacity` rows written; *rows receives their number. */
+int32_t vxr_box_features(vxr_box_world* world, float* features16, float* targets2, int32_t capacity, int32_t* rows);
+
 /* ---- The sphere package: XPBD spheres (core/sphere/) ------------------------------------------------------------
  * The reference's SphereSimulation (gui/SphereSimulation.java:33-295) over SphereStep and SphereStepper. A call of
  * steps is one persistent kernel: every pass of every substep, and Gauss-Seidel's run until done with the

@@ -1,0 +1,74 @@
+"""The learned warm start in a box world: the features a step gathers, a network's impulses written in place of the
+carried ones, and the whole loop (gather from the plain solver, train on the GPU, judge by sweeps to the residual,
+keep the network only if it gains)."""
+import numpy as np
+import pytest
+
+from vxr import learned as Lm
+from vxr import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def small_scene(spheres=0.8, seed=2):
+    return scenes.large_mixed(4096, seed=seed, volume=(24.0, 12.0, 24.0), sphere_share=spheres)
+
+
+def test_gpu_features_hold_what_they_describe():
+    sc = small_scene()
+    w = Lm.settled_world(sc, 200, 16)
+    w.learned(None, 1)
+    w.step_and_wait(1)
+    f, t = w.features()
+    rep = w.last()
+    assert len(f) == rep.points > 0
+    assert np.all(np.isfinite(f)) and np.all(np.isfinite(t))
+    assert np.allclose(f[:, 11:15].sum(1), 1.0), "one feature kind a point"
+    assert np.all(f[:, 9] >= 1) and np.all(f[:, 10] >= 1), "each body of a touching pair has a pair"
+    assert np.all(f[:, 3] >= 0) and np.all(f[:, 4] >= 0) and np.all(f[:, 3] + f[:, 4] > 0)
+    assert np.all(t[:, 0] >= 0) and np.all(t[:, 1] >= 0), "impulses a solve reaches are not negative"
+    assert np.all(np.abs(f[:, 15]) <= 1.0 + 1e-6)
+    w.close()
+
+
+def test_gpu_a_network_of_zeros_starts_like_a_cold_start():
+    """Boxes only (no rolling impulse is carried): starting every point from a network whose outputs are zero is
+    starting from no impulse, so the steps equal the cold start's to the bit."""
+    from vxr.learned import Mlp
+    sc = small_scene(spheres=0.0, seed=4)
+    net = Mlp(seed=0)
+    p, _, _ = net.get()
+    for k in p:
+        p[k][:] = 0.0
+    net.set(p)
+    a = Lm.settled_world(sc, 150, 16)
+    b = Lm.settled_world(sc, 150, 16)
+    a.measure(residual=False, cold_start=True, sweeps=sc["sweeps"])
+    b.learned(net, 2)
+    a.step_and_wait(3)
+    b.step_and_wait(3)
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x.view(np.int32), y.view(np.int32))
+    a.close()
+    b.close()
+    net.close()
+
+
+def test_gpu_gather_train_judge():
+    """The loop end to end on a small pile: rows gathered from the plain solver, a network trained on them by the
+    GPU's kernels (its loss falls), then judged by the plain solver: the judgement reports sweeps for all three
+    starts, and the network is kept exactly when it needs fewer sweeps than the carried impulses."""
+    from vxr.learned import Mlp
+    sc = small_scene(seed=6)
+    w = Lm.settled_world(sc, 250, 64)
+    f, t = Lm.gather(w, steps=6, rows_wanted=20000)
+    assert len(f) > 1000
+    net = Mlp(seed=1)
+    losses = net.train(f, t, epochs=5, batch=1024, lr=1e-3, seed=2)
+    assert losses[-1] < losses[0]
+    verdict = Lm.judge(w, net, steps=2)
+    for k in ("plain_warm_start", "plain_cold_start", "learned"):
+        assert 1 <= verdict[k] <= 64
+    assert verdict["kept"] == (verdict["learned"] < verdict["plain_warm_start"])
+    w.close()
+    net.close()

@@ -180,7 +180,15 @@ struct vxr_box_world {
     cudaGraphExec_t graph_exec = nullptr;
     long long graph_launches = 0;  // kernels in the captured pair of steps
     int capturing = 0;
+    // the learned warm start: 0 off, 1 gather features and targets, 2 start from the network's impulses
+    int learn_mode = 0;
+    vxr_mlp* learn_net = nullptr;
+    float *lfeat = nullptr, *lpred = nullptr, *ltarget = nullptr;  // [cap * 4 rows] x 16, 2, 2
 };
+
+// The network's forward over rows counted on the device (mlp.cu).
+int vxr_mlp_forward_device(vxr_mlp* net, const float* feats, const int* rows_dev, int rows_mult, int rows_max,
+                           float* out, cudaStream_t stream);
 
 namespace {
 
@@ -1160,6 +1168,153 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(SolveArgs A) {
     if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) A.counters->trace_len = tr.len;
 }
 
+// ------------------------------------------------------------------------------------------------------------
+// The learned warm start (no reference counterpart): 16 features a contact point at the step's start, a network's
+// starting impulses written in place of the carried ones, and after the solve the impulses it reached (the
+// training targets). A row is (round-order position x 4 + point slot); rows past a pair's point count are zero.
+// Impulses are scaled by the pair's effective mass x |g| x h, the impulse that holds that mass a substep.
+
+constexpr int FEATURES = 16;
+
+__device__ __forceinline__ float impulse_scale_of(const Params& P, const Params* scene_params, const int* body_scene,
+                                                  int a, float im_sum) {
+    float gx = P.w[P_GX], gy = P.w[P_GY], gz = P.w[P_GZ];
+    if (body_scene) {
+        const Params& S = scene_params[body_scene[a]];
+        gx = S.w[P_GX], gy = S.w[P_GY], gz = S.w[P_GZ];
+    }
+    const float g = sqrtf(gx * gx + gy * gy + gz * gz);
+    const float s = (g * P.w[P_H]) / fmaxf(im_sum, 1e-30f);
+    return s > 0.0f ? s : 1.0f;
+}
+
+// A contact point's anchors in the world's frame, and its relative velocity (second's point minus first's).
+__device__ __forceinline__ void point_of(const Held& A, const Held& B, const float* n, float4 pa, float4 pb, float* rA,
+                                         float* rB, float* rel) {
+    if (A.sphere()) {
+        for (int k = 0; k < 3; k++) rA[k] = A.half[0] * n[k];
+    } else {
+        const float anchor[3] = {pa.x, pa.y, pa.z};
+        rotate_by(A.q, A.twice, anchor, rA);
+    }
+    if (B.sphere()) {
+        for (int k = 0; k < 3; k++) rB[k] = -(B.half[0] * n[k]);
+    } else {
+        const float anchor[3] = {pb.x, pb.y, pb.z};
+        rotate_by(B.q, B.twice, anchor, rB);
+    }
+    float va[3], vb[3];
+    A.point_velocity(rA, va);
+    B.point_velocity(rB, vb);
+    for (int k = 0; k < 3; k++) rel[k] = vb[k] - va[k];
+}
+
+__global__ void k_features(const int* __restrict__ touching_n, const PairGen now, const Bodies b,
+                           const int* __restrict__ degree, Params P, const Params* __restrict__ scene_params,
+                           const int* __restrict__ body_scene, float* __restrict__ feat) {
+    const int total = *touching_n;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const int4 rec = now.pair[k];
+        const float4 nm = now.normal[k];
+        const float n[3] = {nm.x, nm.y, nm.z};
+        const int axis = (int)nm.w;
+        Held A, B;
+        A.load(b.pose[rec.x], b.turn[rec.x], b.half[rec.x], b.vel[rec.x], b.mom[rec.x], b.inv[rec.x]);
+        B.load(b.pose[rec.y], b.turn[rec.y], b.half[rec.y], b.vel[rec.y], b.mom[rec.y], b.inv[rec.y]);
+        const float s = impulse_scale_of(P, scene_params, body_scene, rec.x, A.im + B.im);
+        float ia[3], ib[3];
+        A.times_inverse_inertia(n, ia);
+        B.times_inverse_inertia(n, ib);
+        const float kind[4] = {axis < 3 ? 1.0f : 0.0f, axis >= 3 && axis < 6 ? 1.0f : 0.0f,
+                               axis >= 6 && axis < 15 ? 1.0f : 0.0f, axis >= 15 ? 1.0f : 0.0f};
+        for (int slot = 0; slot < MOST_POINTS; slot++) {
+            float* f = feat + ((size_t)k * MOST_POINTS + slot) * FEATURES;
+            if (slot >= rec.z) {
+                for (int j = 0; j < FEATURES; j++) f[j] = 0.0f;
+                continue;
+            }
+            const size_t at = (size_t)k * MOST_POINTS + slot;
+            float rA[3], rB[3], rel[3];
+            point_of(A, B, n, now.pa[at], now.pb[at], rA, rB, rel);
+            float gap = 0.0f;
+            for (int j = 0; j < 3; j++) gap += ((B.at[j] + rB[j]) - (A.at[j] + rA[j])) * n[j];
+            const float vn = rel[0] * n[0] + rel[1] * n[1] + rel[2] * n[2];
+            float vt2 = 0.0f;
+            for (int j = 0; j < 3; j++) {
+                const float t = rel[j] - vn * n[j];
+                vt2 += t * t;
+            }
+            const float4 imp = now.imp[at];
+            const float lt = sqrtf(imp.y * imp.y + imp.z * imp.z + imp.w * imp.w);
+            f[0] = gap;
+            f[1] = vn;
+            f[2] = sqrtf(vt2);
+            f[3] = A.im;
+            f[4] = B.im;
+            f[5] = n[0] * ia[0] + n[1] * ia[1] + n[2] * ia[2];
+            f[6] = n[0] * ib[0] + n[1] * ib[1] + n[2] * ib[2];
+            f[7] = imp.x / s;
+            f[8] = lt / s;
+            f[9] = (float)degree[rec.x];
+            f[10] = (float)degree[rec.y];
+            for (int j = 0; j < 4; j++) f[11 + j] = kind[j];
+            f[15] = n[1];
+        }
+    }
+}
+
+// The network's starting impulses in place of the carried ones: normal max(0, p0) s; friction max(0, p1) s along
+// the carried tangential impulse, or against the tangential slip where none is carried.
+__global__ void k_apply_learned(const int* __restrict__ touching_n, PairGen now, const Bodies b,
+                                const float* __restrict__ pred, Params P, const Params* __restrict__ scene_params,
+                                const int* __restrict__ body_scene) {
+    const int total = *touching_n;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const int4 rec = now.pair[k];
+        const float4 nm = now.normal[k];
+        const float n[3] = {nm.x, nm.y, nm.z};
+        Held A, B;
+        A.load(b.pose[rec.x], b.turn[rec.x], b.half[rec.x], b.vel[rec.x], b.mom[rec.x], b.inv[rec.x]);
+        B.load(b.pose[rec.y], b.turn[rec.y], b.half[rec.y], b.vel[rec.y], b.mom[rec.y], b.inv[rec.y]);
+        const float s = impulse_scale_of(P, scene_params, body_scene, rec.x, A.im + B.im);
+        for (int slot = 0; slot < rec.z && slot < MOST_POINTS; slot++) {
+            const size_t at = (size_t)k * MOST_POINTS + slot;
+            const float ln = fmaxf(0.0f, pred[2 * at] * s);
+            const float lt = fmaxf(0.0f, pred[2 * at + 1] * s);
+            const float4 old = now.imp[at];
+            float dir[3] = {old.y, old.z, old.w};
+            float len = sqrtf(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+            if (!(len > 1e-12f)) {
+                float rA[3], rB[3], rel[3];
+                point_of(A, B, n, now.pa[at], now.pb[at], rA, rB, rel);
+                const float vn = rel[0] * n[0] + rel[1] * n[1] + rel[2] * n[2];
+                for (int j = 0; j < 3; j++) dir[j] = -(rel[j] - vn * n[j]);
+                len = sqrtf(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+            }
+            const float c = len > 1e-12f ? lt / len : 0.0f;
+            now.imp[at] = make_float4(ln, dir[0] * c, dir[1] * c, dir[2] * c);
+        }
+    }
+}
+
+// The impulses the step's solve reached, scaled: the training targets.
+__global__ void k_targets(const int* __restrict__ touching_n, const PairGen now, const Bodies b, Params P,
+                          const Params* __restrict__ scene_params, const int* __restrict__ body_scene,
+                          float* __restrict__ target) {
+    const int total = *touching_n;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const int4 rec = now.pair[k];
+        const float s = impulse_scale_of(P, scene_params, body_scene, rec.x, b.pose[rec.x].w + b.pose[rec.y].w);
+        for (int slot = 0; slot < MOST_POINTS; slot++) {
+            const size_t at = (size_t)k * MOST_POINTS + slot;
+            float4 imp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (slot < rec.z) imp = now.imp[at];
+            target[2 * at] = imp.x / s;
+            target[2 * at + 1] = sqrtf(imp.y * imp.y + imp.z * imp.z + imp.w * imp.w) / s;
+        }
+    }
+}
+
 // Boxes.show :801-820.
 __global__ void k_show(int n, const Bodies b, float* __restrict__ shown) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1350,6 +1505,22 @@ int enqueue_step(vxr_box_world* w) {
                                             w->tcand, w->man, w->imp_t, w->impr_t, now,
                                             w->body_colours, w->b.half);
         LAUNCHED(1 + 3 + 1 + 1 + 1 + 3 + 1 + 1);  // inc count, scan, inc fill, colour, round count, scan, starts, order
+        if (w->learn_mode > 0) {
+            const int* tn = now.tstart + n;
+            k_features<<<tblocks, THREADS, 0, st>>>(tn, now, w->b, w->inc_count, w->params, w->scene_params,
+                                                    w->body_scene, w->lfeat);
+            LAUNCHED(1);
+            if (w->learn_mode == 2) {
+                if (vxr_mlp_forward_device(w->learn_net, w->lfeat, tn, MOST_POINTS, w->cap * MOST_POINTS, w->lpred,
+                                           st) != VXR_OK) {
+                    w->error = "the learned warm start's network did not launch";
+                    return VXR_ECUDA;
+                }
+                k_apply_learned<<<tblocks, THREADS, 0, st>>>(tn, now, w->b, w->lpred, w->params, w->scene_params,
+                                                             w->body_scene);
+                LAUNCHED(2);
+            }
+        }
     } else {
         if (int rc = mark(w, 1)) return rc;
         if (int rc = mark(w, 2)) return rc;
@@ -1391,6 +1562,11 @@ int enqueue_step(vxr_box_world* w) {
         if (rc) return rc;
     }
     if (int rc = mark(w, 4)) return rc;
+    if (w->has_grid && w->learn_mode == 1) {
+        k_targets<<<w->sms * 4, THREADS, 0, st>>>(now.tstart + n, now, w->b, w->params, w->scene_params,
+                                                  w->body_scene, w->ltarget);
+        LAUNCHED(1);
+    }
     k_show<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->b, w->shown);
     k_totals<<<1, 1, 0, st>>>(w->counters, w->totals);
     LAUNCHED(1 + 2);  // solve, show, totals
@@ -1827,6 +2003,55 @@ int32_t vxr_box_scenes(const vxr_box_world* w, int32_t* first_body) {
     if (first_body)
         for (int sc = 0; sc <= w->scenes && w->scenes > 0; sc++) first_body[sc] = w->scene_first[sc];
     return w->scenes;
+}
+
+int32_t vxr_box_learned(vxr_box_world* w, vxr_mlp* net, int32_t mode) {
+    if (!w || mode < 0 || mode > 2 || (mode == 2 && !net)) return VXR_EINVAL;
+    if (!w->has_grid) {
+        w->error = "the learned warm start works on a world with a grid";
+        return VXR_EINVAL;
+    }
+    if (mode > 0 && !w->lfeat) {
+        const size_t rows = (size_t)w->cap * MOST_POINTS;
+        if (alloc(w, &w->lfeat, rows * FEATURES) || alloc(w, &w->lpred, rows * 2) || alloc(w, &w->ltarget, rows * 2))
+            return VXR_ECUDA;
+    }
+    drop_graph(w);
+    w->learn_mode = mode;
+    w->learn_net = net;
+    return VXR_OK;
+}
+
+int32_t vxr_box_features(vxr_box_world* w, float* features16, float* targets2, int32_t capacity, int32_t* rows) {
+    if (!w || !rows) return VXR_EINVAL;
+    if (!w->lfeat) {
+        w->error = "no features gathered: vxr_box_learned(world, net, 1) first";
+        return VXR_EINVAL;
+    }
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    Counters c;
+    VXR_CUDA(cudaMemcpy(&c, w->counters, sizeof(Counters), cudaMemcpyDeviceToHost));
+    const int touching = std::min(c.touching, w->cap);
+    const PairGen& last = w->gen[w->cur ^ 1];  // the step just taken (the generations swapped after it)
+    std::vector<int4> pair(touching);
+    std::vector<float> f((size_t)touching * MOST_POINTS * FEATURES), t((size_t)touching * MOST_POINTS * 2);
+    if (touching) {
+        VXR_CUDA(cudaMemcpy(pair.data(), last.pair, sizeof(int4) * touching, cudaMemcpyDeviceToHost));
+        VXR_CUDA(cudaMemcpy(f.data(), w->lfeat, sizeof(float) * f.size(), cudaMemcpyDeviceToHost));
+        VXR_CUDA(cudaMemcpy(t.data(), w->ltarget, sizeof(float) * t.size(), cudaMemcpyDeviceToHost));
+    }
+    int k = 0;
+    for (int p = 0; p < touching; p++)
+        for (int slot = 0; slot < pair[p].z && slot < MOST_POINTS; slot++) {
+            const size_t row = (size_t)p * MOST_POINTS + slot;
+            if (k < capacity) {
+                if (features16) std::memcpy(features16 + (size_t)k * FEATURES, &f[row * FEATURES], sizeof(float) * FEATURES);
+                if (targets2) std::memcpy(targets2 + (size_t)k * 2, &t[row * 2], sizeof(float) * 2);
+            }
+            k++;
+        }
+    *rows = k;
+    return VXR_OK;
 }
 
 int32_t vxr_box_step_graph(vxr_box_world* w, int32_t pairs) {

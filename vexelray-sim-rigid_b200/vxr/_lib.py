@@ -23,7 +23,9 @@ SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_c
            "vxr_box_touching", "vxr_box_candidates", "vxr_box_walls", "vxr_box_colour_waves", "vxr_collide",
            "vxr_box_launches", "vxr_box_profile", "vxr_box_activity", "vxr_box_trace", "vxr_box_broadphase_static",
            "vxr_box_measure", "vxr_box_residuals", "vxr_box_create_batch", "vxr_box_scene_params",
-           "vxr_box_scenes", "vxr_box_step_graph",
+           "vxr_box_scenes", "vxr_box_step_graph", "vxr_mlp_create", "vxr_mlp_destroy", "vxr_mlp_error",
+           "vxr_mlp_set", "vxr_mlp_get", "vxr_mlp_forward", "vxr_mlp_gradients", "vxr_mlp_train", "vxr_box_learned",
+           "vxr_box_features",
            "vxr_sphere_make_params", "vxr_sphere_make_grid", "vxr_sphere_create", "vxr_sphere_destroy",
            "vxr_sphere_error", "vxr_sphere_start", "vxr_sphere_load_state", "vxr_sphere_params", "vxr_sphere_friction",
            "vxr_sphere_step", "vxr_sphere_step_async", "vxr_sphere_sync", "vxr_sphere_stream", "vxr_sphere_state",
@@ -146,6 +148,25 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_scenes.restype = i32
         L.vxr_box_step_graph.argtypes = [vp, i32]
         L.vxr_box_step_graph.restype = i32
+        L.vxr_mlp_create.argtypes = [i32, ctypes.c_uint64, ctypes.POINTER(i32)]
+        L.vxr_mlp_create.restype = vp
+        L.vxr_mlp_destroy.argtypes = [vp]
+        L.vxr_mlp_error.argtypes = [vp]
+        L.vxr_mlp_error.restype = ctypes.c_char_p
+        L.vxr_mlp_set.argtypes = [vp, vp, vp, vp]
+        L.vxr_mlp_set.restype = i32
+        L.vxr_mlp_get.argtypes = [vp, vp, vp, vp]
+        L.vxr_mlp_get.restype = i32
+        L.vxr_mlp_forward.argtypes = [vp, vp, i32, vp]
+        L.vxr_mlp_forward.restype = i32
+        L.vxr_mlp_gradients.argtypes = [vp, vp, vp, i32, vp, vp]
+        L.vxr_mlp_gradients.restype = i32
+        L.vxr_mlp_train.argtypes = [vp, vp, vp, i32, i32, i32, ctypes.c_float, ctypes.c_uint64, vp]
+        L.vxr_mlp_train.restype = i32
+        L.vxr_box_learned.argtypes = [vp, vp, i32]
+        L.vxr_box_learned.restype = i32
+        L.vxr_box_features.argtypes = [vp, vp, vp, i32, ctypes.POINTER(i32)]
+        L.vxr_box_features.restype = i32
         L.vxr_sphere_make_params.argtypes = [f64] * 8 + [i32] + [f64] * 4 + [vp]
         L.vxr_sphere_make_params.restype = i32
         L.vxr_sphere_make_grid.argtypes = [f64] * 4 + [ctypes.POINTER(Grid)]

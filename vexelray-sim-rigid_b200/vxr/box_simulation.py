@@ -129,6 +129,19 @@ class BoxSimulation:
     def step(self, steps: int = 1) -> Report:
         return self.step_and_wait(steps)
 
+    def learned(self, net, mode: int) -> None:
+        """The learned warm start: mode 0 off, 1 gather features and targets, 2 start from `net`'s impulses."""
+        self._check(self.L.vxr_box_learned(self.h, net.h if net is not None else None, mode))
+
+    def features(self):
+        """The last step's gathered rows: features (rows, 16) and targets (rows, 2)."""
+        rows = ctypes.c_int32(0)
+        self._check(self.L.vxr_box_features(self.h, None, None, 0, ctypes.byref(rows)))
+        f = np.zeros((rows.value, 16), np.float32)
+        t = np.zeros((rows.value, 2), np.float32)
+        self._check(self.L.vxr_box_features(self.h, ptr(f), ptr(t), rows.value, ctypes.byref(rows)))
+        return f, t
+
     def step_graph(self, pairs: int = 1) -> None:
         """pairs x 2 steps as replays of one captured CUDA graph of two whole steps, not waited for (sync waits)."""
         self._check(self.L.vxr_box_step_graph(self.h, pairs))
