@@ -292,7 +292,9 @@ int32_t vxr_box_features(vxr_box_world* world, float* features16, float* targets
 #define VXR_SPHERE_SHOWN_STRIDE 40      /* core/sphere/Spheres.java:1654 */
 #define VXR_SPHERE_FIELDS 24            /* core/sphere/Spheres.java:240-241 */
 #define VXR_MOST_LISTED_SPHERES 46340   /* core/sphere/Spheres.java:787 */
-#define VXR_SPHERE_ONE_BLOCK 8192       /* scenes up to this many spheres run as one block of the GPU */
+#define VXR_SPHERE_ONE_BLOCK 8192       /* scenes up to this many spheres run on one block or one cluster */
+#define VXR_SPHERE_CLUSTER_FROM 256     /* ... on a cluster from this many spheres (by default) */
+#define VXR_SPHERE_CLUSTER 8            /* ... of this many blocks */
 /* How a pass solves (SphereStep.Solve, core/sphere/SphereStep.java:37-43). */
 #define VXR_JACOBI 0
 #define VXR_GAUSS_SEIDEL_BY_CONTACT 1   /* run until every contact is solved (SphereStepper) */
@@ -311,7 +313,10 @@ typedef struct {
     int32_t contacts_per_sphere;  /* list places a sphere; 0 = 6 (SphereStep.CONTACTS_PER_SPHERE) */
     vxr_grid grid;                /* nx = 0: every pair (Jacobi only) */
     int32_t device;
-    int32_t blocks;               /* 0: one block up to VXR_SPHERE_ONE_BLOCK spheres, else enough for the list */
+    int32_t blocks;               /* 0: up to VXR_SPHERE_ONE_BLOCK spheres one block (a cluster of
+                                     VXR_SPHERE_CLUSTER from VXR_SPHERE_CLUSTER_FROM), else enough for the list */
+    int32_t cluster;              /* 2 to 16: the step runs on one thread-block cluster of this many blocks (one an
+                                     SM), its passes separated by the cluster's barrier; 0: as `blocks` says */
 } vxr_sphere_config;
 
 /* SphereStepper.Report(waits, rounds, mostRounds, unlisted) (core/sphere/SphereStepper.java:40-47) of the call's

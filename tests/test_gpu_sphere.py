@@ -108,6 +108,22 @@ def test_gpu_many_blocks_match_the_oracle(blocks):
     assert g[0] is not None
 
 
+@pytest.mark.parametrize("cluster", [4, 8, 16])
+def test_gpu_a_cluster_matches_the_oracle(cluster):
+    """The step on one thread-block cluster (the cluster's barrier between passes): the same as the oracle."""
+    def make():
+        s = C.until_done_pile()
+        s.mu_static = s.mu_kinetic = 0.5
+        s.mu_rolling = 0.05
+        s.restitution = 0.2
+        return s
+    compare_runs(make, 8, gpu_kw={"cluster": cluster})
+
+
+def test_gpu_a_cluster_runs_the_lattice_as_the_oracle_does():
+    compare_runs(lattice_scene, 90, gpu_kw={"cluster": 8})
+
+
 def test_gpu_an_overfull_list_counts_what_did_not_fit():
     """With one list place a sphere, a crowded pile leaves contacts unlisted; the GPU counts and drops the same
     ones as the oracle."""

@@ -79,6 +79,7 @@ struct Counts {
 
 struct Kernel {
     int n, cap, substeps, iterations, solve, rounds, gridded, nx, ny, nz, cells, friction, steps;
+    int cluster;  // the blocks form one thread-block cluster: passes are separated by the cluster's barrier
     float cell;
     SParams p;
     State s;
@@ -846,11 +847,20 @@ __device__ void block_scan(const int* in, int* out, int m) {
 
 __device__ __forceinline__ int read_int(const int* p) { return *(const volatile int*)p; }
 
-// The barrier between passes: the block's own when the kernel is one block, else the bounded grid barrier.
+// The cluster's hardware barrier, with release and acquire at cluster scope: every block's writes before it
+// (global memory included) are seen by every block after it.
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// The barrier between passes: the block's own when the kernel is one block, the cluster's when its blocks form
+// one cluster, else the bounded grid barrier.
 #define SYNC()                                                    \
     do {                                                          \
         if (gridDim.x == 1) {                                     \
             __syncthreads();                                      \
+        } else if (K.cluster) {                                   \
+            cluster_sync();                                       \
         } else if (!grid_sync(K.bar, epoch)) {                    \
             return;                                               \
         }                                                         \
@@ -1038,7 +1048,7 @@ struct vxr_sphere_world {
     int n = 0, substeps = 1, iterations = 1, solve = 0, rounds = 32, cap = 0;
     int gridded = 0, nx = 1, ny = 1, nz = 1, cells = 1;
     float cell = 1.0f;
-    int device = 0, sms = 148, blocks = 1, friction = 1;
+    int device = 0, sms = 148, blocks = 1, friction = 1, cluster = 0;
     cudaStream_t stream = nullptr;
     SParams params{};
     std::string error;
@@ -1165,6 +1175,7 @@ int launch_steps(vxr_sphere_world* w, int steps) {
     K.cells = w->cells;
     K.friction = w->friction;
     K.steps = steps;
+    K.cluster = w->cluster;
     K.cell = w->cell;
     K.p = w->params;
     K.s = w->s;
@@ -1194,10 +1205,24 @@ int launch_steps(vxr_sphere_world* w, int steps) {
     SPH_CUDA(cudaMemsetAsync(&w->counts->status, 0, sizeof(int) * 4, st));
     void* args[] = {&K};
     cudaError_t e;
-    if (w->blocks == 1)
+    if (w->blocks == 1) {
         e = cudaLaunchKernel((const void*)k_sphere_steps, dim3(1), dim3(THREADS), args, 0, st);
-    else
+    } else if (w->cluster) {  // every block in one cluster: co-scheduled by the hardware, the cluster barrier between
+        cudaLaunchConfig_t c = {};
+        c.gridDim = dim3(w->blocks);
+        c.blockDim = dim3(THREADS);
+        c.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = w->blocks;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        c.attrs = attr;
+        c.numAttrs = 1;
+        e = cudaLaunchKernelExC(&c, (const void*)k_sphere_steps, args);
+    } else {
         e = cudaLaunchCooperativeKernel((const void*)k_sphere_steps, dim3(w->blocks), dim3(THREADS), args, 0, st);
+    }
     if (e != cudaSuccess) return sfail(w, VXR_ECUDA, std::string("sphere step launch: ") + cudaGetErrorString(e));
     w->launches++;
     SPH_CUDA(cudaMemcpyAsync(w->host_counts, w->counts, sizeof(Counts), cudaMemcpyDeviceToHost, st));
@@ -1359,6 +1384,33 @@ vxr_sphere_world* vxr_sphere_create(const vxr_sphere_config* cfg, int32_t* statu
     const long work = std::max<long>(n, w->solve != 0 ? 3L * n : n);
     int blocks = cfg->blocks > 0 ? cfg->blocks : (n <= VXR_SPHERE_ONE_BLOCK ? 1 : (int)((work + THREADS - 1) / THREADS));
     w->blocks = std::max(1, std::min(blocks, most));
+    // By default a scene of VXR_SPHERE_CLUSTER_FROM spheres or more (that one block would run alone) runs on a
+    // cluster of VXR_SPHERE_CLUSTER blocks: measured on the 1,024-sphere lattice at rest, 5.0 ms a step against
+    // 9.4 ms on one block; 12 and 16 blocks gain nothing more.
+    int cluster = cfg->cluster;
+    if (cluster == 0 && cfg->blocks == 0 && n >= VXR_SPHERE_CLUSTER_FROM && n <= VXR_SPHERE_ONE_BLOCK)
+        cluster = VXR_SPHERE_CLUSTER;
+    if (cluster > 1) {  // one thread-block cluster of `cluster` blocks (at most 16, one a SM)
+        if (cluster > 16) return bad(VXR_EINVAL);
+        if (cluster > 8 &&
+            cudaFuncSetAttribute(k_sphere_steps, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+            return bad(VXR_EINVAL);
+        cudaLaunchConfig_t c = {};
+        c.gridDim = dim3(cluster);
+        c.blockDim = dim3(THREADS);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        c.attrs = attr;
+        c.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_sphere_steps, &c) != cudaSuccess || clusters < 1)
+            return bad(VXR_EINVAL);
+        w->blocks = cluster;
+        w->cluster = 1;
+    }
     // the stepper's batch sizing starts at BATCH a pass (SphereStepper.java:59-64)
     std::vector<int> batch(w->iterations, BATCH);
     if (cudaMemcpy(w->opening, batch.data(), sizeof(int) * w->iterations, cudaMemcpyHostToDevice) != cudaSuccess)

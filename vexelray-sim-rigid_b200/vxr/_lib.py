@@ -67,7 +67,7 @@ class BoxReport(ctypes.Structure):
 class SphereConfig(ctypes.Structure):
     _fields_ = [("spheres", ctypes.c_int32), ("substeps", ctypes.c_int32), ("iterations", ctypes.c_int32),
                 ("solve", ctypes.c_int32), ("rounds", ctypes.c_int32), ("contacts_per_sphere", ctypes.c_int32),
-                ("grid", Grid), ("device", ctypes.c_int32), ("blocks", ctypes.c_int32)]
+                ("grid", Grid), ("device", ctypes.c_int32), ("blocks", ctypes.c_int32), ("cluster", ctypes.c_int32)]
 
 
 class SphereReport(ctypes.Structure):

@@ -26,11 +26,12 @@ class SphereSimulation:
 
     def __init__(self, spheres: int, substeps: int, iterations: int, grid: S.SphereGrid | None,
                  solve: int = S.JACOBI, rounds: int = S.ROUNDS, contacts_per_sphere: int = S.CONTACTS_PER_SPHERE,
-                 device: int = 0, blocks: int = 0):
+                 device: int = 0, blocks: int = 0, cluster: int = 0):
         L = lib()
         cfg = SphereConfig()
         cfg.spheres, cfg.substeps, cfg.iterations, cfg.solve = spheres, substeps, iterations, solve
         cfg.rounds, cfg.contacts_per_sphere, cfg.device, cfg.blocks = rounds, contacts_per_sphere, device, blocks
+        cfg.cluster = cluster
         if grid is not None:
             cfg.grid = Grid(grid.nx, grid.ny, grid.nz, grid.cell)
         status = ctypes.c_int32(0)
