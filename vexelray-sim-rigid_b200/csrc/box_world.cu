@@ -859,10 +859,31 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
                 touched = true;
             }
         } else {
+            // The held corners' records, each loaded while the corner before it is solved (a corner's record is
+            // written only by its own turn, after it is read).
+            const unsigned held_bits = (unsigned)((mask >> (wall * 8)) & 0xffull);
+            int next = -1;
+            for (int j = 0; j < 8 && next < 0; j++) {
+                const int c = reverse ? 7 - j : j;
+                if ((held_bits >> c) & 1u) next = j;
+            }
+            float4 ahead = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (next >= 0) ahead = __ldcg(&A.wall[(long)s * WALL_RECORDS + wall * 8 + (reverse ? 7 - next : next)]);
             for (int k2 = 0; k2 < 8; k2++) {
                 const int c = reverse ? 7 - k2 : k2;
                 const int bit = wall * 8 + c;
                 const bool held = (mask >> bit) & 1ull;
+                float4 loaded = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (held) {
+                    loaded = ahead;
+                    next = -1;
+                    for (int j = k2 + 1; j < 8 && next < 0; j++) {
+                        const int cj = reverse ? 7 - j : j;
+                        if ((held_bits >> cj) & 1u) next = j;
+                    }
+                    if (next >= 0)
+                        ahead = __ldcg(&A.wall[(long)s * WALL_RECORDS + wall * 8 + (reverse ? 7 - next : next)]);
+                }
                 if (!held && (sweep == WARM || !((near >> wall) & 1u))) continue;
                 float offset[3], r[3];
                 for (int a = 0; a < 3; a++) {
@@ -874,7 +895,7 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
                 const float gap = high ? pick3(extent, axis) - reach : reach;
                 if (!(held || (sweep != WARM && gap < margin))) continue;
                 const long at = (long)s * WALL_RECORDS + bit;
-                float4 rec = held ? __ldcg(&A.wall[at]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                float4 rec = loaded;
                 contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft, -1.0f, track);
                 if (sweep != WARM) {
                     __stcg(&A.wall[at], rec);
@@ -1083,6 +1104,9 @@ struct Tracer {
     }
 };
 
+// Rounds of at most this many pairs (one a thread of a block) are run by one block, without grid barriers.
+constexpr int SMALL_ROUND = SOLVE_THREADS;
+
 // One sweep (BoxStep.sweep :253-267): every round of pairs, then the walls; backward, the walls first and the
 // rounds last to first.
 __device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsigned int& epoch, int kind, bool reverse,
@@ -1093,11 +1117,36 @@ __device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsign
         if (!grid_sync(A.bar, epoch)) return false;
         tr.mark(TR_WALLS | kind << 4);
     }
-    for (int order = 0; order < rounds; order++) {
+    for (int order = 0; order < rounds;) {
         const int r = reverse ? rounds - 1 - order : order;
-        phase_round(A, kind, reverse, r, fill, track);
+        if (A.round_start[r + 1] - A.round_start[r] > SMALL_ROUND) {
+            phase_round(A, kind, reverse, r, fill, track);
+            if (!grid_sync(A.bar, epoch)) return false;
+            tr.mark(TR_ROUND | kind << 4 | r << 8);
+            order++;
+            continue;
+        }
+        // A run of small rounds: block 0 alone, a block barrier between them (each round's pairs are at most one a
+        // thread), one grid barrier after the run. The other blocks wait at that barrier; the per-body order of
+        // operations is the same. Every block reads the same round sizes, so every block takes the same path.
+        int end = order;
+        while (end < rounds) {
+            const int q = reverse ? rounds - 1 - end : end;
+            if (A.round_start[q + 1] - A.round_start[q] > SMALL_ROUND) break;
+            end++;
+        }
+        if (blockIdx.x == 0) {
+            for (int o = order; o < end; o++) {
+                const int q = reverse ? rounds - 1 - o : o;
+                const int lo = A.round_start[q], hi = A.round_start[q + 1];
+                for (int k = lo + threadIdx.x; k < hi; k += blockDim.x)
+                    solve_pair(A, k, __ldg(&A.pairs.pair[k]), kind, reverse, fill, track);
+                __syncthreads();
+                tr.mark(TR_ROUND | kind << 4 | q << 8);
+            }
+        }
         if (!grid_sync(A.bar, epoch)) return false;
-        tr.mark(TR_ROUND | kind << 4 | r << 8);
+        order = end;
     }
     if (!reverse) {
         phase_walls(A, kind, false, slot, track);
