@@ -463,6 +463,95 @@ def run_batched(args):
     return 0
 
 
+TOWERS_WORKLOAD = ("box stacking: 64 towers of 64 boxes (4,096) on an 8x8 grid at 3 m, half-extents U[0.25,0.75] m, "
+                   "yaw U(+-15 deg), offset U(+-0.02) m; mu 0.6, no restitution; dt 1/60 s, 8 substeps, 16 sweeps")
+
+
+def run_towers(args):
+    """Box stacking: K timed steps; then the configuration's 1,000 steps judged by penetration and energy drift
+    (the GPU's diagnostics every 10 steps)."""
+    world_size, rank, local, pg = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from vxr import learned as Lm
+    from vxr import scenes
+    sc = scenes.towers(seed=1 + rank)
+    n = sc["bodies"]
+    w = Lm.settled_world(sc, 0, sc["sweeps"], device=local)
+    stream = torch.cuda.ExternalStream(w.stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    w.step_and_wait(args.warmup)
+    launches0 = w.launches()
+    w.profile(True)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier(pg)
+    torch.cuda.synchronize()
+    with Clocks(local) as clocks:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                starts[k].record(stream)
+            w.step_async(1)
+            with torch.cuda.stream(stream):
+                ends[k].record(stream)
+            if k % 20 == 19:
+                w.sync()
+        rep = w.sync()
+    torch.cuda.synchronize()
+    barrier(pg)
+    phases = w.profile(False)
+    activity = w.activity()
+    launches = w.launches() - launches0
+    total_ms = float(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+    slowest_ms = all_max(pg, total_ms)
+    value = all_sum(pg, float(n)) * args.steps / (slowest_ms / 1e3)
+    solve_ms = phases[3] / args.steps
+    hbm, which = peaks()
+    b_solve = algorithmic_solve_bytes(n, sc["substeps"], sc["sweeps"], activity["touching"], activity["points"],
+                                      activity["bodies_active"], activity["wall_records"])
+    achieved = b_solve / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
+    w.close()
+    # the judged run: the configuration's 1,000 steps from the start
+    j = Lm.settled_world(sc, 0, sc["sweeps"], device=local)
+    d0 = j.gpu_diagnostics()
+    e0 = d0["kinetic"] + d0["potential"]
+    worst_pen, worst_wall, energy = 0.0, 0.0, []
+    for _ in range(100):
+        j.step_and_wait(10)
+        d = j.gpu_diagnostics()
+        worst_pen = max(worst_pen, d["max_penetration"])
+        worst_wall = max(worst_wall, d["max_wall_penetration"])
+        energy.append(d["kinetic"] + d["potential"])
+    top = float(np.max(j.field("y")))
+    j.close()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": slowest_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": TOWERS_WORKLOAD, "bodies": n, "substeps": sc["substeps"], "sweeps": sc["sweeps"],
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": "replicas" if world_size > 1 else "single"},
+        "judged_1000_steps": {"max_penetration_m": worst_pen, "max_wall_penetration_m": worst_wall,
+                              "energy_start_J": e0, "energy_end_J": energy[-1],
+                              "energy_drift": (energy[-1] - e0) / abs(e0), "energy_max_rise": (max(energy) - e0) / abs(e0),
+                              "highest_box_top_m": top},
+        "phase_ms_per_step": {"broad": phases[0] / args.steps, "narrow": phases[1] / args.steps,
+                              "colour": phases[2] / args.steps, "solve": solve_ms},
+        "last_step": {"touching": rep.touching, "points": rep.points, "rounds": rep.rounds, **activity},
+        "roofline": {"bound": "hbm", "kernel": "k_solve", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "peak_source": which, "bytes_per_launch": b_solve,
+                     "ms_per_launch": solve_ms},
+        "gpu_launches": int(launches),
+    }
+    line["clocks"] = clocks.summary()
+    if pg is not None:
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def run_reference(args):
     world, rank, local, pg = dist_setup()
     if rank != 0:
@@ -516,7 +605,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-iterations", action="store_true")
     ap.add_argument("--max-pairs", type=int, default=0, help="pair capacity of the world (0: 32 a body)")
-    ap.add_argument("--workload", default="large-mixed", choices=["large-mixed", "sphere-lattice", "batched-scenes"])
+    ap.add_argument("--workload", default="large-mixed",
+                    choices=["large-mixed", "sphere-lattice", "batched-scenes", "towers"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -526,6 +616,8 @@ def main():
         return run_spheres(args)
     if args.workload == "batched-scenes":
         return run_batched(args)
+    if args.workload == "towers":
+        return run_towers(args)
 
     world_size, rank, local, pg = dist_setup()
     import torch

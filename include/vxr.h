@@ -239,6 +239,18 @@ int32_t vxr_box_scene_params(vxr_box_world* world, const int32_t* params);
  * scene's first body and the total. */
 int32_t vxr_box_scenes(const vxr_box_world* world, int32_t* first_body);
 
+/* Diagnostics computed on the GPU where the state lies: BoxDiagnostics.of (core/box/BoxDiagnostics.java:18-43:
+ * kinetic energy with the spin's 1/2 L.w, momentum, angular momentum about the origin, in doubles), the potential
+ * energy against each body's gravity, the deepest overlap at the last step's contact points (their gaps measured
+ * again from the present poses), the farthest any body reaches past a wall, the fastest body, and whether any state
+ * word is not finite. */
+typedef struct {
+    double kinetic, rotational, potential, momentum[3], angular[3];
+    double max_penetration, max_wall_penetration, max_speed;  /* metres, metres, metres a second */
+    int32_t broken, pad;
+} vxr_box_diag;
+int32_t vxr_box_diagnostics(vxr_box_world* world, vxr_box_diag* out);
+
 /* `pairs` x 2 steps as replays of one CUDA graph holding two whole steps, enqueued without waiting (vxr_box_sync
  * waits and reports). The first call captures the graph; changing the parameters, the measuring switches or the
  * state captures it again at the next call. Profiling and tracing must be off. */
@@ -385,9 +397,68 @@ int32_t vxr_sphere_contacts(vxr_sphere_world* world, int32_t* ab, int32_t* done,
 int32_t vxr_sphere_walls(vxr_sphere_world* world, float* out);
 /* contactCount: listed, missed, longest (core/sphere/Spheres.java:797-804). */
 int32_t vxr_sphere_counts(vxr_sphere_world* world, int32_t* out3);
+/* SphereDiagnostics.of (core/sphere/SphereDiagnostics.java:34-83) computed on the GPU: the deepest overlap between
+ * two spheres over the smaller radius (searched in each sphere's grid neighbourhood as the last substep sorted them,
+ * every pair without a grid), the farthest past a wall over the radius, kinetic energy with spin, the spin's part,
+ * potential energy (-gy y), momentum, angular momentum about the origin, the fastest speed, non-finite state. */
+typedef struct {
+    double kinetic, rotational, potential, momentum[3], angular[3];
+    double max_overlap, max_wall, max_speed;
+    int32_t broken, pad;
+} vxr_sphere_diag;
+int32_t vxr_sphere_diagnostics(vxr_sphere_world* world, vxr_sphere_diag* out);
+
 /* Blocks the world's kernel runs on, and kernels it has launched. */
 int32_t vxr_sphere_blocks(const vxr_sphere_world* world);
 int64_t vxr_sphere_launches(const vxr_sphere_world* world);
+
+/* ---- The picture's hand-off: a ring of finished steps ------------------------------------------------------------
+ * The reference's ShownRing (gui/ShownRing.java:37-177) with device buffers for its three slots: one the reader's
+ * front, one ready (the newest finished step it has not taken), the rest free, the next step kept in one of them. A
+ * slot's CUDA event stands for the reference's timeline value; a reader's stream waits on it (vxr_ring_wait) before it
+ * reads the slot. A new simulation installs a new generation; the old one is retired once the reader has taken from
+ * the new, and freed when the writer collects it (vxr_ring_retired). Thread-safe: one writer thread, one reader. */
+#define VXR_RING_SPHERES 0   /* VXR_SPHERE_SHOWN_STRIDE floats a body (ShownRing.Shape.SPHERES) */
+#define VXR_RING_BOXES 1     /* VXR_SHOWN_STRIDE floats a body */
+typedef struct vxr_ring vxr_ring;
+/* ShownRing.Frame (gui/ShownRing.java:88-96), with where its slot lies and the event to wait on. */
+typedef struct {
+    int64_t generation, step, finished_ns, words;
+    int32_t slot, shape, bodies, pad;
+    double extent[3];
+    const float* data;  /* device pointer of the slot */
+    void* event;        /* cudaEvent_t: the slot's contents are complete once it has fired */
+} vxr_frame;
+vxr_ring* vxr_ring_create(int32_t device);
+void vxr_ring_destroy(vxr_ring* ring);
+const char* vxr_ring_error(const vxr_ring* ring);
+/* ShownRing.install: a generation of `bodies` bodies of `shape` in a box of extent3; returns its id (from 1) or
+ * minus a status. bodies = 0: the roles alone, no buffers (for a caller that keeps its own). */
+int64_t vxr_ring_install(vxr_ring* ring, int32_t shape, int32_t bodies, const double* extent3);
+/* ShownRing.back: the slot the next step is kept in. */
+int32_t vxr_ring_back(vxr_ring* ring);
+/* ShownRing.publish: the step kept in back() is finished. */
+int32_t vxr_ring_publish(vxr_ring* ring, int64_t step, int64_t finished_ns);
+/* The writer's keep (Spheres.keep / Boxes.keep and publish): `words` floats of `shown` (a device pointer, e.g.
+ * vxr_box_shown_device) copied into the back slot on `stream`, the slot's event recorded after it, then published. */
+int32_t vxr_ring_keep(vxr_ring* ring, const float* shown, int64_t words, void* stream, int64_t step);
+/* ShownRing.take: the newest finished step as the front (or the front as it was); returns 1 before any step has been
+ * published, VXR_OK otherwise. */
+int32_t vxr_ring_take(vxr_ring* ring, vxr_frame* out);
+/* The reader's stream waits for the frame's slot to be complete. */
+int32_t vxr_ring_wait(const vxr_frame* frame, void* stream);
+/* The frame's slot copied to host memory once it is complete (frame->words floats): the picture handed to a reader
+ * on another device, as ShownSlots.on reads it (gui/ShownSlots.java:35-156). */
+int32_t vxr_ring_read(const vxr_frame* frame, float* out);
+/* ShownRing.retired: generations the reader has moved past, each once; their slots are freed here. Returns how many,
+ * their ids in ids (capacity entries at most). */
+int32_t vxr_ring_retired(vxr_ring* ring, int64_t* ids, int32_t capacity);
+/* The generations still live (not freed), the current one included. */
+int32_t vxr_ring_live(vxr_ring* ring, int64_t* ids, int32_t capacity);
+/* The world's resident `shown` (RigidSimulation.shown, gui/RigidSimulation.java:33-37): its device address, and its
+ * length in floats into *words. */
+const float* vxr_box_shown_device(vxr_box_world* world, int64_t* words);
+const float* vxr_sphere_shown_device(vxr_sphere_world* world, int64_t* words);
 
 #ifdef __cplusplus
 }

@@ -1364,6 +1364,106 @@ __global__ void k_targets(const int* __restrict__ touching_n, const PairGen now,
     }
 }
 
+// ------------------------------------------------------------------------------------------------------------
+// Diagnostics on the device (BoxDiagnostics.of, core/box/BoxDiagnostics.java:18-43, and the penetrations and
+// potential energy a long run is judged by): reductions over the state where it lies, sums in doubles.
+
+struct Diag {
+    double kinetic, rotational, potential, momentum[3], angular[3];
+    unsigned max_penetration, max_wall, max_speed;  // non-negative floats as bits
+    int broken;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void k_diag_bodies(int n, const Bodies b, Params P, const Params* __restrict__ scene_params,
+                              const int* __restrict__ body_scene, Diag* d) {
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // kinetic, rotational, potential, momentum 3, angular 3
+    float wall = 0.0f, speed = 0.0f;
+    int broken = 0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        Held h;
+        h.load(b.pose[s], b.turn[s], b.half[s], b.vel[s], b.mom[s], b.inv[s]);
+        for (int k = 0; k < 3; k++)
+            if (!isfinite(h.at[k]) || !isfinite(h.velocity[k]) || !isfinite(h.momentum[k]) || !isfinite(h.q[k]))
+                broken = 1;
+        const float v2 = h.velocity[0] * h.velocity[0] + h.velocity[1] * h.velocity[1] + h.velocity[2] * h.velocity[2];
+        speed = fmaxf(speed, sqrtf(v2));
+        float ext[3] = {P.w[P_SX], P.w[P_SY], P.w[P_SZ]}, g[3] = {P.w[P_GX], P.w[P_GY], P.w[P_GZ]};
+        if (body_scene) {
+            const Params& S = scene_params[body_scene[s]];
+            for (int k = 0; k < 3; k++) ext[k] = S.w[P_SX + k], g[k] = S.w[P_GX + k];
+        }
+        // how far past a wall the body reaches: a sphere's surface, a box's corners
+        if (h.sphere()) {
+            for (int k = 0; k < 3; k++) wall = fmaxf(wall, fmaxf(h.half[0] - h.at[k], (h.at[k] + h.half[0]) - ext[k]));
+        } else {
+            for (int c = 0; c < 8; c++) {
+                float off[3], r[3];
+                for (int k = 0; k < 3; k++) off[k] = ((c >> k) & 1) ? h.half[k] : -h.half[k];
+                rotate_by(h.q, h.twice, off, r);
+                for (int k = 0; k < 3; k++) {
+                    const float p = h.at[k] + r[k];
+                    wall = fmaxf(wall, fmaxf(-p, p - ext[k]));
+                }
+            }
+        }
+        if (!(h.im > 0.0f)) continue;
+        const double m = 1.0 / (double)h.im;
+        double lw = 0.0;
+        for (int k = 0; k < 3; k++) lw += (double)h.momentum[k] * (double)h.omega[k];
+        const double vv = (double)h.velocity[0] * h.velocity[0] + (double)h.velocity[1] * h.velocity[1] +
+                          (double)h.velocity[2] * h.velocity[2];
+        acc[0] += 0.5 * m * vv + 0.5 * lw;
+        acc[1] += 0.5 * lw;
+        acc[2] += -m * ((double)g[0] * h.at[0] + (double)g[1] * h.at[1] + (double)g[2] * h.at[2]);
+        for (int k = 0; k < 3; k++) acc[3 + k] += m * h.velocity[k];
+        const double x = h.at[0], y = h.at[1], z = h.at[2], u = h.velocity[0], v = h.velocity[1], w = h.velocity[2];
+        acc[6] += m * (y * w - z * v) + h.momentum[0];
+        acc[7] += m * (z * u - x * w) + h.momentum[1];
+        acc[8] += m * (x * v - y * u) + h.momentum[2];
+    }
+    for (int k = 0; k < 9; k++) acc[k] = warp_sum(acc[k]);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&d->kinetic, acc[0]);
+        atomicAdd(&d->rotational, acc[1]);
+        atomicAdd(&d->potential, acc[2]);
+        for (int k = 0; k < 3; k++) {
+            atomicAdd(&d->momentum[k], acc[3 + k]);
+            atomicAdd(&d->angular[k], acc[6 + k]);
+        }
+    }
+    atomicMax(&d->max_wall, __float_as_uint(fmaxf(wall, 0.0f)));
+    atomicMax(&d->max_speed, __float_as_uint(speed));
+    if (broken) atomicExch(&d->broken, 1);
+}
+
+// The deepest overlap at the last step's contact points, their gaps measured again from where the bodies are now.
+__global__ void k_diag_contacts(const int* __restrict__ touching_n, const PairGen last, const Bodies b, Diag* d) {
+    const int total = *touching_n;
+    float deepest = 0.0f;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const int4 rec = last.pair[k];
+        const float4 nm = last.normal[k];
+        const float n[3] = {nm.x, nm.y, nm.z};
+        Held A, B;
+        A.load(b.pose[rec.x], b.turn[rec.x], b.half[rec.x], b.vel[rec.x], b.mom[rec.x], b.inv[rec.x]);
+        B.load(b.pose[rec.y], b.turn[rec.y], b.half[rec.y], b.vel[rec.y], b.mom[rec.y], b.inv[rec.y]);
+        for (int slot = 0; slot < rec.z && slot < MOST_POINTS; slot++) {
+            const size_t at = (size_t)k * MOST_POINTS + slot;
+            float rA[3], rB[3], rel[3];
+            point_of(A, B, n, last.pa[at], last.pb[at], rA, rB, rel);
+            float gap = 0.0f;
+            for (int j = 0; j < 3; j++) gap += ((B.at[j] + rB[j]) - (A.at[j] + rA[j])) * n[j];
+            deepest = fmaxf(deepest, -gap);
+        }
+    }
+    atomicMax(&d->max_penetration, __float_as_uint(fmaxf(deepest, 0.0f)));
+}
+
 // Boxes.show :801-820.
 __global__ void k_show(int n, const Bodies b, float* __restrict__ shown) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2101,6 +2201,47 @@ int32_t vxr_box_features(vxr_box_world* w, float* features16, float* targets2, i
         }
     *rows = k;
     return VXR_OK;
+}
+
+int32_t vxr_box_diagnostics(vxr_box_world* w, vxr_box_diag* out) {
+    if (!w || !out) return VXR_EINVAL;
+    cudaSetDevice(w->device);
+    Diag* d = nullptr;
+    VXR_CUDA(cudaMallocAsync(&d, sizeof(Diag), w->stream));
+    VXR_CUDA(cudaMemsetAsync(d, 0, sizeof(Diag), w->stream));
+    k_diag_bodies<<<w->sms * 4, THREADS, 0, w->stream>>>(w->n, w->b, w->params, w->scene_params, w->body_scene, d);
+    if (w->has_grid) {
+        const PairGen& last = w->gen[w->cur ^ 1];
+        k_diag_contacts<<<w->sms * 4, THREADS, 0, w->stream>>>(last.tstart + w->n, last, w->b, d);
+    }
+    VXR_CUDA(cudaGetLastError());
+    Diag h;
+    VXR_CUDA(cudaMemcpyAsync(&h, d, sizeof(Diag), cudaMemcpyDeviceToHost, w->stream));
+    VXR_CUDA(cudaFreeAsync(d, w->stream));
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    out->kinetic = h.kinetic;
+    out->rotational = h.rotational;
+    out->potential = h.potential;
+    for (int k = 0; k < 3; k++) {
+        out->momentum[k] = h.momentum[k];
+        out->angular[k] = h.angular[k];
+    }
+    float f;
+    std::memcpy(&f, &h.max_penetration, 4);
+    out->max_penetration = f;
+    std::memcpy(&f, &h.max_wall, 4);
+    out->max_wall_penetration = f;
+    std::memcpy(&f, &h.max_speed, 4);
+    out->max_speed = f;
+    out->broken = h.broken;
+    out->pad = 0;
+    return VXR_OK;
+}
+
+const float* vxr_box_shown_device(vxr_box_world* w, int64_t* words) {
+    if (!w) return nullptr;
+    if (words) *words = (int64_t)w->n * SHOWN_STRIDE;
+    return w->shown;
 }
 
 int32_t vxr_box_step_graph(vxr_box_world* w, int32_t pairs) {

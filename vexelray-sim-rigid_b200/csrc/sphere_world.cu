@@ -1038,6 +1038,70 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
     if (gtid == 0) K.counts->cur = cur;
 }
 
+// SphereDiagnostics.of (core/sphere/SphereDiagnostics.java:34-83) on the device: each sphere's deepest overlap with
+// the spheres of its neighbourhood (the grid's 27 cells as the last substep sorted them; every sphere without a grid),
+// over the smaller radius; how far it reaches past a wall, over its radius; energies, momenta and the fastest speed,
+// summed in doubles.
+struct SDiag {
+    double kinetic, rotational, potential, momentum[3], angular[3];
+    unsigned max_overlap, max_wall, max_speed;
+    int broken;
+};
+
+__global__ void k_sphere_diag(Kernel K, SDiag* d) {
+    const State& S = K.s;
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    float overlap = 0.0f, wall = 0.0f, speed = 0.0f;
+    int broken = 0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < K.n; s += gridDim.x * blockDim.x) {
+        const float4 p = S.pos[s], v = S.vel[s], w = S.spin[s];
+        const float im = S.disp[s].w, r = p.w;
+        const float f[9] = {p.x, p.y, p.z, v.x, v.y, v.z, w.x, w.y, w.z};
+        for (int k = 0; k < 9; k++)
+            if (!isfinite(f[k])) broken = 1;
+        around(K, s, [&](int o) {
+            if (!(o > s)) return;
+            const float4 q = S.pos[o];
+            const double dx = (double)p.x - q.x, dy = (double)p.y - q.y, dz = (double)p.z - q.z;
+            const double depth = (double)(r + q.w) - sqrt(dx * dx + dy * dy + dz * dz);
+            overlap = fmaxf(overlap, (float)(depth / fmin((double)r, (double)q.w)));
+        });
+        const float at[3] = {p.x, p.y, p.z};
+        for (int a = 0; a < 3; a++)
+            wall = fmaxf(wall, fmaxf((r - at[a]) / r, ((at[a] + r) - K.p.w[SX + a]) / r));
+        const double vv = (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
+        speed = fmaxf(speed, (float)sqrt(vv));
+        if (!(im > 0.0f)) continue;
+        const double m = 1.0 / (double)im;
+        const double inertia = 0.4 * m * r * r;
+        const double spin2 = (double)w.x * w.x + (double)w.y * w.y + (double)w.z * w.z;
+        acc[0] += 0.5 * m * vv + 0.5 * inertia * spin2;
+        acc[1] += 0.5 * inertia * spin2;
+        acc[2] += m * -(double)K.p.w[GY] * p.y;
+        acc[3] += m * v.x;
+        acc[4] += m * v.y;
+        acc[5] += m * v.z;
+        acc[6] += m * ((double)p.y * v.z - (double)p.z * v.y) + inertia * w.x;
+        acc[7] += m * ((double)p.z * v.x - (double)p.x * v.z) + inertia * w.y;
+        acc[8] += m * ((double)p.x * v.y - (double)p.y * v.x) + inertia * w.z;
+    }
+    for (int k = 0; k < 9; k++)
+        for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&d->kinetic, acc[0]);
+        atomicAdd(&d->rotational, acc[1]);
+        atomicAdd(&d->potential, acc[2]);
+        for (int k = 0; k < 3; k++) {
+            atomicAdd(&d->momentum[k], acc[3 + k]);
+            atomicAdd(&d->angular[k], acc[6 + k]);
+        }
+    }
+    atomicMax(&d->max_overlap, __float_as_uint(fmaxf(overlap, 0.0f)));
+    atomicMax(&d->max_wall, __float_as_uint(fmaxf(wall, 0.0f)));
+    atomicMax(&d->max_speed, __float_as_uint(speed));
+    if (broken) atomicExch(&d->broken, 1);
+}
+
 }  // namespace sph
 }  // namespace vxr
 
@@ -1160,7 +1224,7 @@ int write_state(vxr_sphere_world* w, const float* const* fields24, const float* 
     return VXR_OK;
 }
 
-int launch_steps(vxr_sphere_world* w, int steps) {
+Kernel kernel_of(vxr_sphere_world* w, int steps) {
     Kernel K;
     K.n = w->n;
     K.cap = w->cap;
@@ -1198,6 +1262,11 @@ int launch_steps(vxr_sphere_world* w, int steps) {
     K.bar.abort = &w->counts->abort;
     K.bar.status = &w->counts->status;
     K.bar.limit_ns = 2000000000ull;  // 2 s: far above any barrier's honest wait
+    return K;
+}
+
+int launch_steps(vxr_sphere_world* w, int steps) {
+    Kernel K = kernel_of(w, steps);
     cudaStream_t st = w->stream;
     // the barrier's counter, the status and the call's totals start at zero; the list, its counts and the
     // generation carry over
@@ -1589,6 +1658,48 @@ int32_t vxr_sphere_counts(vxr_sphere_world* w, int32_t* out3) {
 }
 
 int32_t vxr_sphere_blocks(const vxr_sphere_world* w) { return w ? w->blocks : 0; }
+
+const float* vxr_sphere_shown_device(vxr_sphere_world* w, int64_t* words) {
+    if (!w) return nullptr;
+    if (w->pending) finish(w, nullptr);
+    if (words) *words = (int64_t)w->n * SHOWN;
+    return w->shown;
+}
+
+int32_t vxr_sphere_diagnostics(vxr_sphere_world* w, vxr_sphere_diag* out) {
+    if (!w || !out) return sfail(w, VXR_EINVAL, "null argument");
+    if (w->pending) {
+        const int rc = finish(w, nullptr);
+        if (rc != VXR_OK) return rc;
+    }
+    const Kernel K = kernel_of(w, 0);
+    SDiag* d = nullptr;
+    SPH_CUDA(cudaMallocAsync(&d, sizeof(SDiag), w->stream));
+    SPH_CUDA(cudaMemsetAsync(d, 0, sizeof(SDiag), w->stream));
+    k_sphere_diag<<<std::max(1, std::min((w->n + 255) / 256, 4 * w->sms)), 256, 0, w->stream>>>(K, d);
+    SPH_CUDA(cudaGetLastError());
+    SDiag h;
+    SPH_CUDA(cudaMemcpyAsync(&h, d, sizeof(SDiag), cudaMemcpyDeviceToHost, w->stream));
+    SPH_CUDA(cudaFreeAsync(d, w->stream));
+    SPH_CUDA(cudaStreamSynchronize(w->stream));
+    out->kinetic = h.kinetic;
+    out->rotational = h.rotational;
+    out->potential = h.potential;
+    for (int k = 0; k < 3; k++) {
+        out->momentum[k] = h.momentum[k];
+        out->angular[k] = h.angular[k];
+    }
+    float f;
+    std::memcpy(&f, &h.max_overlap, 4);
+    out->max_overlap = f;
+    std::memcpy(&f, &h.max_wall, 4);
+    out->max_wall = f;
+    std::memcpy(&f, &h.max_speed, 4);
+    out->max_speed = f;
+    out->broken = h.broken;
+    out->pad = 0;
+    return VXR_OK;
+}
 
 int64_t vxr_sphere_launches(const vxr_sphere_world* w) { return w ? w->launches : 0; }
 

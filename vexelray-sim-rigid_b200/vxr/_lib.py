@@ -25,7 +25,10 @@ SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_c
            "vxr_box_measure", "vxr_box_residuals", "vxr_box_create_batch", "vxr_box_scene_params",
            "vxr_box_scenes", "vxr_box_step_graph", "vxr_mlp_create", "vxr_mlp_destroy", "vxr_mlp_error",
            "vxr_mlp_set", "vxr_mlp_get", "vxr_mlp_forward", "vxr_mlp_gradients", "vxr_mlp_train", "vxr_box_learned",
-           "vxr_box_features",
+           "vxr_box_features", "vxr_box_diagnostics", "vxr_sphere_diagnostics", "vxr_ring_create", "vxr_ring_destroy",
+           "vxr_ring_error", "vxr_ring_install", "vxr_ring_back", "vxr_ring_publish", "vxr_ring_keep", "vxr_ring_take",
+           "vxr_ring_wait", "vxr_ring_read", "vxr_ring_retired", "vxr_ring_live", "vxr_box_shown_device",
+           "vxr_sphere_shown_device",
            "vxr_sphere_make_params", "vxr_sphere_make_grid", "vxr_sphere_create", "vxr_sphere_destroy",
            "vxr_sphere_error", "vxr_sphere_start", "vxr_sphere_load_state", "vxr_sphere_params", "vxr_sphere_friction",
            "vxr_sphere_step", "vxr_sphere_step_async", "vxr_sphere_sync", "vxr_sphere_stream", "vxr_sphere_state",
@@ -62,6 +65,21 @@ class BoxReport(ctypes.Structure):
                 ("unplaced", ctypes.c_int32), ("unlisted", ctypes.c_int32), ("most_rounds", ctypes.c_int32),
                 ("unplaced_total", ctypes.c_int64), ("unlisted_total", ctypes.c_int64), ("status", ctypes.c_int32),
                 ("steps", ctypes.c_int32)]
+
+
+class Diag(ctypes.Structure):
+    """vxr_box_diag and vxr_sphere_diag: the same layout (the overlap words are named for the box's)."""
+    _fields_ = [("kinetic", ctypes.c_double), ("rotational", ctypes.c_double), ("potential", ctypes.c_double),
+                ("momentum", ctypes.c_double * 3), ("angular", ctypes.c_double * 3),
+                ("max_penetration", ctypes.c_double), ("max_wall", ctypes.c_double), ("max_speed", ctypes.c_double),
+                ("broken", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+class Frame(ctypes.Structure):
+    _fields_ = [("generation", ctypes.c_int64), ("step", ctypes.c_int64), ("finished_ns", ctypes.c_int64),
+                ("words", ctypes.c_int64), ("slot", ctypes.c_int32), ("shape", ctypes.c_int32),
+                ("bodies", ctypes.c_int32), ("pad", ctypes.c_int32), ("extent", ctypes.c_double * 3),
+                ("data", ctypes.c_void_p), ("event", ctypes.c_void_p)]
 
 
 class SphereConfig(ctypes.Structure):
@@ -167,6 +185,37 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_learned.restype = i32
         L.vxr_box_features.argtypes = [vp, vp, vp, i32, ctypes.POINTER(i32)]
         L.vxr_box_features.restype = i32
+        L.vxr_box_diagnostics.argtypes = [vp, ctypes.POINTER(Diag)]
+        L.vxr_box_diagnostics.restype = i32
+        L.vxr_sphere_diagnostics.argtypes = [vp, ctypes.POINTER(Diag)]
+        L.vxr_sphere_diagnostics.restype = i32
+        L.vxr_ring_create.argtypes = [i32]
+        L.vxr_ring_create.restype = vp
+        L.vxr_ring_destroy.argtypes = [vp]
+        L.vxr_ring_error.argtypes = [vp]
+        L.vxr_ring_error.restype = ctypes.c_char_p
+        L.vxr_ring_install.argtypes = [vp, i32, i32, vp]
+        L.vxr_ring_install.restype = ctypes.c_int64
+        L.vxr_ring_back.argtypes = [vp]
+        L.vxr_ring_back.restype = i32
+        L.vxr_ring_publish.argtypes = [vp, ctypes.c_int64, ctypes.c_int64]
+        L.vxr_ring_publish.restype = i32
+        L.vxr_ring_keep.argtypes = [vp, vp, ctypes.c_int64, vp, ctypes.c_int64]
+        L.vxr_ring_keep.restype = i32
+        L.vxr_ring_take.argtypes = [vp, ctypes.POINTER(Frame)]
+        L.vxr_ring_take.restype = i32
+        L.vxr_ring_wait.argtypes = [ctypes.POINTER(Frame), vp]
+        L.vxr_ring_wait.restype = i32
+        L.vxr_ring_read.argtypes = [ctypes.POINTER(Frame), vp]
+        L.vxr_ring_read.restype = i32
+        L.vxr_ring_retired.argtypes = [vp, vp, i32]
+        L.vxr_ring_retired.restype = i32
+        L.vxr_ring_live.argtypes = [vp, vp, i32]
+        L.vxr_ring_live.restype = i32
+        L.vxr_box_shown_device.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.vxr_box_shown_device.restype = vp
+        L.vxr_sphere_shown_device.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.vxr_sphere_shown_device.restype = vp
         L.vxr_sphere_make_params.argtypes = [f64] * 8 + [i32] + [f64] * 4 + [vp]
         L.vxr_sphere_make_params.restype = i32
         L.vxr_sphere_make_grid.argtypes = [f64] * 4 + [ctypes.POINTER(Grid)]

@@ -13,7 +13,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import boxes as B
-from ._lib import BatchConfig, BoxConfig, BoxReport, Grid, VxrError, lib, ptr, ptr_array
+from ._lib import BatchConfig, BoxConfig, BoxReport, Diag, Grid, VxrError, lib, ptr, ptr_array
 
 STATE_FIELDS = ["x", "y", "z", "u", "v", "w", "lx", "ly", "lz", "qx", "qy", "qz", "qw"]
 ALL_FIELDS = STATE_FIELDS + ["im", "hx", "hy", "hz", "shape"]
@@ -128,6 +128,15 @@ class BoxSimulation:
 
     def step(self, steps: int = 1) -> Report:
         return self.step_and_wait(steps)
+
+    def gpu_diagnostics(self) -> dict:
+        """Diagnostics computed on the GPU (vxr_box_diagnostics): energies, momenta, the deepest contact and wall
+        penetration, the fastest speed, non-finite state."""
+        d = Diag()
+        self._check(self.L.vxr_box_diagnostics(self.h, ctypes.byref(d)))
+        return {"kinetic": d.kinetic, "rotational": d.rotational, "potential": d.potential,
+                "momentum": tuple(d.momentum), "angular": tuple(d.angular), "max_penetration": d.max_penetration,
+                "max_wall_penetration": d.max_wall, "max_speed": d.max_speed, "broken": bool(d.broken)}
 
     def learned(self, net, mode: int) -> None:
         """The learned warm start: mode 0 off, 1 gather features and targets, 2 start from `net`'s impulses."""

@@ -16,7 +16,7 @@ from collections import namedtuple
 import numpy as np
 
 from . import spheres as S
-from ._lib import Grid, SphereConfig, SphereReport, VxrError, lib, ptr, ptr_array
+from ._lib import Diag, Grid, SphereConfig, SphereReport, VxrError, lib, ptr, ptr_array
 
 Report = namedtuple("Report", "waits rounds most_rounds unlisted")
 
@@ -111,6 +111,13 @@ class SphereSimulation:
 
     def stream(self) -> int:
         return lib().vxr_sphere_stream(self._h)
+
+    def gpu_diagnostics(self) -> S.Diagnostics:
+        """SphereDiagnostics computed on the GPU (vxr_sphere_diagnostics)."""
+        d = Diag()
+        self._check(lib().vxr_sphere_diagnostics(self._h, ctypes.byref(d)))
+        return S.Diagnostics(d.max_penetration, d.max_wall, d.kinetic, d.rotational, d.potential, tuple(d.momentum),
+                             tuple(d.angular), d.max_speed, bool(d.broken))
 
     def blocks(self) -> int:
         return lib().vxr_sphere_blocks(self._h)
