@@ -460,6 +460,26 @@ int32_t vxr_ring_live(vxr_ring* ring, int64_t* ids, int32_t capacity);
 const float* vxr_box_shown_device(vxr_box_world* world, int64_t* words);
 const float* vxr_sphere_shown_device(vxr_sphere_world* world, int64_t* words);
 
+/* ---- The picture: one ray a pixel against every body, into a headless RGB buffer -----------------------------------
+ * The reference's fragment shaders as CUDA: Picture.java (camera ray, sky, checkered floor, light), SphereShader.java
+ * (squashed spheres painted in octants) and BoxShader.java (slab test, edge band, sphere-shaped bodies). The push
+ * constants of Picture.push (gui/Picture.java:202-216), as f32: */
+typedef struct {
+    float eye[3], right[3], up[3], forward[3]; /* right, up, forward unit length */
+    float aspect;  /* width / height */
+    float alpha;   /* how far between the last two steps to show the bodies, 0 to 1 */
+    float extent[3];
+    float squash;  /* spheres only: 0 not squashed, 1.5 overlaps just closed */
+} vxr_camera;
+/* `count` bodies of `shape` (VXR_RING_SPHERES / VXR_RING_BOXES) from `shown` (a device pointer, e.g. a ring
+ * frame's data or vxr_*_shown_device) drawn into rgb (device, width * height * 3 floats, row 0 the top) on `stream`.
+ * Pixel (i, j) is the one at uv ((i + 0.5) / width, (j + 0.5) / height). */
+int32_t vxr_picture(int32_t shape, const float* shown, int32_t count, const vxr_camera* camera, int32_t width,
+                    int32_t height, float* rgb, void* stream);
+/* The same from and into host memory (a picture for a file or a reader without a device). */
+int32_t vxr_picture_host(int32_t shape, const float* shown_host, int32_t count, const vxr_camera* camera,
+                         int32_t width, int32_t height, float* rgb_host);
+
 #ifdef __cplusplus
 }
 #endif

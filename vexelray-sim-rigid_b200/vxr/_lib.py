@@ -28,7 +28,7 @@ SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_c
            "vxr_box_features", "vxr_box_diagnostics", "vxr_sphere_diagnostics", "vxr_ring_create", "vxr_ring_destroy",
            "vxr_ring_error", "vxr_ring_install", "vxr_ring_back", "vxr_ring_publish", "vxr_ring_keep", "vxr_ring_take",
            "vxr_ring_wait", "vxr_ring_read", "vxr_ring_retired", "vxr_ring_live", "vxr_box_shown_device",
-           "vxr_sphere_shown_device",
+           "vxr_sphere_shown_device", "vxr_picture", "vxr_picture_host",
            "vxr_sphere_make_params", "vxr_sphere_make_grid", "vxr_sphere_create", "vxr_sphere_destroy",
            "vxr_sphere_error", "vxr_sphere_start", "vxr_sphere_load_state", "vxr_sphere_params", "vxr_sphere_friction",
            "vxr_sphere_step", "vxr_sphere_step_async", "vxr_sphere_sync", "vxr_sphere_stream", "vxr_sphere_state",
@@ -80,6 +80,13 @@ class Frame(ctypes.Structure):
                 ("words", ctypes.c_int64), ("slot", ctypes.c_int32), ("shape", ctypes.c_int32),
                 ("bodies", ctypes.c_int32), ("pad", ctypes.c_int32), ("extent", ctypes.c_double * 3),
                 ("data", ctypes.c_void_p), ("event", ctypes.c_void_p)]
+
+
+class Camera(ctypes.Structure):
+    """vxr_camera: Picture.push's words (gui/Picture.java:202-216) as a struct."""
+    _fields_ = [("eye", ctypes.c_float * 3), ("right", ctypes.c_float * 3), ("up", ctypes.c_float * 3),
+                ("forward", ctypes.c_float * 3), ("aspect", ctypes.c_float), ("alpha", ctypes.c_float),
+                ("extent", ctypes.c_float * 3), ("squash", ctypes.c_float)]
 
 
 class SphereConfig(ctypes.Structure):
@@ -216,6 +223,10 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_shown_device.restype = vp
         L.vxr_sphere_shown_device.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
         L.vxr_sphere_shown_device.restype = vp
+        L.vxr_picture.argtypes = [i32, vp, i32, ctypes.POINTER(Camera), i32, i32, vp, vp]
+        L.vxr_picture.restype = i32
+        L.vxr_picture_host.argtypes = [i32, vp, i32, ctypes.POINTER(Camera), i32, i32, vp]
+        L.vxr_picture_host.restype = i32
         L.vxr_sphere_make_params.argtypes = [f64] * 8 + [i32] + [f64] * 4 + [vp]
         L.vxr_sphere_make_params.restype = i32
         L.vxr_sphere_make_grid.argtypes = [f64] * 4 + [ctypes.POINTER(Grid)]
