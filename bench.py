@@ -139,11 +139,11 @@ def barrier(pg):
 ITERATION_CAP = 64
 
 
-def make_world(scene, device, max_pairs=0):
+def make_world(scene, device, max_pairs=0, schedule=0, solve_blocks_per_sm=0):
     from vxr.box_simulation import BoxSimulation
     # room for the iteration count measurement's sweeps; the steps run the scene's own
     w = BoxSimulation(scene["bodies"], scene["substeps"], max(scene["sweeps"], ITERATION_CAP), False, scene["grid"],
-                      device=device, max_pairs=max_pairs)
+                      device=device, max_pairs=max_pairs, schedule=schedule, solve_blocks_per_sm=solve_blocks_per_sm)
     w.measure(residual=False, sweeps=scene["sweeps"])
     l = [scene["lx"], scene["ly"], scene["lz"]]
     q = [scene["qx"], scene["qy"], scene["qz"], scene["qw"]]
@@ -253,7 +253,7 @@ def picture_timing(world, shape, n, extent, device, squash=1.5, side=1024, draws
     if cpu:
         from oracle import picture as OP
         shown = world.read_shown()
-        band = max(1, side // 64)
+        band = max(1, min(side // 64, int(2e8 // (side * max(n, 1)))))  # about 2e8 bounding tests
         t0 = time.perf_counter()
         OP.picture(shape, shown, P.push_words(cam, n), side, side, rows=range(side // 2, side // 2 + band))
         dt = time.perf_counter() - t0
@@ -585,6 +585,7 @@ def run_towers(args):
     b_solve = algorithmic_solve_bytes(n, sc["substeps"], sc["sweeps"], activity["touching"], activity["points"],
                                       activity["bodies_active"], activity["wall_records"])
     achieved = b_solve / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
+    pic = picture_timing(w, 1, n, sc["walls"], local, squash=0.0, cpu=rank == 0 and not args.no_cpu)
     w.close()
     judged = judged_run(sc, 1000, 10, local)
     line = {
@@ -595,6 +596,7 @@ def run_towers(args):
                    "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": "replicas" if world_size > 1 else "single"},
         "judged_1000_steps": judged,
+        "picture": pic,
         "phase_ms_per_step": {"broad": phases[0] / args.steps, "narrow": phases[1] / args.steps,
                               "colour": phases[2] / args.steps, "solve": solve_ms},
         "last_step": {"touching": rep.touching, "points": rep.points, "rounds": rep.rounds, **activity},
@@ -664,6 +666,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-iterations", action="store_true")
     ap.add_argument("--no-judge", action="store_true", help="skip the judged run (penetration, energy)")
+    ap.add_argument("--schedule", type=int, default=0, help="solve schedule: 0 barrier phases, 1 per-body dependencies")
+    ap.add_argument("--solve-blocks-per-sm", type=int, default=0, help="solve blocks an SM (0: the library's choice)")
     ap.add_argument("--max-pairs", type=int, default=0, help="pair capacity of the world (0: 32 a body)")
     ap.add_argument("--workload", default="large-mixed",
                     choices=["large-mixed", "sphere-lattice", "batched-scenes", "towers"])
@@ -688,7 +692,7 @@ def main():
         scene = scenes.large_mixed(args.bodies, seed=1 + rank)
     else:  # a smaller case of the same scene: the same body density over a smaller footprint
         scene = scenes.sub_volume(BODIES, args.bodies / BODIES, seed=1 + rank)
-    w = make_world(scene, local, args.max_pairs)
+    w = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm)
     stream = torch.cuda.ExternalStream(w.stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
@@ -770,7 +774,7 @@ def main():
 
     e2e = None
     if not args.no_e2e:
-        w2 = make_world(scene, local, args.max_pairs)
+        w2 = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm)
         for _ in range(args.warmup):
             w2.step_and_wait(1)
             w2.state()
@@ -797,6 +801,7 @@ def main():
                    "grid": [scene["grid"].nx, scene["grid"].ny, scene["grid"].nz, scene["grid"].cell],
                    "timed_steps": f"{args.warmup}..{args.warmup + args.steps - 1} of the drop",
                    "l2": "flushed (256 MiB write) before every timed step",
+                   "schedule": args.schedule, "solve_blocks_per_sm": args.solve_blocks_per_sm,
                    "parallelism": "replicas" if world_size > 1 else "single"},
         "phase_ms_per_step": {"broad": phases[0] / args.steps, "narrow": phases[1] / args.steps,
                               "colour": phases[2] / args.steps, "solve": phases[3] / args.steps},

@@ -293,3 +293,45 @@ def test_gpu_picture_from_a_ring_frame_and_from_host_memory():
     np.testing.assert_array_equal(P.draw_host(P.SPHERES, shown, s.n, cam, 40, 40), want)
     ring.close()
     s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pose", [(1.2, 0.8, -1.6), (0.05, 0.1, 0.02), (-0.4, 0.05, 0.3)])
+def test_gpu_many_bodies_from_outside_and_inside_the_pile(pose):
+    """Thousands of bodies, the camera outside the pile and inside it (bodies beside, behind and around the eye): the
+    tiles keep only the bodies their rays can meet, and the picture is still the oracle's loop over every body."""
+    from vxr import scenes
+    sc = scenes.large_mixed(4096, seed=4, volume=(24.0, 12.0, 24.0))
+    from vxr import learned as Lm
+    w = Lm.settled_world(sc, 60, 10)
+    shown = w.read_shown()
+    n = sc["bodies"]
+    extent = sc["walls"]
+    w.close()
+    cam = P.orbit_camera(extent, pose, alpha=0.3, aspect=160 / 120)
+    got = gpu_picture(P.BOXES, shown, n, cam, 160, 120)
+    want = OP.picture(OP.BOXES, shown, P.push_words(cam, n), 160, 120)
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_gpu_eye_inside_a_sphere_and_spheres_behind():
+    """Spheres around the eye (one holding it), behind it and ahead of it, unpressed and pressed."""
+    rng = np.random.default_rng(11)
+    n = 600
+    s = np.zeros((n, 40), np.float32)
+    s[:, 0:3] = rng.uniform(-1.0, 2.0, (n, 3))
+    s[:, 4:7] = s[:, 0:3] + rng.normal(0, 0.01, (n, 3))
+    s[:, 3] = rng.uniform(0.02, 0.2, n)
+    s[:, 8:20] = np.abs(rng.normal(0, 0.05, (n, 12)))
+    s[:, 20:32] = s[:, 8:20]
+    q = rng.normal(size=(n, 4))
+    s[:, 32:36] = q / np.linalg.norm(q, axis=1, keepdims=True)
+    s[:, 36:40] = s[:, 32:36]
+    eye = np.array([0.5, 0.5, 0.5], np.float32)
+    s[0, 0:3] = s[0, 4:7] = eye + 0.01
+    s[0, 3] = 0.05
+    cam = P.camera(eye, (1, 0, 0), (0, 1, 0), (0, 0, 1), 1.0, 0.5, (1, 1, 1), 1.5)
+    got = gpu_picture(P.SPHERES, s.ravel(), n, cam, 96, 96)
+    want = OP.picture(OP.SPHERES, s.ravel(), P.push_words(cam, n), 96, 96)
+    np.testing.assert_array_equal(got, want)

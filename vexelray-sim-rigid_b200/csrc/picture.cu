@@ -103,92 +103,126 @@ __device__ __forceinline__ void times(const float* m, const float* x, float* y) 
     for (int a = 0; a < 3; a++) y[a] = m[row[a][0]] * x[0] + (m[row[a][1]] * x[1] + m[row[a][2]] * x[2]);
 }
 
-__global__ void k_picture_spheres(Cam c, const float* __restrict__ shown, float* __restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= c.width || j >= c.height) return;
-    float d[3];
-    ray_of(c, i, j, d);
+// ---- a frame's bodies: what no pixel changes ---------------------------------------------------------------------
+// For each body, once a frame: o = eye - its blended centre, the bounding sphere's radius R, and |o|^2 - R^2 (the
+// part of the bounding test's discriminant no pixel changes), each computed as the shaders compute it, so the pixels'
+// results are the same to the bit as computing them per pixel.
+
+constexpr int TILE = 16, THREADS = TILE * TILE, LIST = 1024;
+
+__device__ __forceinline__ float sphere_bound(const Cam& c, const float* s, float* gain_out, float* lift_out) {
+    const float r = s[3];
+    const float trace = mixf(s[PRESSED_BEFORE + TRACE], s[PRESSED_AFTER + TRACE], c.alpha);
+    const float lean_length = mixf(s[PRESSED_BEFORE + LEAN_LENGTH], s[PRESSED_AFTER + LEAN_LENGTH], c.alpha);
+    const float gain = fminf(c.squash, MOST_SQUASH / fmaxf(trace, 1e-9f));
+    const float lift = fmaxf(0.0f, gain * (2.0f / 3.0f) - 1.0f);
+    *gain_out = gain;
+    *lift_out = lift;
+    return r * (1.0f + 0.53f * (gain * trace)) + lift * (r * lean_length);
+}
+
+template <int SHAPE>
+__global__ void k_picture_bodies(Cam c, const float* __restrict__ shown, float4* __restrict__ pre,
+                                 float* __restrict__ reach) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= c.count) return;
+    float o[3], cc, R;
+    if (SHAPE == VXR_RING_SPHERES) {
+        const float* s = shown + (size_t)k * SPHERE_STRIDE;
+        for (int a = 0; a < 3; a++) o[a] = c.eye[a] - mixf(s[a], s[4 + a], c.alpha);
+        float gain, lift;
+        const float bound = sphere_bound(c, s, &gain, &lift);
+        cc = dot3(o, o) - bound * bound;
+        R = bound;
+    } else {
+        const float* s = shown + (size_t)k * BOX_STRIDE;
+        float half[3];
+        for (int a = 0; a < 3; a++) {
+            o[a] = c.eye[a] - mixf(s[CENTRE_BEFORE + a], s[CENTRE_AFTER + a], c.alpha);
+            half[a] = s[HALF + a];
+        }
+        const float reach2 = dot3(half, half);
+        cc = dot3(o, o) - reach2;
+        R = sqrtf(reach2);
+    }
+    pre[k] = make_float4(o[0], o[1], o[2], cc);
+    reach[k] = R;
+}
+
+// ---- one body against one pixel's ray, past the bounding test ------------------------------------------------------
+
+struct SphereHit {
     float best = 1e30f, hit = -1.0f;
     float normal[3] = {0, 0, 0}, local[3] = {0, 0, 0};
-    for (int k = 0; k < c.count; k++) {
-        const float* s = shown + (size_t)k * SPHERE_STRIDE;
-        float ctr[3], o[3];
-        for (int a = 0; a < 3; a++) {
-            ctr[a] = mixf(s[a], s[4 + a], c.alpha);
-            o[a] = c.eye[a] - ctr[a];
-        }
-        const float r = s[3];
-        const float trace = mixf(s[PRESSED_BEFORE + TRACE], s[PRESSED_AFTER + TRACE], c.alpha);
-        const float lean_length = mixf(s[PRESSED_BEFORE + LEAN_LENGTH], s[PRESSED_AFTER + LEAN_LENGTH], c.alpha);
-        const float gain = fminf(c.squash, MOST_SQUASH / fmaxf(trace, 1e-9f));
-        const float lift = fmaxf(0.0f, gain * (2.0f / 3.0f) - 1.0f);
-        const float bound = r * (1.0f + 0.53f * (gain * trace)) + lift * (r * lean_length);
-        const float half = dot3(o, d);
-        const float disc = half * half - (dot3(o, o) - bound * bound);
-        if (!(disc > 0.0f)) continue;
-        const float root = sqrtf(disc);
-        if (!(root - half > 0.0f && -half - root < best)) continue;
-        // squashed :123-176
-        float m[6];
-        for (int q = 0; q < 6; q++) {
-            const float pressed = gain * mixf(s[PRESSED_BEFORE + q], s[PRESSED_AFTER + q], c.alpha);
-            m[q] = q < 3 ? 1.0f - pressed : -pressed;
-        }
-        const float adj[6] = {m[1] * m[2] - m[5] * m[5], m[0] * m[2] - m[4] * m[4], m[0] * m[1] - m[3] * m[3],
-                              m[4] * m[5] - m[3] * m[2], m[3] * m[5] - m[4] * m[1], m[3] * m[4] - m[0] * m[5]};
-        const float det = m[0] * adj[0] + (m[3] * adj[3] + m[4] * adj[4]);
-        float cube = 1.0f - (3.0f - (m[0] + (m[1] + m[2]))) / 3.0f;
-        for (int step = 0; step < 2; step++) cube = (2.0f * cube + det / (cube * cube)) / 3.0f;
-        const float scale = cube / det;
-        float inv[6];
-        for (int q = 0; q < 6; q++) inv[q] = adj[q] * scale;
-        float om[3];
-        for (int a = 0; a < 3; a++) {
-            const float moved = ctr[a] + (lift * r) * mixf(s[PRESSED_BEFORE + LEAN + a], s[PRESSED_AFTER + LEAN + a], c.alpha);
-            om[a] = c.eye[a] - moved;
-        }
-        float os[3], ds[3];
-        times(inv, om, os);
-        times(inv, d, ds);
-        const float aa = dot3(ds, ds), hh = dot3(os, ds);
-        const float disc2 = hh * hh - aa * (dot3(os, os) - r * r);
-        if (!(disc2 > 0.0f)) continue;
-        const float t = (-hh - sqrtf(disc2)) / aa;
-        if (!(t > 0.0f && t < best)) continue;
-        best = t;
-        hit = (float)k;
-        float u[3];
-        for (int a = 0; a < 3; a++) {
-            u[a] = os[a] + t * ds[a];
-            local[a] = u[a];
-        }
-        times(inv, u, normal);
+};
+
+// SphereShader.squashed :158-214
+__device__ __forceinline__ void squashed(const Cam& c, const float* __restrict__ shown, int k, const float* d,
+                                         SphereHit& h) {
+    const float* s = shown + (size_t)k * SPHERE_STRIDE;
+    float ctr[3];
+    for (int a = 0; a < 3; a++) ctr[a] = mixf(s[a], s[4 + a], c.alpha);
+    const float r = s[3];
+    float gain, lift;
+    sphere_bound(c, s, &gain, &lift);
+    float m[6];
+    for (int q = 0; q < 6; q++) {
+        const float pressed = gain * mixf(s[PRESSED_BEFORE + q], s[PRESSED_AFTER + q], c.alpha);
+        m[q] = q < 3 ? 1.0f - pressed : -pressed;
     }
-    float rgb[3];
-    background(c, d, best, rgb);
-    if (hit > -0.5f) {
-        // turned :186-214: the octant in the sphere's own frame, the orientation blended the short way round
-        const float* s = shown + (size_t)(int)hit * SPHERE_STRIDE;
-        const float* before = s + TURNED_BEFORE_S;
-        const float* after = s + TURNED_AFTER_S;
-        float way = 1.0f;
-        if (dot3(before, after) + before[3] * after[3] < 0.0f) way = -1.0f;
-        float q[3];
-        for (int a = 0; a < 3; a++) q[a] = -mixf(before[a] * way, after[a], c.alpha);
-        const float w = mixf(before[3] * way, after[3], c.alpha);
-        float t[3], qt[3];
-        cross(q, local, t);
-        for (int a = 0; a < 3; a++) t[a] = 2.0f * t[a];
-        cross(q, t, qt);
-        float p[3];
-        for (int a = 0; a < 3; a++) p[a] = local[a] + (w * t[a] + qt[a]);
-        const float patch = (p[0] * p[1]) * p[2] > 0.0f ? PALE : 0.0f;
-        shade(d, hit, normal, patch, rgb);
+    const float adj[6] = {m[1] * m[2] - m[5] * m[5], m[0] * m[2] - m[4] * m[4], m[0] * m[1] - m[3] * m[3],
+                          m[4] * m[5] - m[3] * m[2], m[3] * m[5] - m[4] * m[1], m[3] * m[4] - m[0] * m[5]};
+    const float det = m[0] * adj[0] + (m[3] * adj[3] + m[4] * adj[4]);
+    float cube = 1.0f - (3.0f - (m[0] + (m[1] + m[2]))) / 3.0f;
+    for (int step = 0; step < 2; step++) cube = (2.0f * cube + det / (cube * cube)) / 3.0f;
+    const float scale = cube / det;
+    float inv[6];
+    for (int q = 0; q < 6; q++) inv[q] = adj[q] * scale;
+    float om[3];
+    for (int a = 0; a < 3; a++) {
+        const float moved = ctr[a] + (lift * r) * mixf(s[PRESSED_BEFORE + LEAN + a], s[PRESSED_AFTER + LEAN + a], c.alpha);
+        om[a] = c.eye[a] - moved;
     }
-    float* o = out + 3 * ((size_t)j * c.width + i);
-    o[0] = rgb[0];
-    o[1] = rgb[1];
-    o[2] = rgb[2];
+    float os[3], ds[3];
+    times(inv, om, os);
+    times(inv, d, ds);
+    const float aa = dot3(ds, ds), hh = dot3(os, ds);
+    const float disc = hh * hh - aa * (dot3(os, os) - r * r);
+    if (!(disc > 0.0f)) return;
+    const float t = (-hh - sqrtf(disc)) / aa;
+    if (!(t > 0.0f && t < h.best)) return;
+    h.best = t;
+    h.hit = (float)k;
+    float u[3];
+    for (int a = 0; a < 3; a++) {
+        u[a] = os[a] + t * ds[a];
+        h.local[a] = u[a];
+    }
+    times(inv, u, h.normal);
+}
+
+// SphereShader.fragmentSpirv's colour (:131-140) and turned (:225-253): the octant in the sphere's own frame, the
+// orientation blended the short way round.
+__device__ __forceinline__ void sphere_colour(const Cam& c, const float* __restrict__ shown, const float* d,
+                                              SphereHit& h, float* rgb) {
+    background(c, d, h.best, rgb);
+    if (!(h.hit > -0.5f)) return;
+    const float* s = shown + (size_t)(int)h.hit * SPHERE_STRIDE;
+    const float* before = s + TURNED_BEFORE_S;
+    const float* after = s + TURNED_AFTER_S;
+    float way = 1.0f;
+    if (dot3(before, after) + before[3] * after[3] < 0.0f) way = -1.0f;
+    float q[3];
+    for (int a = 0; a < 3; a++) q[a] = -mixf(before[a] * way, after[a], c.alpha);
+    const float w = mixf(before[3] * way, after[3], c.alpha);
+    float t[3], qt[3];
+    cross(q, h.local, t);
+    for (int a = 0; a < 3; a++) t[a] = 2.0f * t[a];
+    cross(q, t, qt);
+    float p[3];
+    for (int a = 0; a < 3; a++) p[a] = h.local[a] + (w * t[a] + qt[a]);
+    const float patch = (p[0] * p[1]) * p[2] > 0.0f ? PALE : 0.0f;
+    shade(d, h.hit, h.normal, patch, rgb);
 }
 
 // BoxShader.rotate :197-211: p turned by q of any length.
@@ -201,94 +235,195 @@ __device__ __forceinline__ void rotate(const float* q, const float* p, float* ou
     for (int a = 0; a < 3; a++) out[a] = p[a] + (q[3] * t[a] + qt[a]);
 }
 
-__global__ void k_picture_boxes(Cam c, const float* __restrict__ shown, float* __restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= c.width || j >= c.height) return;
-    float d[3];
-    ray_of(c, i, j, d);
+struct BoxHit {
     float best = 1e30f, hit = -1.0f, edged = 0.0f, pale = 0.0f;
     float normal[3] = {0, 0, 0};
-    for (int k = 0; k < c.count; k++) {
-        const float* s = shown + (size_t)k * BOX_STRIDE;
-        float o[3], half[3];
-        for (int a = 0; a < 3; a++) {
-            o[a] = c.eye[a] - mixf(s[CENTRE_BEFORE + a], s[CENTRE_AFTER + a], c.alpha);
-            half[a] = s[HALF + a];
+};
+
+// BoxShader.slabs :115-190; o is the eye less the box's blended centre.
+__device__ __forceinline__ void slabs(const Cam& c, const float* __restrict__ shown, int k, const float* o,
+                                      const float* d, BoxHit& h) {
+    const float* s = shown + (size_t)k * BOX_STRIDE;
+    float half[3];
+    for (int a = 0; a < 3; a++) half[a] = s[HALF + a];
+    const float* before = s + TURNED_BEFORE_B;
+    const float* after = s + TURNED_AFTER_B;
+    float way = 1.0f;
+    if (dot3(before, after) + before[3] * after[3] < 0.0f) way = -1.0f;
+    float q[4];
+    for (int a = 0; a < 4; a++) q[a] = mixf(before[a] * way, after[a], c.alpha);
+    const float inverse[4] = {-q[0], -q[1], -q[2], q[3]};
+    float os[3], ds[3];
+    rotate(inverse, o, os);
+    rotate(inverse, d, ds);
+    const float round = s[SHAPE];
+    if (round > 0.5f) {
+        const float hh = dot3(os, ds);
+        const float cc = dot3(os, os) - half[0] * half[0];
+        const float bdisc = hh * hh - dot3(ds, ds) * cc;
+        if (bdisc > 0.0f) {
+            const float t = (-hh - sqrtf(bdisc)) / dot3(ds, ds);
+            if (t > 0.0f && t < h.best) {
+                h.best = t;
+                h.hit = (float)k;
+                float own[3];
+                for (int a = 0; a < 3; a++) own[a] = os[a] + t * ds[a];
+                rotate(q, own, h.normal);
+                h.edged = 0.0f;
+                h.pale = (own[0] * own[1]) * own[2] > 0.0f ? 1.0f : 0.0f;
+            }
         }
-        const float reach2 = dot3(half, half);
-        const float along = dot3(o, d);
-        const float disc = along * along - (dot3(o, o) - reach2);
-        if (!(disc > 0.0f)) continue;
-        const float root = sqrtf(disc);
-        if (!(root - along > 0.0f && -along - root < best)) continue;
-        // slabs :94-191
-        const float* before = s + TURNED_BEFORE_B;
-        const float* after = s + TURNED_AFTER_B;
-        float way = 1.0f;
-        if (dot3(before, after) + before[3] * after[3] < 0.0f) way = -1.0f;
-        float q[4];
-        for (int a = 0; a < 4; a++) q[a] = mixf(before[a] * way, after[a], c.alpha);
-        const float inverse[4] = {-q[0], -q[1], -q[2], q[3]};
-        float os[3], ds[3];
-        rotate(inverse, o, os);
-        rotate(inverse, d, ds);
-        const float round = s[SHAPE];
-        if (round > 0.5f) {
-            const float hh = dot3(os, ds);
-            const float cc = dot3(os, os) - half[0] * half[0];
-            const float bdisc = hh * hh - dot3(ds, ds) * cc;
-            if (bdisc > 0.0f) {
-                const float t = (-hh - sqrtf(bdisc)) / dot3(ds, ds);
-                if (t > 0.0f && t < best) {
-                    best = t;
-                    hit = (float)k;
-                    float own[3];
-                    for (int a = 0; a < 3; a++) own[a] = os[a] + t * ds[a];
-                    rotate(q, own, normal);
-                    edged = 0.0f;
-                    pale = (own[0] * own[1]) * own[2] > 0.0f ? 1.0f : 0.0f;
+    }
+    float enter = -1e30f, leave = 1e30f, face = 0.0f;
+    for (int a = 0; a < 3; a++) {
+        float step = ds[a];
+        if (fabsf(step) < PARALLEL) step = PARALLEL;
+        const float t1 = (-half[a] - os[a]) / step;
+        const float t2 = (half[a] - os[a]) / step;
+        const float near = fminf(t1, t2);
+        leave = fminf(leave, fmaxf(t1, t2));
+        if (near > enter) {
+            enter = near;
+            face = (float)a;
+        }
+    }
+    if (enter < leave && enter > 0.0f && enter < h.best && !(round > 0.5f)) {
+        h.best = enter;
+        h.hit = (float)k;
+        float own[3], gap[3];
+        for (int a = 0; a < 3; a++) {
+            const float on = (face > (float)a - 0.5f && face < (float)a + 0.5f) ? 1.0f : 0.0f;
+            own[a] = -(on * ds[a]);
+            const float p = os[a] + enter * ds[a];
+            gap[a] = half[a] - fabsf(p);
+        }
+        rotate(q, own, h.normal);
+        const float sum = (gap[0] + gap[1]) + gap[2];
+        const float least = fminf(gap[0], fminf(gap[1], gap[2]));
+        const float most = fmaxf(gap[0], fmaxf(gap[1], gap[2]));
+        const float to_edge = (sum - least) - most;
+        const float band = EDGE * fminf(half[0], fminf(half[1], half[2]));
+        h.edged = to_edge < band ? 1.0f : 0.0f;
+        h.pale = 0.0f;
+    }
+}
+
+__device__ __forceinline__ void box_colour(const Cam& c, const float* d, BoxHit& h, float* rgb) {
+    background(c, d, h.best, rgb);
+    if (!(h.hit > -0.5f)) return;
+    shade(d, h.hit, h.normal, PALE * h.pale, rgb);
+    for (int a = 0; a < 3; a++) rgb[a] = rgb[a] * mixf(1.0f, EDGE_LIGHT, h.edged);
+}
+
+// ---- a tile of pixels ----------------------------------------------------------------------------------------------
+// One block a 16 x 16 tile. The block first keeps, in ascending order, the bodies whose bounding sphere can meet a
+// ray of the tile: those within R (plus a slack far above f32 rounding) of the inside of the four planes through the
+// eye and the tile's corner rays. Every pixel then runs the shaders' loop over the kept bodies alone. A body left out
+// is one whose bounding test fails at every pixel of the tile, so it changes nothing there: the picture is the one the
+// shaders' loop over every body gives, to the bit.
+
+// The side planes of the tile's rays, through the eye, inward: from the f32 corner rays, in doubles, so that the
+// planes hold those rays exactly; a plane whose corner rays coincide (a tile one pixel wide or high) is left out.
+__device__ void tile_planes(const Cam& c, int i0, int j0, int i1, int j1, float (*plane)[4]) {
+    const int q = threadIdx.y * TILE + threadIdx.x;
+    if (q >= 4) return;
+    float f[4][3];
+    ray_of(c, i0, j0, f[0]);
+    ray_of(c, i1, j0, f[1]);
+    ray_of(c, i1, j1, f[2]);
+    ray_of(c, i0, j1, f[3]);
+    const float* x = f[q];
+    const float* y = f[(q + 1) & 3];
+    double n[3] = {(double)x[1] * y[2] - (double)x[2] * y[1], (double)x[2] * y[0] - (double)x[0] * y[2],
+                   (double)x[0] * y[1] - (double)x[1] * y[0]};
+    double inward = 0.0;
+    for (int a = 0; a < 3; a++) inward += n[a] * ((double)f[0][a] + f[1][a] + f[2][a] + f[3][a]);
+    const double len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    const double sign = inward < 0.0 ? -1.0 : 1.0;
+    for (int a = 0; a < 3; a++) plane[q][a] = len > 0.0 ? (float)(sign * n[a] / len) : 0.0f;
+    plane[q][3] = len > 0.0 ? 1.0f : 0.0f;
+}
+
+template <int SHAPE>
+__global__ void __launch_bounds__(THREADS) k_picture(Cam c, const float* __restrict__ shown,
+                                                     const float4* __restrict__ pre, const float* __restrict__ reach,
+                                                     float* __restrict__ out) {
+    __shared__ float4 s_pre[LIST];
+    __shared__ int s_body[LIST];
+    __shared__ float s_plane[4][4];
+    __shared__ int s_warp[THREADS / 32];
+    const int tid = threadIdx.y * TILE + threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i0 = blockIdx.x * TILE, j0 = blockIdx.y * TILE;
+    const int i1 = min(i0 + TILE - 1, c.width - 1), j1 = min(j0 + TILE - 1, c.height - 1);
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+    const bool inside = i < c.width && j < c.height;
+    float d[3];
+    ray_of(c, min(i, c.width - 1), min(j, c.height - 1), d);
+    tile_planes(c, i0, j0, i1, j1, s_plane);
+    __syncthreads();
+    SphereHit sh;
+    BoxHit bh;
+    int listed = 0;
+    for (int base = 0; base < c.count; base += THREADS) {
+        const int k = base + tid;
+        bool keep = false;
+        float4 p = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (k < c.count) {
+            p = pre[k];
+            const float R = reach[k];
+            const float len = sqrtf(p.x * p.x + p.y * p.y + p.z * p.z);
+            // rounding in the pixels' f32 tests moves a ray's reach by far less than this (1e-6 relative at most)
+            const float slack = R + 1e-5f * (R + len + len * (len / fmaxf(R, 1e-20f)));
+            keep = true;
+            for (int q = 0; q < 4; q++) {
+                if (s_plane[q][3] == 0.0f) continue;
+                const float inside_by = -(p.x * s_plane[q][0] + p.y * s_plane[q][1] + p.z * s_plane[q][2]);
+                if (inside_by < -slack) keep = false;
+            }
+        }
+        const unsigned vote = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_warp[warp] = __popc(vote);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < THREADS / 32; w++) {
+            const int n = s_warp[w];
+            before += w < warp ? n : 0;
+            total += n;
+        }
+        if (keep) {
+            const int at = listed + before + __popc(vote & ((1u << lane) - 1u));
+            s_pre[at] = p;
+            s_body[at] = k;
+        }
+        listed += total;
+        __syncthreads();
+        if (listed > LIST - THREADS || base + THREADS >= c.count) {
+            if (inside) {
+                for (int e = 0; e < listed; e++) {
+                    const float4 q = s_pre[e];
+                    const float o[3] = {q.x, q.y, q.z};
+                    const float half = dot3(o, d);
+                    const float disc = half * half - q.w;
+                    if (!(disc > 0.0f)) continue;
+                    const float root = sqrtf(disc);
+                    const float best = SHAPE == VXR_RING_SPHERES ? sh.best : bh.best;
+                    if (!(root - half > 0.0f && -half - root < best)) continue;
+                    if (SHAPE == VXR_RING_SPHERES)
+                        squashed(c, shown, s_body[e], d, sh);
+                    else
+                        slabs(c, shown, s_body[e], o, d, bh);
                 }
             }
-        }
-        float enter = -1e30f, leave = 1e30f, face = 0.0f;
-        for (int a = 0; a < 3; a++) {
-            float step = ds[a];
-            if (fabsf(step) < PARALLEL) step = PARALLEL;
-            const float t1 = (-half[a] - os[a]) / step;
-            const float t2 = (half[a] - os[a]) / step;
-            const float near = fminf(t1, t2);
-            leave = fminf(leave, fmaxf(t1, t2));
-            if (near > enter) {
-                enter = near;
-                face = (float)a;
-            }
-        }
-        if (enter < leave && enter > 0.0f && enter < best && !(round > 0.5f)) {
-            best = enter;
-            hit = (float)k;
-            float own[3], gap[3];
-            for (int a = 0; a < 3; a++) {
-                const float on = (face > (float)a - 0.5f && face < (float)a + 0.5f) ? 1.0f : 0.0f;
-                own[a] = -(on * ds[a]);
-                const float p = os[a] + enter * ds[a];
-                gap[a] = half[a] - fabsf(p);
-            }
-            rotate(q, own, normal);
-            const float sum = (gap[0] + gap[1]) + gap[2];
-            const float least = fminf(gap[0], fminf(gap[1], gap[2]));
-            const float most = fmaxf(gap[0], fmaxf(gap[1], gap[2]));
-            const float to_edge = (sum - least) - most;
-            const float band = EDGE * fminf(half[0], fminf(half[1], half[2]));
-            edged = to_edge < band ? 1.0f : 0.0f;
-            pale = 0.0f;
+            listed = 0;
+            __syncthreads();
         }
     }
+    if (!inside) return;
     float rgb[3];
-    background(c, d, best, rgb);
-    if (hit > -0.5f) {
-        shade(d, hit, normal, PALE * pale, rgb);
-        for (int a = 0; a < 3; a++) rgb[a] = rgb[a] * mixf(1.0f, EDGE_LIGHT, edged);
-    }
+    if (SHAPE == VXR_RING_SPHERES)
+        sphere_colour(c, shown, d, sh, rgb);
+    else
+        box_colour(c, d, bh, rgb);
     float* o = out + 3 * ((size_t)j * c.width + i);
     o[0] = rgb[0];
     o[1] = rgb[1];
@@ -335,12 +470,28 @@ int32_t vxr_picture(int32_t shape, const float* shown, int32_t count, const vxr_
     if (shape != VXR_RING_SPHERES && shape != VXR_RING_BOXES) return VXR_EINVAL;
     if (set_light() != VXR_OK) return VXR_ECUDA;
     const Cam c = cam_of(camera, count, width, height);
-    const dim3 block(16, 16), grid((width + 15) / 16, (height + 15) / 16);
     cudaStream_t st = (cudaStream_t)stream;
+    float4* pre = nullptr;
+    float* reach = nullptr;
+    if (count > 0) {
+        // a frame's scratch from the stream-ordered pool: no synchronisation, nothing shared between streams
+        void* scratch = nullptr;
+        if (cudaMallocAsync(&scratch, (size_t)count * (sizeof(float4) + sizeof(float)), st) != cudaSuccess)
+            return VXR_ECUDA;
+        pre = (float4*)scratch;
+        reach = (float*)(pre + count);
+        const int blocks = (count + 255) / 256;
+        if (shape == VXR_RING_SPHERES)
+            k_picture_bodies<VXR_RING_SPHERES><<<blocks, 256, 0, st>>>(c, shown, pre, reach);
+        else
+            k_picture_bodies<VXR_RING_BOXES><<<blocks, 256, 0, st>>>(c, shown, pre, reach);
+    }
+    const dim3 block(TILE, TILE), grid((width + TILE - 1) / TILE, (height + TILE - 1) / TILE);
     if (shape == VXR_RING_SPHERES)
-        k_picture_spheres<<<grid, block, 0, st>>>(c, shown, rgb);
+        k_picture<VXR_RING_SPHERES><<<grid, block, 0, st>>>(c, shown, pre, reach, rgb);
     else
-        k_picture_boxes<<<grid, block, 0, st>>>(c, shown, rgb);
+        k_picture<VXR_RING_BOXES><<<grid, block, 0, st>>>(c, shown, pre, reach, rgb);
+    if (pre && cudaFreeAsync(pre, st) != cudaSuccess) return VXR_ECUDA;
     return cudaGetLastError() == cudaSuccess ? VXR_OK : VXR_ECUDA;
 }
 
