@@ -727,6 +727,13 @@ def main():
     slowest_ms = all_max(pg, total_ms)
     bodies_all = all_sum(pg, float(scene["bodies"]))
     value = bodies_all * args.steps / (slowest_ms / 1e3)
+    # the drop's phases: body-steps/s over windows of 100 timed steps (this rank's own events)
+    windows = []
+    for lo in range(0, args.steps, 100):
+        ms = float(sum(step_ms[lo:lo + 100]))
+        hi = min(lo + 100, args.steps)
+        windows.append({"steps": f"{args.warmup + lo}..{args.warmup + hi - 1}", "ms_per_step": ms / (hi - lo),
+                        "value": scene["bodies"] * (hi - lo) / (ms / 1e3)})
 
     # roofline of the solve kernel: bytes per launch from the last step's activity, time per launch from events
     hbm, which = peaks()
@@ -734,6 +741,8 @@ def main():
     b_solve = algorithmic_solve_bytes(scene["bodies"], scene["substeps"], scene["sweeps"], activity["touching"],
                                       activity["points"], activity["bodies_active"], activity["wall_records"])
     achieved = b_solve / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
+    pic = picture_timing(w, 1, scene["bodies"], scene["walls"], local, squash=0.0,
+                         cpu=rank == 0 and not args.no_cpu)
 
     # Iterations to residual: the same world, the pile as the timed steps left it, a substep's solve sweeps run until
     # a sweep's residual (the largest positional correction it makes at any contact point) is 1e-4 m or less, at most
@@ -805,6 +814,7 @@ def main():
                    "parallelism": "replicas" if world_size > 1 else "single"},
         "phase_ms_per_step": {"broad": phases[0] / args.steps, "narrow": phases[1] / args.steps,
                               "colour": phases[2] / args.steps, "solve": phases[3] / args.steps},
+        "windows": windows,
         "last_step": {"touching": rep.touching, "points": rep.points, "rounds": rep.rounds,
                       "unplaced": rep.unplaced, "unlisted": rep.unlisted, **activity},
         "roofline": {"bound": "hbm", "kernel": "k_solve", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -813,6 +823,7 @@ def main():
         "gpu_launches": int(launches),
         "iterations_to_residual": iters,
         "judged_500_steps": judged,
+        "picture": pic,
         "e2e": e2e,
     }
     line["clocks"] = clocks.summary()

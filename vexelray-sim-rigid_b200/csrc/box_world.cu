@@ -822,8 +822,8 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
         soft.mu_static = word_of(A, sc, P_MU_STATIC);
         soft.mu_kinetic = word_of(A, sc, P_MU_KINETIC);
     }
-    bool touched = false;
-    for (int order = 0; order < 6; order++) {
+    bool touched = false, box_corners = false;
+    for (int order = 0; order < 6 && !box_corners; order++) {
         const int wall = reverse ? 5 - order : order;
         if (!((visit >> wall) & 1u)) continue;
         const int axis = wall / 2;
@@ -859,50 +859,67 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
                 touched = true;
             }
         } else {
-            // The held corners' records, each loaded while the corner before it is solved (a corner's record is
-            // written only by its own turn, after it is read).
+            box_corners = true;
+        }
+    }
+    if (box_corners) {
+        // A box: first which corners run, wall by wall in the sweep's order and corner by corner in it (a held
+        // corner always; another, outside the warm sweep, where its wall is near and its gap is under the margin),
+        // then those corners alone, in that order. Whether a corner runs depends only on the pose, which the walls
+        // do not change, and on its own held bit, which only its own turn changes, so the order and every result
+        // are the reference's. Lanes of a warp then solve their k-th corners together, whichever corners they are.
+        unsigned long long todo = 0ull;
+        for (int order = 0; order < 6; order++) {
+            const int wall = reverse ? 5 - order : order;
+            if (!((visit >> wall) & 1u)) continue;
             const unsigned held_bits = (unsigned)((mask >> (wall * 8)) & 0xffull);
-            int next = -1;
-            for (int j = 0; j < 8 && next < 0; j++) {
-                const int c = reverse ? 7 - j : j;
-                if ((held_bits >> c) & 1u) next = j;
-            }
-            float4 ahead = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (next >= 0) ahead = __ldcg(&A.wall[(long)s * WALL_RECORDS + wall * 8 + (reverse ? 7 - next : next)]);
-            for (int k2 = 0; k2 < 8; k2++) {
-                const int c = reverse ? 7 - k2 : k2;
-                const int bit = wall * 8 + c;
-                const bool held = (mask >> bit) & 1ull;
-                float4 loaded = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                if (held) {
-                    loaded = ahead;
-                    next = -1;
-                    for (int j = k2 + 1; j < 8 && next < 0; j++) {
-                        const int cj = reverse ? 7 - j : j;
-                        if ((held_bits >> cj) & 1u) next = j;
-                    }
-                    if (next >= 0)
-                        ahead = __ldcg(&A.wall[(long)s * WALL_RECORDS + wall * 8 + (reverse ? 7 - next : next)]);
-                }
-                if (!held && (sweep == WARM || !((near >> wall) & 1u))) continue;
+            todo |= (unsigned long long)held_bits << (wall * 8);
+            if (sweep == WARM || !((near >> wall) & 1u)) continue;
+            const int axis = wall / 2;
+            const bool high = wall % 2 == 1;
+            for (int c = 0; c < 8; c++) {
+                if ((held_bits >> c) & 1u) continue;
                 float offset[3], r[3];
-                for (int a = 0; a < 3; a++) {
-                    const int sgn = (c >> a) & 1;
-                    offset[a] = box.half[a] * (2.0f * (float)sgn - 1.0f);
-                }
+                for (int a = 0; a < 3; a++) offset[a] = box.half[a] * (2.0f * (float)((c >> a) & 1) - 1.0f);
                 rotate_by(box.q, box.twice, offset, r);
                 const float reach = pick3(box.at, axis) + pick3(r, axis);
                 const float gap = high ? pick3(extent, axis) - reach : reach;
-                if (!(held || (sweep != WARM && gap < margin))) continue;
-                const long at = (long)s * WALL_RECORDS + bit;
-                float4 rec = loaded;
-                contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft, -1.0f, track);
-                if (sweep != WARM) {
-                    __stcg(&A.wall[at], rec);
-                    mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
-                }
-                touched = true;
+                if (gap < margin) todo |= 1ull << (wall * 8 + c);
             }
+        }
+        // the corners in the sweep's order: walls ascending and corners ascending, or both descending
+        int bit = -1;
+        auto next_bit = [&](unsigned long long left) {
+            if (left == 0ull) return -1;
+            return reverse ? 63 - __clzll((long long)left) : __ffsll((long long)left) - 1;
+        };
+        bit = next_bit(todo);
+        float4 ahead = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (bit >= 0 && ((mask >> bit) & 1ull)) ahead = __ldcg(&A.wall[(long)s * WALL_RECORDS + bit]);
+        while (bit >= 0) {
+            todo &= ~(1ull << bit);
+            const int wall = bit / 8, c = bit % 8;
+            const bool held = (mask >> bit) & 1ull;
+            const float4 loaded = held ? ahead : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            const int after = next_bit(todo);
+            if (after >= 0 && ((mask >> after) & 1ull)) ahead = __ldcg(&A.wall[(long)s * WALL_RECORDS + after]);
+            const int axis = wall / 2;
+            const bool high = wall % 2 == 1;
+            float n[3];
+            for (int a = 0; a < 3; a++) n[a] = a == axis ? (high ? -1.0f : 1.0f) : 0.0f;
+            float offset[3], r[3];
+            for (int a = 0; a < 3; a++) offset[a] = box.half[a] * (2.0f * (float)((c >> a) & 1) - 1.0f);
+            rotate_by(box.q, box.twice, offset, r);
+            const float reach = pick3(box.at, axis) + pick3(r, axis);
+            const float gap = high ? pick3(extent, axis) - reach : reach;
+            float4 rec = loaded;
+            contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft, -1.0f, track);
+            if (sweep != WARM) {
+                __stcg(&A.wall[(long)s * WALL_RECORDS + bit], rec);
+                mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
+            }
+            touched = true;
+            bit = after;
         }
     }
     if (touched) __stcg(&A.wmask[s], mask);
@@ -951,11 +968,22 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
     }
     const float n[3] = {head.x, head.y, head.z};
     const bool anySphere = first.sphere() || second.sphere();
+    // The points in turn (backward: last to first). Past the first sweep of a half, each point's kept terms and
+    // impulses are loaded while the point before it is solved: their addresses depend on the pair alone, and no
+    // point writes another's records.
+    float4 next_a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), next_b = next_a, next_imp = next_a;
+    if (!fill && count > 0) {
+        const long at0 = k * MOST_POINTS + (reverse ? count - 1 : 0);
+        next_a = __ldcg(&A.pairs.prepA[at0]);
+        next_b = __ldcg(&A.pairs.prepB[at0]);
+        next_imp = __ldcg(&A.pairs.imp[at0]);
+    }
     for (int order = 0; order < MOST_POINTS; order++) {
         const int slot = reverse ? MOST_POINTS - 1 - order : order;
         if (!(slot < count)) continue;
         const long at = k * MOST_POINTS + slot;
         float rA[3], rB[3], gap, kn;
+        float4 rec;
         if (fill) {
             if (first.sphere()) {
                 for (int a = 0; a < 3; a++) rA[a] = first.half[0] * n[a];
@@ -977,12 +1005,20 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
             kn = mass_along<true>(first, rA, second, rB, n);
             __stcg(&A.pairs.prepA[at], make_float4(rA[0], rA[1], rA[2], gap));
             __stcg(&A.pairs.prepB[at], make_float4(rB[0], rB[1], rB[2], kn));
+            rec = __ldcg(&A.pairs.imp[at]);
         } else {
-            const float4 pa = __ldcg(&A.pairs.prepA[at]), pb = __ldcg(&A.pairs.prepB[at]);
+            const float4 pa = next_a, pb = next_b;
+            rec = next_imp;
+            const int later = reverse ? slot - 1 : slot + 1;
+            if (later >= 0 && later < count) {
+                const long at1 = k * MOST_POINTS + later;
+                next_a = __ldcg(&A.pairs.prepA[at1]);
+                next_b = __ldcg(&A.pairs.prepB[at1]);
+                next_imp = __ldcg(&A.pairs.imp[at1]);
+            }
             rA[0] = pa.x; rA[1] = pa.y; rA[2] = pa.z; gap = pa.w;
             rB[0] = pb.x; rB[1] = pb.y; rB[2] = pb.z; kn = pb.w;
         }
-        float4 rec = __ldcg(&A.pairs.imp[at]);
         contact<true>(sweep, gap, n, first, rA, second, rB, rec, soft, kn, track);
         if (sweep != WARM) __stcg(&A.pairs.imp[at], rec);
         if (anySphere) {
@@ -999,12 +1035,16 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
     store_held(second, A.b, ib);
 }
 
-// One round of pairs that share no body (the barrier schedule).
+// One round of pairs that share no body (the barrier schedule). A round's pairs lie in kind order (sphere pairs
+// first, box pairs by point count last); its runs of 32 are dealt to the blocks in turn, so the heavy runs at the
+// round's end spread over every SM instead of crowding a few, and each warp's pairs stay of one kind. Which
+// thread solves a pair of a round changes no result: the round's pairs share no body.
 __device__ __forceinline__ void phase_round(const SolveArgs& A, int sweep, bool reverse, int r, bool fill,
                                             unsigned* track) {
-    const int stride = gridDim.x * blockDim.x;
+    const long runs = (long)gridDim.x * (blockDim.x >> 5);
+    const long run = (long)(threadIdx.x >> 5) * gridDim.x + blockIdx.x;
     const int lo = A.round_start[r], hi = A.round_start[r + 1];
-    for (int k = lo + blockIdx.x * blockDim.x + threadIdx.x; k < hi; k += stride)
+    for (long k = lo + run * 32 + (threadIdx.x & 31); k < hi; k += runs * 32)
         solve_pair(A, k, __ldg(&A.pairs.pair[k]), sweep, reverse, fill, track);
 }
 
@@ -1091,7 +1131,7 @@ __device__ __forceinline__ bool block_of_sweeps(const SolveArgs& A, int first_ki
     return true;
 }
 
-// Phase codes of the trace: kind | sweep << 4 | round << 8.
+// Phase codes of the trace: kind | sweep << 4 | one-block run << 7 | round << 8.
 enum : int { TR_START = 0, TR_VELOCITIES = 1, TR_WALLS = 2, TR_POSITIONS = 3, TR_ROUND = 4, TR_WALL_LIST = 5,
             TR_BLOCK = 6 };
 
@@ -1142,7 +1182,7 @@ __device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsign
                 for (int k = lo + threadIdx.x; k < hi; k += blockDim.x)
                     solve_pair(A, k, __ldg(&A.pairs.pair[k]), kind, reverse, fill, track);
                 __syncthreads();
-                tr.mark(TR_ROUND | kind << 4 | q << 8);
+                tr.mark(TR_ROUND | kind << 4 | 1 << 7 | q << 8);  // bit 7: a round of a one-block run
             }
         }
         if (!grid_sync(A.bar, epoch)) return false;
@@ -1163,7 +1203,7 @@ __device__ __forceinline__ bool converged(const SolveArgs& A, int index) {
     return __uint_as_float(*(volatile unsigned*)&A.residual[index]) <= A.tolerance;
 }
 
-__global__ void __launch_bounds__(SOLVE_THREADS) k_solve(SolveArgs A) {
+__global__ void __launch_bounds__(SOLVE_THREADS, 2) k_solve(SolveArgs A) {
     const int rounds = *(volatile int*)&A.counters->rounds;
     Tracer tr{A.trace, A.trace_cap, 0};
     unsigned int epoch = 0;
