@@ -209,3 +209,29 @@ def test_gpu_a_warm_start_converges_in_fewer_sweeps_than_a_cold_one():
     warm = iterations(scene.world, 5, cold=False)
     cold = iterations(scene.world, 5, cold=True)
     assert warm < cold, (warm, cold)
+
+
+def test_gpu_towers_match_the_oracle():
+    """The box-stacking configuration's towers, a 2 x 2 block 16 high, at its 8 substeps and 16 sweeps: after
+    every 20 of 100 steps every state word equals the oracle's, to the bit (the towers settle, lean and start to
+    topple over these steps)."""
+    from oracle.box import OracleBoxWorld
+    from vxr import scenes
+    from vxr.box_simulation import BoxSimulation
+    sc = scenes.towers(seed=5, towers_x=2, towers_z=2, height=16)
+    o = OracleBoxWorld(sc["bodies"], sc["substeps"], sc["sweeps"], False, sc["grid"], threads=True)
+    for k in scenes.FIELDS:
+        o.set_field(k, sc[k])
+    o.set_params(sc["params"])
+    g = BoxSimulation(sc["bodies"], sc["substeps"], sc["sweeps"], False, sc["grid"])
+    g.load_state([sc[k] for k in scenes.FIELDS], sc["params"])
+    names = ["x", "y", "z", "u", "v", "w", "lx", "ly", "lz", "qx", "qy", "qz", "qw"]
+    for _ in range(5):
+        o.step(20)
+        g.step_and_wait(20)
+        got = g.state()
+        for name, a in zip(names, got):
+            assert np.array_equal(a.view(np.int32), o.field(name).view(np.int32)), name
+    assert g.touching_pairs() == o.touching_pairs()
+    o.close()
+    g.close()

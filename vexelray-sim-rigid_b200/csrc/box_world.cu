@@ -68,12 +68,15 @@ struct PairGen {
     int* pos;        // [cap] round-order position of touching pair t
     int4* pair;      // [cap] by position: first, second, point count, t
     float4* normal;  // [cap] by position: normal, winning axis
-    float4* pa;      // [cap * 4] by position: anchor on first, depth
-    float4* pb;      // [cap * 4] by position: anchor on second
-    float4* imp;     // [cap * 4] by position: normal impulse, tangential impulse
-    float4* impr;    // [cap * 4] by position: rolling impulse
-    float4* prepA;   // [cap * 4] by position, this half-substep: anchor on first in the world's frame, gap
-    float4* prepB;   // [cap * 4] by position, this half-substep: anchor on second in the world's frame, k normal
+    int* pstart;     // [cap] by position: where its points begin in the point arrays below
+    // The point arrays hold a pair's points at pstart[position] + point, packed: a pair of one point takes one
+    // entry, so the lanes of a warp, holding neighbouring positions, read neighbouring entries.
+    float4* pa;      // [cap * 4] by point: anchor on first, depth
+    float4* pb;      // [cap * 4] by point: anchor on second
+    float4* imp;     // [cap * 4] by point: normal impulse, tangential impulse
+    float4* impr;    // [cap * 4] by point: rolling impulse
+    float4* prepA;   // [cap * 4] by point, this half-substep: anchor on first in the world's frame, gap
+    float4* prepB;   // [cap * 4] by point, this half-substep: anchor on second in the world's frame, k normal
 };
 
 struct Counters {  // device-side counts of a step
@@ -154,6 +157,7 @@ struct vxr_box_world {
     int *colour = nullptr, *inc_count = nullptr, *inc_start = nullptr, *inc_fill = nullptr, *inc_list = nullptr;
     int *round_count = nullptr, *round_start = nullptr, *round_fill = nullptr;  // by (round, kind) bucket
     int* bucket_start = nullptr;
+    int *bucket_most = nullptr, *bucket_pstart = nullptr;  // by bucket: most points of a pair, first point
     Counters* counters = nullptr;
     Totals* totals = nullptr;
     Totals* host_totals = nullptr;  // pinned
@@ -452,10 +456,11 @@ __global__ void k_carry(const int* __restrict__ touching_n, const int* __restric
         for (int u = was.tstart[s]; u < was.tstart[s + 1]; u++)
             if (was.tb[u] == partner) old = u;
         int before = 0;
-        long op = 0;
+        long wbase = 0;
         if (old >= 0) {
-            op = was.pos[old];
+            const long op = was.pos[old];
             before = was.pair[op].z;
+            wbase = was.pstart[op];
         }
         const float4 h = half[s];
         const float smallest = fminf(h.x, fminf(h.y, h.z));
@@ -467,19 +472,19 @@ __global__ void k_carry(const int* __restrict__ touching_n, const int* __restric
                 float nearest = reach;
                 for (int o = 0; o < MOST_POINTS; o++) {
                     if (!(o < before)) continue;
-                    const float4 then = was.pa[op * MOST_POINTS + o];
+                    const float4 then = was.pa[wbase + o];
                     const float gap[3] = {anchor.x - then.x, anchor.y - then.y, anchor.z - then.z};
                     const float d2 = dot3(gap, gap);
                     if (d2 < nearest) {
                         nearest = d2;
-                        t0 = was.imp[op * MOST_POINTS + o];
-                        t1 = was.impr[op * MOST_POINTS + o];
+                        t0 = was.imp[wbase + o];
+                        t1 = was.impr[wbase + o];
                     }
                 }
             }
             if (point == 0 && count == 1 && before == 1) {
-                t0 = was.imp[op * MOST_POINTS];
-                t1 = was.impr[op * MOST_POINTS];
+                t0 = was.imp[wbase];
+                t1 = was.impr[wbase];
             }
             imp_t[(long)t * MOST_POINTS + point] = t0;
             impr_t[(long)t * MOST_POINTS + point] = t1;
@@ -580,10 +585,10 @@ __device__ __forceinline__ int pair_kind(float shapeA, float shapeB, int count) 
 }
 
 __global__ void k_round_count(const int* __restrict__ touching_n, const int* __restrict__ colour,
-                              int* __restrict__ round_count, Counters* counters, const int* __restrict__ ta,
-                              const int* __restrict__ tb, unsigned* __restrict__ body_colours,
-                              const int* __restrict__ tcand, const float4* __restrict__ head,
-                              const float4* __restrict__ half) {
+                              int* __restrict__ round_count, int* __restrict__ bucket_most, Counters* counters,
+                              const int* __restrict__ ta, const int* __restrict__ tb,
+                              unsigned* __restrict__ body_colours, const int* __restrict__ tcand,
+                              const float4* __restrict__ head, const float4* __restrict__ half) {
     const int total = *touching_n;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         int c = colour[t];
@@ -591,8 +596,10 @@ __global__ void k_round_count(const int* __restrict__ touching_n, const int* __r
             atomicCAS(&counters->status, ST_OK, ST_ROUNDS);
             c = MOST_ROUNDS;
         }
-        const int kind = pair_kind(half[ta[t]].w, half[tb[t]].w, (int)head[tcand[t]].w);
+        const int count = (int)head[tcand[t]].w;
+        const int kind = pair_kind(half[ta[t]].w, half[tb[t]].w, count);
         atomicAdd(&round_count[c * PAIR_KINDS + kind], 1);
+        atomicMax(&bucket_most[c * PAIR_KINDS + kind], min(max(count, 1), MOST_POINTS));
         if (c < MOST_ROUNDS) {
             atomicMax(&counters->rounds, c + 1);
             atomicOr(&body_colours[ta[t]], 1u << c);
@@ -607,7 +614,8 @@ __global__ void k_round_count(const int* __restrict__ touching_n, const int* __r
 // carried impulses next to it, so a solve phase reads one contiguous record per pair. Within a round the order is
 // the atomic fill's: the pairs of a round share no body, so their order does not change any result.
 __global__ void k_order(const int* __restrict__ touching_n, const int* __restrict__ colour,
-                        const int* __restrict__ bucket_start, int* __restrict__ round_fill, const int* __restrict__ ta,
+                        const int* __restrict__ bucket_start, const int* __restrict__ bucket_most,
+                        const int* __restrict__ bucket_pstart, int* __restrict__ round_fill, const int* __restrict__ ta,
                         const int* __restrict__ tcand, const Manifolds m, const float4* __restrict__ imp_t,
                         const float4* __restrict__ impr_t, PairGen now,
                         const unsigned* __restrict__ body_colours, const float4* __restrict__ half) {
@@ -617,8 +625,11 @@ __global__ void k_order(const int* __restrict__ touching_n, const int* __restric
         if (c < 0 || c > MOST_ROUNDS) c = MOST_ROUNDS;
         const int kind = pair_kind(half[ta[t]].w, half[now.tb[t]].w, (int)m.head[tcand[t]].w);
         const int bucket = c * PAIR_KINDS + kind;
-        const int p = bucket_start[bucket] + atomicAdd(&round_fill[bucket], 1);
+        const int rank = atomicAdd(&round_fill[bucket], 1);
+        const int p = bucket_start[bucket] + rank;
+        const long first = bucket_pstart[bucket] + (long)rank * bucket_most[bucket];
         now.pos[t] = p;
+        now.pstart[p] = (int)first;
         const int cd = tcand[t];
         const float4 head = m.head[cd];
         const int count = (int)head.w;
@@ -630,13 +641,26 @@ __global__ void k_order(const int* __restrict__ touching_n, const int* __restric
                                 (unsigned)__popc(ma) << 16 | (unsigned)__popc(mb) << 24;
         now.pair[p] = make_int4(a, b, count, (int)packed);
         now.normal[p] = make_float4(head.x, head.y, head.z, m.axis[cd]);
-        for (int i = 0; i < count; i++) {
-            now.pa[(long)p * MOST_POINTS + i] = m.pa[(long)cd * MOST_POINTS + i];
-            now.pb[(long)p * MOST_POINTS + i] = m.pb[(long)cd * MOST_POINTS + i];
-            now.imp[(long)p * MOST_POINTS + i] = imp_t[(long)t * MOST_POINTS + i];
-            now.impr[(long)p * MOST_POINTS + i] = impr_t[(long)t * MOST_POINTS + i];
+        for (int i = 0; i < count && i < MOST_POINTS; i++) {
+            now.pa[first + i] = m.pa[(long)cd * MOST_POINTS + i];
+            now.pb[first + i] = m.pb[(long)cd * MOST_POINTS + i];
+            now.imp[first + i] = imp_t[(long)t * MOST_POINTS + i];
+            now.impr[first + i] = impr_t[(long)t * MOST_POINTS + i];
         }
     }
+}
+
+// Where each bucket's points begin: its pairs take `most` entries each (every pair of a box-box bucket has the
+// same point count, and sphere pairs have one point, so the points are packed). One thread: BUCKETS entries.
+__global__ void k_bucket_points(const int* __restrict__ round_count, const int* __restrict__ bucket_most,
+                                int* __restrict__ bucket_pstart) {
+    if (threadIdx.x != 0) return;
+    int at = 0;
+    for (int b = 0; b < BUCKETS; b++) {
+        bucket_pstart[b] = at;
+        at += round_count[b] * bucket_most[b];
+    }
+    bucket_pstart[BUCKETS] = at;
 }
 
 // Where each round begins: its first bucket's start.
@@ -928,11 +952,14 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
 
 // Boxes.walls :357-416 over the listed bodies, each loaded afresh (its angular velocity from its angular
 // momentum, as the reference's walls kernel loads it).
+// The list's runs of 32 are dealt to the blocks in turn (as a round's pairs are), so the boxes, listed at its
+// end and the heavier work, spread over every SM.
 __device__ __forceinline__ void phase_walls(const SolveArgs& A, int sweep, bool reverse, int slot,
                                             unsigned* track) {
-    const int stride = gridDim.x * blockDim.x;
+    const int runs = gridDim.x * (blockDim.x >> 5);
+    const int run = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
     const int spheres = *(volatile int*)&A.wall_count[2 * slot], boxes = *(volatile int*)&A.wall_count[2 * slot + 1];
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < spheres + boxes; k += stride) {
+    for (int k = run * 32 + (threadIdx.x & 31); k < spheres + boxes; k += runs * 32) {
         const int s = A.wall_list[k < spheres ? k : A.n - 1 - (k - spheres)];
         Held box;
         load_held(box, A.b, s);
@@ -971,9 +998,10 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
     // The points in turn (backward: last to first). Past the first sweep of a half, each point's kept terms and
     // impulses are loaded while the point before it is solved: their addresses depend on the pair alone, and no
     // point writes another's records.
+    const long base = __ldg(&A.pairs.pstart[k]);
     float4 next_a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), next_b = next_a, next_imp = next_a;
     if (!fill && count > 0) {
-        const long at0 = k * MOST_POINTS + (reverse ? count - 1 : 0);
+        const long at0 = base + (reverse ? count - 1 : 0);
         next_a = __ldcg(&A.pairs.prepA[at0]);
         next_b = __ldcg(&A.pairs.prepB[at0]);
         next_imp = __ldcg(&A.pairs.imp[at0]);
@@ -981,7 +1009,7 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
     for (int order = 0; order < MOST_POINTS; order++) {
         const int slot = reverse ? MOST_POINTS - 1 - order : order;
         if (!(slot < count)) continue;
-        const long at = k * MOST_POINTS + slot;
+        const long at = base + slot;
         float rA[3], rB[3], gap, kn;
         float4 rec;
         if (fill) {
@@ -1011,7 +1039,7 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
             rec = next_imp;
             const int later = reverse ? slot - 1 : slot + 1;
             if (later >= 0 && later < count) {
-                const long at1 = k * MOST_POINTS + later;
+                const long at1 = base + later;
                 next_a = __ldcg(&A.pairs.prepA[at1]);
                 next_b = __ldcg(&A.pairs.prepB[at1]);
                 next_imp = __ldcg(&A.pairs.imp[at1]);
@@ -1322,7 +1350,7 @@ __global__ void k_features(const int* __restrict__ touching_n, const PairGen now
                 for (int j = 0; j < FEATURES; j++) f[j] = 0.0f;
                 continue;
             }
-            const size_t at = (size_t)k * MOST_POINTS + slot;
+            const size_t at = (size_t)now.pstart[k] + slot;
             float rA[3], rB[3], rel[3];
             point_of(A, B, n, now.pa[at], now.pb[at], rA, rB, rel);
             float gap = 0.0f;
@@ -1367,9 +1395,9 @@ __global__ void k_apply_learned(const int* __restrict__ touching_n, PairGen now,
         B.load(b.pose[rec.y], b.turn[rec.y], b.half[rec.y], b.vel[rec.y], b.mom[rec.y], b.inv[rec.y]);
         const float s = impulse_scale_of(P, scene_params, body_scene, rec.x, A.im + B.im);
         for (int slot = 0; slot < rec.z && slot < MOST_POINTS; slot++) {
-            const size_t at = (size_t)k * MOST_POINTS + slot;
-            const float ln = fmaxf(0.0f, pred[2 * at] * s);
-            const float lt = fmaxf(0.0f, pred[2 * at + 1] * s);
+            const size_t row = (size_t)k * MOST_POINTS + slot, at = (size_t)now.pstart[k] + slot;
+            const float ln = fmaxf(0.0f, pred[2 * row] * s);
+            const float lt = fmaxf(0.0f, pred[2 * row + 1] * s);
             const float4 old = now.imp[at];
             float dir[3] = {old.y, old.z, old.w};
             float len = sqrtf(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
@@ -1395,11 +1423,11 @@ __global__ void k_targets(const int* __restrict__ touching_n, const PairGen now,
         const int4 rec = now.pair[k];
         const float s = impulse_scale_of(P, scene_params, body_scene, rec.x, b.pose[rec.x].w + b.pose[rec.y].w);
         for (int slot = 0; slot < MOST_POINTS; slot++) {
-            const size_t at = (size_t)k * MOST_POINTS + slot;
+            const size_t row = (size_t)k * MOST_POINTS + slot;
             float4 imp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (slot < rec.z) imp = now.imp[at];
-            target[2 * at] = imp.x / s;
-            target[2 * at + 1] = sqrtf(imp.y * imp.y + imp.z * imp.z + imp.w * imp.w) / s;
+            if (slot < rec.z) imp = now.imp[(size_t)now.pstart[k] + slot];
+            target[2 * row] = imp.x / s;
+            target[2 * row + 1] = sqrtf(imp.y * imp.y + imp.z * imp.z + imp.w * imp.w) / s;
         }
     }
 }
@@ -1493,7 +1521,7 @@ __global__ void k_diag_contacts(const int* __restrict__ touching_n, const PairGe
         A.load(b.pose[rec.x], b.turn[rec.x], b.half[rec.x], b.vel[rec.x], b.mom[rec.x], b.inv[rec.x]);
         B.load(b.pose[rec.y], b.turn[rec.y], b.half[rec.y], b.vel[rec.y], b.mom[rec.y], b.inv[rec.y]);
         for (int slot = 0; slot < rec.z && slot < MOST_POINTS; slot++) {
-            const size_t at = (size_t)k * MOST_POINTS + slot;
+            const size_t at = (size_t)last.pstart[k] + slot;
             float rA[3], rB[3], rel[3];
             point_of(A, B, n, last.pa[at], last.pb[at], rA, rB, rel);
             float gap = 0.0f;
@@ -1684,16 +1712,21 @@ int enqueue_step(vxr_box_world* w) {
             if (rc) return rc;
         }
         VXR_CUDA(cudaMemsetAsync(w->round_count, 0, sizeof(int) * BUCKETS, st));
+        VXR_CUDA(cudaMemsetAsync(w->bucket_most, 0, sizeof(int) * BUCKETS, st));
         VXR_CUDA(cudaMemsetAsync(w->round_fill, 0, sizeof(int) * BUCKETS, st));
         VXR_CUDA(cudaMemsetAsync(w->body_colours, 0, sizeof(unsigned) * n, st));
-        k_round_count<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_count, w->counters, w->ta,
+        k_round_count<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_count, w->bucket_most,
+                                                  w->counters, w->ta,
                                                   now.tb, w->body_colours, w->tcand, w->man.head, w->b.half);
         exclusive_scan(w->round_count, w->bucket_start, BUCKETS, w->scan_tiles, st);
         k_round_starts<<<1, 64, 0, st>>>(w->bucket_start, w->round_start);
-        k_order<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->bucket_start, w->round_fill, w->ta,
+        k_bucket_points<<<1, 32, 0, st>>>(w->round_count, w->bucket_most, w->bucket_pstart);
+        k_order<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->bucket_start, w->bucket_most,
+                                            w->bucket_pstart, w->round_fill, w->ta,
                                             w->tcand, w->man, w->imp_t, w->impr_t, now,
                                             w->body_colours, w->b.half);
-        LAUNCHED(1 + 3 + 1 + 1 + 1 + 3 + 1 + 1);  // inc count, scan, inc fill, colour, round count, scan, starts, order
+        LAUNCHED(1 + 3 + 1 + 1 + 1 + 3 + 1 + 1 + 1);  // inc count, scan, inc fill, colour, round count, scan,
+                                                    // starts, bucket points, order
         if (w->learn_mode > 0) {
             const int* tn = now.tstart + n;
             k_features<<<tblocks, THREADS, 0, st>>>(tn, now, w->b, w->inc_count, w->params, w->scene_params,
@@ -1966,6 +1999,8 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     rc |= alloc(w, &w->round_count, BUCKETS);
     rc |= alloc(w, &w->round_start, MOST_ROUNDS + 2);
     rc |= alloc(w, &w->bucket_start, BUCKETS + 1);
+    rc |= alloc(w, &w->bucket_most, BUCKETS);
+    rc |= alloc(w, &w->bucket_pstart, BUCKETS + 1);
     rc |= alloc(w, &w->wall_list, n);
     rc |= alloc(w, &w->wall_count, 4 * (size_t)w->substeps);
     rc |= alloc(w, &w->version, n);
@@ -2004,6 +2039,7 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
             rc |= alloc(w, &p.pos, w->cap);
             rc |= alloc(w, &p.pair, w->cap);
             rc |= alloc(w, &p.normal, w->cap);
+            rc |= alloc(w, &p.pstart, w->cap);
             rc |= alloc(w, &p.pa, (size_t)w->cap * MOST_POINTS);
             rc |= alloc(w, &p.pb, (size_t)w->cap * MOST_POINTS);
             rc |= alloc(w, &p.imp, (size_t)w->cap * MOST_POINTS);
@@ -2477,12 +2513,13 @@ int32_t vxr_box_touching(vxr_box_world* w, int32_t* first, int32_t* second, int3
     if (!first && !second && !points && !manifold && !impulses) return P;
     if (P > capacity) return -VXR_ECAPACITY;
     if (P == 0) return 0;
-    std::vector<int> pos(P);
+    std::vector<int> pos(P), pstart(P);
     std::vector<int4> pair(P);
     std::vector<float4> normal(P), pa((size_t)P * MOST_POINTS), pb((size_t)P * MOST_POINTS),
         imp((size_t)P * MOST_POINTS), impr((size_t)P * MOST_POINTS);
     VXR_CUDA(cudaMemcpy(pos.data(), g.pos, sizeof(int) * P, cudaMemcpyDeviceToHost));
     VXR_CUDA(cudaMemcpy(pair.data(), g.pair, sizeof(int4) * P, cudaMemcpyDeviceToHost));
+    VXR_CUDA(cudaMemcpy(pstart.data(), g.pstart, sizeof(int) * P, cudaMemcpyDeviceToHost));
     VXR_CUDA(cudaMemcpy(normal.data(), g.normal, sizeof(float4) * P, cudaMemcpyDeviceToHost));
     VXR_CUDA(cudaMemcpy(pa.data(), g.pa, sizeof(float4) * pa.size(), cudaMemcpyDeviceToHost));
     VXR_CUDA(cudaMemcpy(pb.data(), g.pb, sizeof(float4) * pb.size(), cudaMemcpyDeviceToHost));
@@ -2504,7 +2541,7 @@ int32_t vxr_box_touching(vxr_box_world* w, int32_t* first, int32_t* second, int3
             m[4] = normal[p].w;
             for (int i = 0; i < cnt && i < MOST_POINTS; i++) {
                 float* q = m + M_POINTS + i * M_POINT_WORDS;
-                const float4 a = pa[(size_t)p * MOST_POINTS + i], b = pb[(size_t)p * MOST_POINTS + i];
+                const float4 a = pa[(size_t)pstart[p] + i], b = pb[(size_t)pstart[p] + i];
                 q[0] = a.x;
                 q[1] = a.y;
                 q[2] = a.z;
@@ -2518,7 +2555,7 @@ int32_t vxr_box_touching(vxr_box_world* w, int32_t* first, int32_t* second, int3
             float* r = impulses + (size_t)t * 28;
             std::memset(r, 0, sizeof(float) * 28);
             for (int i = 0; i < cnt && i < MOST_POINTS; i++) {
-                const float4 a = imp[(size_t)p * MOST_POINTS + i], b = impr[(size_t)p * MOST_POINTS + i];
+                const float4 a = imp[(size_t)pstart[p] + i], b = impr[(size_t)pstart[p] + i];
                 r[7 * i + 0] = a.x;
                 r[7 * i + 1] = a.y;
                 r[7 * i + 2] = a.z;
