@@ -113,22 +113,33 @@ def dist_setup():
     return world, rank, local, pg
 
 
-def all_max(pg, value: float) -> float:
-    if pg is None:
-        return value
+def _reduce(pg, value: float, op) -> float:
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    device = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=op)
     return float(t.item())
+
+
+def all_max(pg, value: float) -> float:
+    """The largest of the ranks' values (a time: the job is as slow as its slowest rank)."""
+    return value if pg is None else _reduce(pg, value, pg.ReduceOp.MAX)
 
 
 def all_sum(pg, value: float) -> float:
-    if pg is None:
-        return value
-    import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.SUM)
-    return float(t.item())
+    return value if pg is None else _reduce(pg, value, pg.ReduceOp.SUM)
+
+
+def whole_job_rate(pg, units: float, steps: int, ms: float) -> float:
+    """Units all ranks stepped, per second of the slowest rank's device time: this rank stepped `units` bodies
+    `steps` times in `ms` milliseconds."""
+    return all_sum(pg, float(units)) * steps / (all_max(pg, ms) / 1e3)
+
+
+def shard_scenes(scenes: int, world_size: int, rank: int) -> list:
+    """This rank's scenes of a batch: scene k to rank k mod N. No data-path collective: the scenes are
+    independent."""
+    return [k for k in range(scenes) if k % world_size == rank]
 
 
 def barrier(pg):
@@ -137,6 +148,13 @@ def barrier(pg):
 
 
 ITERATION_CAP = 64
+
+
+# DRAM traffic of one k_solve launch of the large scene late in the drop, from an ncu capture (one pass:
+# dram__bytes_read.sum + dram__bytes_write.sum) of the step after step 480, the state saved at step 480 and loaded.
+# A late launch is where the pair records outgrow L2; that launch's own algorithmic bytes are given beside it.
+LATE_SOLVE_TRAFFIC = {"step": 481, "dram_bytes": 5.17e9, "dram_read_bytes": 3.76e9, "dram_write_bytes": 1.41e9,
+                      "algorithmic_bytes": 7.85e9, "ms": 18.85, "source": "ncu, one launch"}
 
 
 def make_world(scene, device, max_pairs=0, schedule=0, solve_blocks_per_sm=0):
@@ -412,7 +430,7 @@ def run_batched(args):
     from vxr import autotune, scenes
     from vxr.box_simulation import BatchSimulation
     full = scenes.batched(seed=1)
-    mine = [k for k in range(full["scenes"]) if k % world_size == rank]  # scenes shared out across the ranks
+    mine = shard_scenes(full["scenes"], world_size, rank)  # scenes shared out across the ranks
     b = batch_subset(full, mine) if world_size > 1 else full
     tune = autotune.tune_batch(b, local)
     grids = autotune.scaled_grids(b, tune["cell_scale"])
@@ -667,6 +685,8 @@ def main():
     ap.add_argument("--no-iterations", action="store_true")
     ap.add_argument("--no-judge", action="store_true", help="skip the judged run (penetration, energy)")
     ap.add_argument("--schedule", type=int, default=0, help="solve schedule: 0 barrier phases, 1 per-body dependencies")
+    ap.add_argument("--save-state", default="", help="large scene: save the state after the warm-up steps and exit")
+    ap.add_argument("--load-state", default="", help="large scene: start from a state saved by --save-state")
     ap.add_argument("--solve-blocks-per-sm", type=int, default=0, help="solve blocks an SM (0: the library's choice)")
     ap.add_argument("--max-pairs", type=int, default=0, help="pair capacity of the world (0: 32 a body)")
     ap.add_argument("--workload", default="large-mixed",
@@ -693,17 +713,29 @@ def main():
     else:  # a smaller case of the same scene: the same body density over a smaller footprint
         scene = scenes.sub_volume(BODIES, args.bodies / BODIES, seed=1 + rank)
     w = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm)
+    if args.load_state:  # a state saved by --save-state: the 13 moving fields; shapes, masses and params the scene's
+        z = np.load(args.load_state)
+        moving = [z[f"arr_{i}"] for i in range(13)]
+        w.load_state(moving + [scene["im"], scene["hx"], scene["hy"], scene["hz"], scene["shape"]], scene["params"])
     stream = torch.cuda.ExternalStream(w.stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
     # warm-up: steps 0..W-1
     w.step_async(args.warmup)
     w.sync()
+    if args.save_state:  # the state after the warm-up steps, for a later run (or a profile of one late step)
+        np.savez(args.save_state, *w.state())
+        if rank == 0:
+            print(json.dumps({"saved": args.save_state, "after_steps": args.warmup, "touching": w.last().touching}))
+        w.close()
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
     launches0 = w.launches()
     w.profile(True)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    activity = []
+    sampled = []
     barrier(pg)
     torch.cuda.synchronize()
     with Clocks(local) as clocks:
@@ -716,6 +748,11 @@ def main():
                 ends[k].record(stream)
             if k % 20 == 19:
                 rep = w.sync()
+                # the solve's algorithmic bytes, sampled every 20th step at the sync the loop makes anyway
+                a = w.activity()
+                sampled.append(algorithmic_solve_bytes(scene["bodies"], scene["substeps"], scene["sweeps"],
+                                                       a["touching"], a["points"], a["bodies_active"],
+                                                       a["wall_records"]))
         rep = w.sync()
     torch.cuda.synchronize()
     barrier(pg)
@@ -735,11 +772,15 @@ def main():
         windows.append({"steps": f"{args.warmup + lo}..{args.warmup + hi - 1}", "ms_per_step": ms / (hi - lo),
                         "value": scene["bodies"] * (hi - lo) / (ms / 1e3)})
 
-    # roofline of the solve kernel: bytes per launch from the last step's activity, time per launch from events
+    # roofline of the solve kernel: algorithmic bytes per launch averaged over the timed steps (sampled every 20th),
+    # over its mean launch time from the per-phase events
     hbm, which = peaks()
     solve_ms = phases[3] / args.steps
-    b_solve = algorithmic_solve_bytes(scene["bodies"], scene["substeps"], scene["sweeps"], activity["touching"],
-                                      activity["points"], activity["bodies_active"], activity["wall_records"])
+    if not sampled:
+        sampled.append(algorithmic_solve_bytes(scene["bodies"], scene["substeps"], scene["sweeps"],
+                                               activity["touching"], activity["points"], activity["bodies_active"],
+                                               activity["wall_records"]))
+    b_solve = float(np.mean(sampled))
     achieved = b_solve / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
     pic = picture_timing(w, 1, scene["bodies"], scene["walls"], local, squash=0.0,
                          cpu=rank == 0 and not args.no_cpu)
@@ -818,8 +859,10 @@ def main():
         "last_step": {"touching": rep.touching, "points": rep.points, "rounds": rep.rounds,
                       "unplaced": rep.unplaced, "unlisted": rep.unlisted, **activity},
         "roofline": {"bound": "hbm", "kernel": "k_solve", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None, "peak_source": which,
-                     "bytes_per_launch": b_solve, "ms_per_launch": solve_ms},
+                     "frac": achieved / hbm, "traffic": LATE_SOLVE_TRAFFIC["dram_bytes"] if args.bodies == BODIES
+                     else None, "peak_source": which, "bytes_per_launch": b_solve, "ms_per_launch": solve_ms,
+                     "bytes_per_launch_sampled": "every 20th timed step",
+                     "traffic_launch": LATE_SOLVE_TRAFFIC if args.bodies == BODIES else None},
         "gpu_launches": int(launches),
         "iterations_to_residual": iters,
         "judged_500_steps": judged,

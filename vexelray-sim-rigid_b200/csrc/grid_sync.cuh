@@ -1,7 +1,7 @@
 // A grid-wide barrier for a cooperative (all blocks co-resident) launch, with a bounded wait.
 //
-// Arrival is one atomic add per block on a counter that only grows during the kernel (zeroed before the
-// launch): barrier number e is passed once the counter reaches (e + 1) x blocks, so no block resets anything
+// Arrival is one release-ordered add per block on a counter that only grows during the kernel (zeroed before the
+// launch), and the wait an acquire load of it: barrier number e is passed once the counter reaches (e + 1) x blocks, so no block resets anything
 // and no second word is needed. Every wait gives up after a time limit (the device's global nanosecond timer):
 // the waiter then raises the abort word and the status word, and every block leaves at its next barrier, so a
 // barrier that can never complete ends the kernel with an error the host reads, not a hung GPU.
@@ -40,8 +40,9 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& b, unsigned int& ep
     if (threadIdx.x == 0) {
         leave = 0;
         const unsigned int target = (epoch + 1) * gridDim.x;
-        __threadfence();
-        atomicAdd(b.count, 1u);
+        // Arrival as a release at GPU scope: the block's writes (ordered before it by the block barrier) are
+        // visible to every block whose acquire load then sees the count. No separate full fence is needed.
+        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(b.count), "r"(1u) : "memory");
         if (load_acquire(b.count) < target) {
             const unsigned long long start = global_ns();
             unsigned int spins = 0;
@@ -54,7 +55,6 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& b, unsigned int& ep
                 }
             }
         }
-        __threadfence();
         if (*(volatile int*)b.abort) leave = 1;
     }
     epoch++;
