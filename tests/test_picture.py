@@ -335,3 +335,24 @@ def test_gpu_eye_inside_a_sphere_and_spheres_behind():
     got = gpu_picture(P.SPHERES, s.ravel(), n, cam, 96, 96)
     want = OP.picture(OP.SPHERES, s.ravel(), P.push_words(cam, n), 96, 96)
     np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_gpu_a_super_tile_past_its_list_tests_every_body():
+    """17,000 small spheres strung along the view's axis: the super-tiles at the picture's centre keep more bodies
+    than their lists hold and fall back to every body, the others use their lists; the picture is the oracle's."""
+    n = 17000
+    rng = np.random.default_rng(5)
+    s = np.zeros((n, 40), np.float32)
+    z = 1.0 + 0.002 * np.arange(n)
+    s[:, 0] = 0.5 + rng.uniform(-0.002, 0.002, n) * z
+    s[:, 1] = 0.5 + rng.uniform(-0.002, 0.002, n) * z
+    s[:, 2] = z
+    s[:, 4:7] = s[:, 0:3]
+    s[:, 3] = 0.003
+    s[:, 32:36] = s[:, 36:40] = (0, 0, 0, 1)
+    cam = P.camera((0.5, 0.5, 0.0), (1, 0, 0), (0, 1, 0), (0, 0, 1), 1.0, 0.0, (1, 1, 40), 0.0)
+    got = gpu_picture(P.SPHERES, s.ravel(), n, cam, 192, 192)
+    want = OP.picture(OP.SPHERES, s.ravel(), P.push_words(cam, n), 192, 192)
+    np.testing.assert_array_equal(got, want)
+    assert (np.abs(got - OP.picture(OP.SPHERES, s.ravel(), P.push_words(cam, 0), 192, 192)) > 0).any()

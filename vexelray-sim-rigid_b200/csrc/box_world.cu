@@ -162,6 +162,7 @@ struct vxr_box_world {
     Totals* totals = nullptr;
     Totals* host_totals = nullptr;  // pinned
     float* pinned = nullptr;        // pinned staging for state transfers
+    float* state13 = nullptr;       // [13 n] the state split into fields, for vxr_box_state
     size_t pinned_bytes = 0;
     std::vector<void*> allocations;
     long long launches = 0;  // kernels this world has launched
@@ -1849,20 +1850,14 @@ int upload4(vxr_box_world* w, float4* dst, const float* a, const float* b, const
     return VXR_OK;
 }
 
-int download4(vxr_box_world* w, const float4* src, float* a, float* b, float* c, float* d) {
-    const int n = w->n;
-    int rc = ensure_pinned(w, sizeof(float4) * (size_t)n);
-    if (rc) return rc;
-    VXR_CUDA(cudaMemcpyAsync(w->pinned, src, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost, w->stream));
-    VXR_CUDA(cudaStreamSynchronize(w->stream));
-    const float* p = w->pinned;
-    for (int s = 0; s < n; s++) {
-        if (a) a[s] = p[4 * s + 0];
-        if (b) b[s] = p[4 * s + 1];
-        if (c) c[s] = p[4 * s + 2];
-        if (d) d[s] = p[4 * s + 3];
+// x y z u v w lx ly lz qx qy qz qw, field after field.
+__global__ void k_state13(int n, const Bodies b, float* __restrict__ out) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const float4 p = b.pose[s], v = b.vel[s], l = b.mom[s], q = b.turn[s];
+        const float f[13] = {p.x, p.y, p.z, v.x, v.y, v.z, l.x, l.y, l.z, q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int k = 0; k < 13; k++) out[(size_t)k * n + s] = f[k];
     }
-    return VXR_OK;
 }
 
 // Boxes.params / softness (Boxes.java:212-251), computed in double and rounded to f32 bits.
@@ -2486,12 +2481,18 @@ void* vxr_box_stream(vxr_box_world* w) { return w ? (void*)w->stream : nullptr; 
 int32_t vxr_box_state(vxr_box_world* w, float* const* out) {
     if (!w || !out) return VXR_EINVAL;
     cudaSetDevice(w->device);
-    int rc = 0;
-    rc |= download4(w, w->b.pose, out[0], out[1], out[2], nullptr);
-    rc |= download4(w, w->b.vel, out[3], out[4], out[5], nullptr);
-    rc |= download4(w, w->b.mom, out[6], out[7], out[8], nullptr);
-    rc |= download4(w, w->b.turn, out[9], out[10], out[11], out[12]);
-    return rc ? VXR_ECUDA : VXR_OK;
+    // the 13 fields split out of the float4 arrays on the device, then copied straight into the caller's arrays
+    // (at the copy engine's full rate when they are pinned), one synchronisation for all
+    if (!w->state13 && alloc(w, &w->state13, (size_t)13 * w->n)) return VXR_ECUDA;
+    const int n = w->n;
+    k_state13<<<blocks_for(n, THREADS), THREADS, 0, w->stream>>>(n, w->b, w->state13);
+    w->launches += 1;
+    for (int f = 0; f < 13; f++)
+        if (out[f])
+            VXR_CUDA(cudaMemcpyAsync(out[f], w->state13 + (size_t)f * n, sizeof(float) * (size_t)n,
+                                     cudaMemcpyDeviceToHost, w->stream));
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    return VXR_OK;
 }
 
 int32_t vxr_box_read_shown(vxr_box_world* w, float* out) {

@@ -325,7 +325,7 @@ __device__ __forceinline__ void box_colour(const Cam& c, const float* d, BoxHit&
 // The side planes of the tile's rays, through the eye, inward: from the f32 corner rays, in doubles, so that the
 // planes hold those rays exactly; a plane whose corner rays coincide (a tile one pixel wide or high) is left out.
 __device__ void tile_planes(const Cam& c, int i0, int j0, int i1, int j1, float (*plane)[4]) {
-    const int q = threadIdx.y * TILE + threadIdx.x;
+    const int q = threadIdx.y * blockDim.x + threadIdx.x;
     if (q >= 4) return;
     float f[4][3];
     ray_of(c, i0, j0, f[0]);
@@ -344,15 +344,79 @@ __device__ void tile_planes(const Cam& c, int i0, int j0, int i1, int j1, float 
     plane[q][3] = len > 0.0 ? 1.0f : 0.0f;
 }
 
+// Whether a body's bounding sphere can meet a ray inside the four planes: within R plus a slack of each plane's
+// inside. Rounding in the pixels' f32 tests moves a ray's reach by far less than the slack (1e-6 relative at most).
+__device__ __forceinline__ bool may_meet(float4 p, float R, const float (*plane)[4]) {
+    const float len = sqrtf(p.x * p.x + p.y * p.y + p.z * p.z);
+    const float slack = R + 1e-5f * (R + len + len * (len / fmaxf(R, 1e-20f)));
+    bool keep = true;
+    for (int q = 0; q < 4; q++) {
+        if (plane[q][3] == 0.0f) continue;
+        const float inside_by = -(p.x * plane[q][0] + p.y * plane[q][1] + p.z * plane[q][2]);
+        if (inside_by < -slack) keep = false;
+    }
+    return keep;
+}
+
+// Block-wide ordered compaction: this thread's place among the kept of its block's chunk (warp by warp, lane by
+// lane), and the chunk's kept count. Every thread of the block calls it; `tid` is its flat index in a block of
+// THREADS (whatever the block's shape).
+__device__ __forceinline__ int kept_before(bool keep, int tid, int* s_warp, int& total) {
+    const int lane = tid & 31, warp = tid >> 5;
+    const unsigned vote = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) s_warp[warp] = __popc(vote);
+    __syncthreads();
+    int before = 0;
+    total = 0;
+    for (int w = 0; w < THREADS / 32; w++) {
+        const int n = s_warp[w];
+        before += w < warp ? n : 0;
+        total += n;
+    }
+    return before + __popc(vote & ((1u << lane) - 1u));
+}
+
+// Scenes of many bodies: one block a super-tile of SUPER x SUPER pixels keeps, in ascending order, the bodies that
+// may meet a ray of it; its tiles then test only those. A super-tile's rays lie inside its corner rays' planes and
+// hold every ray of its tiles, so a body left out here is one every tile of it would leave out. More than `cap`
+// kept: the list is marked full and its tiles test every body.
+constexpr int SUPER = 64, SUPER_FROM = 2048, SUPER_CAP = 16384;
+
+__global__ void __launch_bounds__(THREADS) k_picture_super(Cam c, const float4* __restrict__ pre,
+                                                           const float* __restrict__ reach, int* __restrict__ list,
+                                                           int* __restrict__ list_n, int cap) {
+    __shared__ float s_plane[4][4];
+    __shared__ int s_warp[THREADS / 32];
+    const int supers_x = (c.width + SUPER - 1) / SUPER;
+    const int st = blockIdx.x;
+    const int i0 = (st % supers_x) * SUPER, j0 = (st / supers_x) * SUPER;
+    const int i1 = min(i0 + SUPER - 1, c.width - 1), j1 = min(j0 + SUPER - 1, c.height - 1);
+    tile_planes(c, i0, j0, i1, j1, s_plane);
+    __syncthreads();
+    int* mine = list + (size_t)st * cap;
+    int listed = 0;
+    for (int base = 0; base < c.count; base += THREADS) {
+        const int k = base + threadIdx.x;
+        const bool keep = k < c.count && may_meet(pre[k], reach[k], s_plane);
+        int total;
+        const int at = listed + kept_before(keep, threadIdx.x, s_warp, total);
+        if (keep && at < cap) mine[at] = k;
+        listed += total;
+        __syncthreads();  // s_warp is written again by the next chunk
+    }
+    if (threadIdx.x == 0) list_n[st] = listed;
+}
+
 template <int SHAPE>
 __global__ void __launch_bounds__(THREADS) k_picture(Cam c, const float* __restrict__ shown,
                                                      const float4* __restrict__ pre, const float* __restrict__ reach,
-                                                     float* __restrict__ out) {
+                                                     const int* __restrict__ list, const int* __restrict__ list_n,
+                                                     int cap, float* __restrict__ out) {
     __shared__ float4 s_pre[LIST];
     __shared__ int s_body[LIST];
     __shared__ float s_plane[4][4];
     __shared__ int s_warp[THREADS / 32];
-    const int tid = threadIdx.y * TILE + threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.y * TILE + threadIdx.x;
     const int i0 = blockIdx.x * TILE, j0 = blockIdx.y * TILE;
     const int i1 = min(i0 + TILE - 1, c.width - 1), j1 = min(j0 + TILE - 1, c.height - 1);
     const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
@@ -360,50 +424,46 @@ __global__ void __launch_bounds__(THREADS) k_picture(Cam c, const float* __restr
     float d[3];
     ray_of(c, min(i, c.width - 1), min(j, c.height - 1), d);
     tile_planes(c, i0, j0, i1, j1, s_plane);
+    // the bodies to go through: the super-tile's list, or every body (no lists, or the list overflowed)
+    const int* from = nullptr;
+    int m = c.count;
+    if (list) {
+        const int st = (j0 / SUPER) * ((c.width + SUPER - 1) / SUPER) + i0 / SUPER;
+        const int kept = list_n[st];
+        if (kept <= cap) {
+            from = list + (size_t)st * cap;
+            m = kept;
+        }
+    }
     __syncthreads();
     SphereHit sh;
     BoxHit bh;
     int listed = 0;
-    for (int base = 0; base < c.count; base += THREADS) {
-        const int k = base + tid;
+    for (int base = 0; base < m; base += THREADS) {
+        const int e = base + tid;
         bool keep = false;
+        int k = 0;
         float4 p = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (k < c.count) {
+        if (e < m) {
+            k = from ? from[e] : e;
             p = pre[k];
-            const float R = reach[k];
-            const float len = sqrtf(p.x * p.x + p.y * p.y + p.z * p.z);
-            // rounding in the pixels' f32 tests moves a ray's reach by far less than this (1e-6 relative at most)
-            const float slack = R + 1e-5f * (R + len + len * (len / fmaxf(R, 1e-20f)));
-            keep = true;
-            for (int q = 0; q < 4; q++) {
-                if (s_plane[q][3] == 0.0f) continue;
-                const float inside_by = -(p.x * s_plane[q][0] + p.y * s_plane[q][1] + p.z * s_plane[q][2]);
-                if (inside_by < -slack) keep = false;
-            }
+            keep = may_meet(p, reach[k], s_plane);
         }
-        const unsigned vote = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) s_warp[warp] = __popc(vote);
-        __syncthreads();
-        int before = 0, total = 0;
-        for (int w = 0; w < THREADS / 32; w++) {
-            const int n = s_warp[w];
-            before += w < warp ? n : 0;
-            total += n;
-        }
+        int total;
+        const int at = listed + kept_before(keep, tid, s_warp, total);
         if (keep) {
-            const int at = listed + before + __popc(vote & ((1u << lane) - 1u));
             s_pre[at] = p;
             s_body[at] = k;
         }
         listed += total;
         __syncthreads();
-        if (listed > LIST - THREADS || base + THREADS >= c.count) {
+        if (listed > LIST - THREADS || base + THREADS >= m) {
             if (inside) {
                 for (int e = 0; e < listed; e++) {
-                    const float4 q = s_pre[e];
-                    const float o[3] = {q.x, q.y, q.z};
+                    const float4 v = s_pre[e];
+                    const float o[3] = {v.x, v.y, v.z};
                     const float half = dot3(o, d);
-                    const float disc = half * half - q.w;
+                    const float disc = half * half - v.w;
                     if (!(disc > 0.0f)) continue;
                     const float root = sqrtf(disc);
                     const float best = SHAPE == VXR_RING_SPHERES ? sh.best : bh.best;
@@ -471,26 +531,36 @@ int32_t vxr_picture(int32_t shape, const float* shown, int32_t count, const vxr_
     if (set_light() != VXR_OK) return VXR_ECUDA;
     const Cam c = cam_of(camera, count, width, height);
     cudaStream_t st = (cudaStream_t)stream;
+    const int supers = ((width + SUPER - 1) / SUPER) * ((height + SUPER - 1) / SUPER);
+    const bool use_supers = count >= SUPER_FROM;
+    const int cap = std::min(count, SUPER_CAP);
     float4* pre = nullptr;
     float* reach = nullptr;
+    int *list = nullptr, *list_n = nullptr;
     if (count > 0) {
         // a frame's scratch from the stream-ordered pool: no synchronisation, nothing shared between streams
+        size_t bytes = (size_t)count * (sizeof(float4) + sizeof(float));
+        if (use_supers) bytes += (size_t)supers * (cap + 1) * sizeof(int);
         void* scratch = nullptr;
-        if (cudaMallocAsync(&scratch, (size_t)count * (sizeof(float4) + sizeof(float)), st) != cudaSuccess)
-            return VXR_ECUDA;
+        if (cudaMallocAsync(&scratch, bytes, st) != cudaSuccess) return VXR_ECUDA;
         pre = (float4*)scratch;
         reach = (float*)(pre + count);
+        if (use_supers) {
+            list_n = (int*)(reach + count);
+            list = list_n + supers;
+        }
         const int blocks = (count + 255) / 256;
         if (shape == VXR_RING_SPHERES)
             k_picture_bodies<VXR_RING_SPHERES><<<blocks, 256, 0, st>>>(c, shown, pre, reach);
         else
             k_picture_bodies<VXR_RING_BOXES><<<blocks, 256, 0, st>>>(c, shown, pre, reach);
+        if (use_supers) k_picture_super<<<supers, THREADS, 0, st>>>(c, pre, reach, list, list_n, cap);
     }
     const dim3 block(TILE, TILE), grid((width + TILE - 1) / TILE, (height + TILE - 1) / TILE);
     if (shape == VXR_RING_SPHERES)
-        k_picture<VXR_RING_SPHERES><<<grid, block, 0, st>>>(c, shown, pre, reach, rgb);
+        k_picture<VXR_RING_SPHERES><<<grid, block, 0, st>>>(c, shown, pre, reach, list, list_n, cap, rgb);
     else
-        k_picture<VXR_RING_BOXES><<<grid, block, 0, st>>>(c, shown, pre, reach, rgb);
+        k_picture<VXR_RING_BOXES><<<grid, block, 0, st>>>(c, shown, pre, reach, list, list_n, cap, rgb);
     if (pre && cudaFreeAsync(pre, st) != cudaSuccess) return VXR_ECUDA;
     return cudaGetLastError() == cudaSuccess ? VXR_OK : VXR_ECUDA;
 }

@@ -168,9 +168,14 @@ class BoxSimulation:
     def last(self) -> Report:
         return self._last
 
-    def state(self) -> list[np.ndarray]:
-        """x y z u v w lx ly lz qx qy qz qw, read back."""
-        out = [np.empty(self.n, dtype=np.float32) for _ in STATE_FIELDS]
+    def state(self, out=None) -> list[np.ndarray]:
+        """x y z u v w lx ly lz qx qy qz qw, read back; into `out` (13 float32 arrays of n, e.g. in pinned memory)
+        when given."""
+        if out is None:
+            out = [np.empty(self.n, dtype=np.float32) for _ in STATE_FIELDS]
+        elif len(out) != len(STATE_FIELDS) or any(a.dtype != np.float32 or a.shape != (self.n,) or
+                                                   not a.flags.c_contiguous for a in out):
+            raise ValueError(f"out holds {len(STATE_FIELDS)} contiguous float32 arrays of {self.n}")
         self._check(self.L.vxr_box_state(self.h, ptr_array(out)))
         return out
 
