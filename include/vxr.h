@@ -171,7 +171,8 @@ int32_t vxr_box_measure(vxr_box_world* world, int32_t residual, int32_t cold_sta
  * solve and the relax sweeps each substep ran. Returns the count of residuals, or minus a status. */
 int32_t vxr_box_residuals(vxr_box_world* world, float* out, int32_t capacity, int32_t* used);
 
-/* Kernels this world has launched since creation (each step launches the same number). */
+/* Kernels this world's steps have launched since creation (each step launches the same number; reading the
+ * state back is not counted). */
 long long vxr_box_launches(vxr_box_world* world);
 
 /* Per-phase device time: with enable = 1 each following step records CUDA events on the world's stream around
@@ -408,7 +409,8 @@ typedef struct {
 } vxr_sphere_diag;
 int32_t vxr_sphere_diagnostics(vxr_sphere_world* world, vxr_sphere_diag* out);
 
-/* Blocks the world's kernel runs on, and kernels it has launched. */
+/* Blocks the world's kernel runs on, and kernels its steps have launched (reading the state back is not
+ * counted). */
 int32_t vxr_sphere_blocks(const vxr_sphere_world* world);
 int64_t vxr_sphere_launches(const vxr_sphere_world* world);
 

@@ -12,7 +12,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "vxr.h")).read()
+    with open(os.path.join(ROOT, "include", "vxr.h")) as f:
+        text = f.read()
     return sorted(set(re.findall(r"\b(vxr_[a-z0-9_]+)\s*\(", text)))
 
 

@@ -2485,8 +2485,7 @@ int32_t vxr_box_state(vxr_box_world* w, float* const* out) {
     // (at the copy engine's full rate when they are pinned), one synchronisation for all
     if (!w->state13 && alloc(w, &w->state13, (size_t)13 * w->n)) return VXR_ECUDA;
     const int n = w->n;
-    k_state13<<<blocks_for(n, THREADS), THREADS, 0, w->stream>>>(n, w->b, w->state13);
-    w->launches += 1;
+    k_state13<<<blocks_for(n, THREADS), THREADS, 0, w->stream>>>(n, w->b, w->state13);  // not a step's launch
     for (int f = 0; f < 13; f++)
         if (out[f])
             VXR_CUDA(cudaMemcpyAsync(out[f], w->state13 + (size_t)f * n, sizeof(float) * (size_t)n,

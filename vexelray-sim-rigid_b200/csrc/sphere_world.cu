@@ -1126,6 +1126,7 @@ struct vxr_sphere_world {
     Counts* host_counts = nullptr;  // pinned
     int *opening = nullptr, *enough = nullptr;
     float* pinned = nullptr;
+    float* state9 = nullptr;  // [9 n] the state split into fields, for vxr_sphere_state
     size_t pinned_bytes = 0;
     std::vector<void*> allocations;
     long long launches = 0;
@@ -1562,6 +1563,17 @@ int32_t vxr_sphere_step(vxr_sphere_world* w, int32_t steps, vxr_sphere_report* r
 
 void* vxr_sphere_stream(vxr_sphere_world* w) { return w ? (void*)w->stream : nullptr; }
 
+// x y z u v w ax ay az, field after field.
+__global__ void k_state9(int n, const float4* __restrict__ pos, const float4* __restrict__ vel,
+                         const float4* __restrict__ spin, float* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 p = pos[s], v = vel[s], a = spin[s];
+    const float f[9] = {p.x, p.y, p.z, v.x, v.y, v.z, a.x, a.y, a.z};
+#pragma unroll
+    for (int k = 0; k < 9; k++) out[(size_t)k * n + s] = f[k];
+}
+
 int32_t vxr_sphere_field(vxr_sphere_world* w, int32_t field, float* out) {
     if (!w || !out || field < 0 || field >= 24) return sfail(w, VXR_EINVAL, "field is 0 to 23");
     if (w->pending) {
@@ -1581,12 +1593,20 @@ int32_t vxr_sphere_field(vxr_sphere_world* w, int32_t field, float* out) {
 
 int32_t vxr_sphere_state(vxr_sphere_world* w, float* const* out9) {
     if (!w || !out9) return sfail(w, VXR_EINVAL, "null argument");
-    const int fields[9] = {0, 1, 2, 3, 4, 5, 14, 15, 16};  // x y z u v w ax ay az
-    for (int k = 0; k < 9; k++) {
-        if (!out9[k]) continue;
-        const int rc = vxr_sphere_field(w, fields[k], out9[k]);
+    if (w->pending) {
+        const int rc = finish(w, nullptr);
         if (rc != VXR_OK) return rc;
     }
+    // the 9 fields split out of the float4 arrays on the device, then copied straight into the caller's arrays
+    // (at the copy engine's full rate when they are pinned), one synchronisation for all
+    const int n = w->n;
+    if (!w->state9 && salloc(w, &w->state9, (size_t)9 * n) != VXR_OK) return VXR_ECUDA;
+    k_state9<<<(n + 255) / 256, 256, 0, w->stream>>>(n, w->s.pos, w->s.vel, w->s.spin, w->state9);  // not a step's
+    for (int k = 0; k < 9; k++)
+        if (out9[k])
+            SPH_CUDA(cudaMemcpyAsync(out9[k], w->state9 + (size_t)k * n, sizeof(float) * (size_t)n,
+                                     cudaMemcpyDeviceToHost, w->stream));
+    SPH_CUDA(cudaStreamSynchronize(w->stream));
     return VXR_OK;
 }
 

@@ -91,9 +91,13 @@ class SphereSimulation:
         self.totals = Report(r.waits_total, r.rounds_total, r.most_rounds_total, r.unlisted_total)
         return self.last_report
 
-    def state(self):
-        """x y z u v w ax ay az."""
-        out = [np.empty(self.n, np.float32) for _ in range(9)]
+    def state(self, out=None):
+        """x y z u v w ax ay az; into `out` (9 float32 arrays of n, e.g. in pinned memory) when given."""
+        if out is None:
+            out = [np.empty(self.n, np.float32) for _ in range(9)]
+        elif len(out) != 9 or any(a.dtype != np.float32 or a.shape != (self.n,) or not a.flags.c_contiguous
+                                  for a in out):
+            raise ValueError(f"out holds 9 contiguous float32 arrays of {self.n}")
         self._check(lib().vxr_sphere_state(self._h, ptr_array(out)))
         return out
 
