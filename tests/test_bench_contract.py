@@ -1,0 +1,53 @@
+"""bench.py's reference arm on CPU, as the round's driver launches it: one JSON line per run, with the keys the
+driver reads (impl, metric, value, unit, e2e with no host copies, cpu_baseline with its cores and sample), for
+each workload, on a bounded sample; ranks other than 0 exit 0 without work. And the product path without a GPU:
+creating a world fails loudly, with no CPU fallback."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+import torch
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+
+def run_bench(*args, env=None):
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], cwd=ROOT, capture_output=True,
+                         text=True, timeout=600, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    return out.stdout.strip().splitlines()
+
+
+@pytest.mark.parametrize("workload", ["large-mixed", "sphere-lattice", "batched-scenes"])
+def test_reference_arm_prints_one_line_of_the_contract(workload):
+    import bench
+    lines = run_bench("--impl", "reference", "--steps", "2", "--warmup", "1", "--workload", workload)
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference"
+    assert line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
+    assert line["value"] > 0 and line["higher_is_better"] is True
+    assert line["warmup"] >= 1 and line["steps"] >= 1 and line["n_gpus"] == 1
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    base = line["cpu_baseline"]
+    assert base["value"] == line["value"] and base["kind"] == "port" and base["cores"] >= 1 and base["sample"]
+    assert line["config"]["workload"]
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="1")
+    assert run_bench("--impl", "reference", "--steps", "2", "--warmup", "1", env=env) == []
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the behaviour with no GPU")
+def test_a_world_without_a_gpu_fails_loudly():
+    sys.path.insert(0, os.path.join(ROOT, "vexelray-sim-rigid_b200"))
+    from vxr import boxes as B
+    from vxr._lib import VxrError
+    from vxr.box_simulation import BoxSimulation
+    with pytest.raises((VxrError, RuntimeError, OSError)):
+        BoxSimulation(8, 1, 1, False, B.grid(1.0, 1.0, 1.0, 0.1, 0.005))
