@@ -286,7 +286,8 @@ int32_t vxr_mlp_train(vxr_mlp* net, const float* features, const float* targets,
 
 /* The learned warm start in a box world. mode 0: off (the reference's carried impulses); 1: each step gathers 16
  * features a contact point at its start and the impulses its solve reached (vxr_box_features reads them); 2: each
- * step starts every contact point from `net`'s predicted normal and friction impulse instead of the carried ones.
+ * step starts every contact point from `net`'s predicted normal and friction impulse instead of the carried ones;
+ * 3: only the points that carried nothing (new contacts) start from the prediction, the others keep theirs.
  * Features: gap, relative normal and tangential speed, the two inverse masses, the two inverse inertias along the
  * normal, the carried normal and friction impulse, the two bodies' touching pair counts, the feature kind one-hot
  * (face of first, face of second, edge, sphere) and the normal's vertical component; impulses (carried, targets and

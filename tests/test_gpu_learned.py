@@ -54,6 +54,28 @@ def test_gpu_a_network_of_zeros_starts_like_a_cold_start():
     net.close()
 
 
+def test_gpu_a_network_of_zeros_on_new_contacts_starts_like_the_carried_warm_start():
+    """Mode 3 with a network whose outputs are zero: the points that carried something keep it, and those that
+    carried nothing start from zero as they would anyway, so the steps equal the plain warm start's to the bit."""
+    from vxr.learned import Mlp
+    sc = small_scene(spheres=0.0, seed=4)
+    net = Mlp(seed=0)
+    p, _, _ = net.get()
+    for k in p:
+        p[k][:] = 0.0
+    net.set(p)
+    a = Lm.settled_world(sc, 150, 16)
+    b = Lm.settled_world(sc, 150, 16)
+    b.learned(net, 3)
+    a.step_and_wait(3)
+    b.step_and_wait(3)
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x.view(np.int32), y.view(np.int32))
+    a.close()
+    b.close()
+    net.close()
+
+
 def test_gpu_gather_train_judge():
     """The loop end to end on a small pile: rows gathered from the plain solver, a network trained on them by the
     GPU's kernels (its loss falls), then judged by the plain solver: the judgement reports sweeps for all three
@@ -67,8 +89,10 @@ def test_gpu_gather_train_judge():
     losses = net.train(f, t, epochs=5, batch=1024, lr=1e-3, seed=2)
     assert losses[-1] < losses[0]
     verdict = Lm.judge(w, net, steps=2)
-    for k in ("plain_warm_start", "plain_cold_start", "learned"):
+    for k in ("plain_warm_start", "plain_cold_start", "learned", "learned_new_contacts_only"):
         assert 1 <= verdict[k] <= 64
-    assert verdict["kept"] == (verdict["learned"] < verdict["plain_warm_start"])
+    best = min(verdict["learned"], verdict["learned_new_contacts_only"])
+    assert verdict["kept"] == (best < verdict["plain_warm_start"])
+    assert verdict["mode"] in ((2, 3) if verdict["kept"] else (0,))
     w.close()
     net.close()

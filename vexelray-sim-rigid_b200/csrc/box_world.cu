@@ -1383,9 +1383,11 @@ __global__ void k_features(const int* __restrict__ touching_n, const PairGen now
 
 // The network's starting impulses in place of the carried ones: normal max(0, p0) s; friction max(0, p1) s along
 // the carried tangential impulse, or against the tangential slip where none is carried.
+// fresh_only: only the points that carried nothing (contacts new this step, or carried at zero); the others keep
+// their carried impulses.
 __global__ void k_apply_learned(const int* __restrict__ touching_n, PairGen now, const Bodies b,
                                 const float* __restrict__ pred, Params P, const Params* __restrict__ scene_params,
-                                const int* __restrict__ body_scene) {
+                                const int* __restrict__ body_scene, bool fresh_only) {
     const int total = *touching_n;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
         const int4 rec = now.pair[k];
@@ -1400,6 +1402,7 @@ __global__ void k_apply_learned(const int* __restrict__ touching_n, PairGen now,
             const float ln = fmaxf(0.0f, pred[2 * row] * s);
             const float lt = fmaxf(0.0f, pred[2 * row + 1] * s);
             const float4 old = now.imp[at];
+            if (fresh_only && nonzero_bits(old)) continue;
             float dir[3] = {old.y, old.z, old.w};
             float len = sqrtf(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
             if (!(len > 1e-12f)) {
@@ -1733,14 +1736,14 @@ int enqueue_step(vxr_box_world* w) {
             k_features<<<tblocks, THREADS, 0, st>>>(tn, now, w->b, w->inc_count, w->params, w->scene_params,
                                                     w->body_scene, w->lfeat);
             LAUNCHED(1);
-            if (w->learn_mode == 2) {
+            if (w->learn_mode >= 2) {
                 if (vxr_mlp_forward_device(w->learn_net, w->lfeat, tn, MOST_POINTS, w->cap * MOST_POINTS, w->lpred,
                                            st) != VXR_OK) {
                     w->error = "the learned warm start's network did not launch";
                     return VXR_ECUDA;
                 }
                 k_apply_learned<<<tblocks, THREADS, 0, st>>>(tn, now, w->b, w->lpred, w->params, w->scene_params,
-                                                             w->body_scene);
+                                                             w->body_scene, w->learn_mode == 3);
                 LAUNCHED(2);
             }
         }
@@ -2226,7 +2229,7 @@ int32_t vxr_box_scenes(const vxr_box_world* w, int32_t* first_body) {
 }
 
 int32_t vxr_box_learned(vxr_box_world* w, vxr_mlp* net, int32_t mode) {
-    if (!w || mode < 0 || mode > 2 || (mode == 2 && !net)) return VXR_EINVAL;
+    if (!w || mode < 0 || mode > 3 || (mode >= 2 && !net)) return VXR_EINVAL;
     if (!w->has_grid) {
         w->error = "the learned warm start works on a world with a grid";
         return VXR_EINVAL;

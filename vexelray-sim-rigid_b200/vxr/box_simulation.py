@@ -139,7 +139,8 @@ class BoxSimulation:
                 "max_wall_penetration": d.max_wall, "max_speed": d.max_speed, "broken": bool(d.broken)}
 
     def learned(self, net, mode: int) -> None:
-        """The learned warm start: mode 0 off, 1 gather features and targets, 2 start from `net`'s impulses."""
+        """The learned warm start: mode 0 off, 1 gather features and targets, 2 start every point from `net`'s
+        impulses, 3 only the points that carried nothing (the others keep their carried impulses)."""
         self._check(self.L.vxr_box_learned(self.h, net.h if net is not None else None, mode))
 
     def features(self):

@@ -120,7 +120,7 @@ def gather(world, steps: int, rows_wanted: int, sweeps_cap: int = 64, tolerance:
 
 def sweeps_to_residual(world, steps: int, tolerance: float, cap: int, mode: int, net=None, cold: bool = False):
     """Mean solve sweeps a substep takes to reach the residual (at most `cap`), over `steps` steps, and the share of
-    substeps that reached it: the plain warm start (mode 0, or cold = from zero) or the network's (mode 2)."""
+    substeps that reached it: the plain warm start (mode 0, or cold = from zero) or the network's (mode 2 or 3)."""
     world.learned(net, mode)
     world.measure(residual=True, cold_start=cold, sweeps=cap, tolerance=tolerance)
     used_all = []
@@ -134,14 +134,19 @@ def sweeps_to_residual(world, steps: int, tolerance: float, cap: int, mode: int,
 
 def judge(world, net, steps: int = 3, tolerance: float = 1e-4, cap: int = 64) -> dict:
     """The plain solver judges the network: sweeps to the residual from its impulses against from the carried ones
-    (and from zero), each over the same number of steps from where the world is. The network is kept only if it
-    needs fewer sweeps; otherwise the plain warm start is the fallback."""
+    (and from zero), each over the same number of steps from where the world is. The network is tried on every
+    point (mode 2) and on the points that carried nothing (mode 3, the carried impulses kept elsewhere). It is kept,
+    in its better mode, only if it needs fewer sweeps; otherwise the plain warm start is the fallback."""
     plain, plain_reached = sweeps_to_residual(world, steps, tolerance, cap, 0)
     cold, cold_reached = sweeps_to_residual(world, steps, tolerance, cap, 0, cold=True)
     learned, learned_reached = sweeps_to_residual(world, steps, tolerance, cap, 2, net)
-    use = learned < plain
+    fresh, fresh_reached = sweeps_to_residual(world, steps, tolerance, cap, 3, net)
+    best_mode, best = (2, learned) if learned <= fresh else (3, fresh)
+    use = best < plain
     return {"plain_warm_start": plain, "plain_warm_start_reached": plain_reached, "plain_cold_start": cold,
             "plain_cold_start_reached": cold_reached, "learned": learned, "learned_reached": learned_reached,
-            "gain_vs_warm_start": plain / learned if learned > 0 else None,
-            "gain_vs_cold_start": cold / learned if learned > 0 else None,
-            "kept": bool(use), "fallback": None if use else "plain warm start (the network needs no fewer sweeps)"}
+            "learned_new_contacts_only": fresh, "learned_new_contacts_only_reached": fresh_reached,
+            "gain_vs_warm_start": plain / best if best > 0 else None,
+            "gain_vs_cold_start": cold / best if best > 0 else None,
+            "kept": bool(use), "mode": best_mode if use else 0,
+            "fallback": None if use else "plain warm start (the network needs no fewer sweeps in either mode)"}
