@@ -78,8 +78,9 @@ def test_gpu_a_network_of_zeros_on_new_contacts_starts_like_the_carried_warm_sta
 
 def test_gpu_gather_train_judge():
     """The loop end to end on a small pile: rows gathered from the plain solver, a network trained on them by the
-    GPU's kernels (its loss falls), then judged by the plain solver: the judgement reports sweeps for all three
-    starts, and the network is kept exactly when it needs fewer sweeps than the carried impulses."""
+    GPU's kernels (its loss falls), then judged by the plain solver: the judgement reports sweeps for all four
+    starts (carried, zero, the network everywhere, the network on new contacts), and the network is kept, in its
+    better mode, exactly when that needs fewer sweeps than the carried impulses."""
     from vxr.learned import Mlp
     sc = small_scene(seed=6)
     w = Lm.settled_world(sc, 250, 64)
