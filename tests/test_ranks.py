@@ -46,7 +46,7 @@ def rank_main(rank, world, port, out):
 
 def test_two_ranks_over_gloo():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # spawned, never forked from a threaded process
         out = m.dict()
         mp.spawn(rank_main, args=(world, free_port(), out), nprocs=world, join=True)
         res = [out[r] for r in range(world)]
