@@ -309,6 +309,8 @@ int32_t vxr_box_features(vxr_box_world* world, float* features16, float* targets
 #define VXR_SPHERE_ONE_BLOCK 8192       /* scenes up to this many spheres run on one block or one cluster */
 #define VXR_SPHERE_CLUSTER_FROM 256     /* ... on a cluster from this many spheres (by default) */
 #define VXR_SPHERE_CLUSTER 8            /* ... of this many blocks */
+#define VXR_SPHERE_CLUSTER_WIDE_FROM 2048  /* ... and from this many spheres */
+#define VXR_SPHERE_CLUSTER_WIDE 16     /* ... of this many */
 /* How a pass solves (SphereStep.Solve, core/sphere/SphereStep.java:37-43). */
 #define VXR_JACOBI 0
 #define VXR_GAUSS_SEIDEL_BY_CONTACT 1   /* run until every contact is solved (SphereStepper) */
@@ -328,7 +330,8 @@ typedef struct {
     vxr_grid grid;                /* nx = 0: every pair (Jacobi only) */
     int32_t device;
     int32_t blocks;               /* 0: up to VXR_SPHERE_ONE_BLOCK spheres one block (a cluster of
-                                     VXR_SPHERE_CLUSTER from VXR_SPHERE_CLUSTER_FROM), else enough for the list */
+                                     VXR_SPHERE_CLUSTER from VXR_SPHERE_CLUSTER_FROM, of VXR_SPHERE_CLUSTER_WIDE
+                                     from VXR_SPHERE_CLUSTER_WIDE_FROM), else enough for the list */
     int32_t cluster;              /* 2 to 16: the step runs on one thread-block cluster of this many blocks (one an
                                      SM), its passes separated by the cluster's barrier; 0: as `blocks` says */
 } vxr_sphere_config;

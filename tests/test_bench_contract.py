@@ -21,7 +21,7 @@ def run_bench(*args, env=None):
     return out.stdout.strip().splitlines()
 
 
-@pytest.mark.parametrize("workload", ["large-mixed", "sphere-lattice", "batched-scenes"])
+@pytest.mark.parametrize("workload", ["large-mixed", "sphere-lattice", "batched-scenes", "sphere-pile"])
 def test_reference_arm_prints_one_line_of_the_contract(workload):
     import bench
     lines = run_bench("--impl", "reference", "--steps", "2", "--warmup", "1", "--workload", workload)

@@ -209,3 +209,29 @@ def test_gpu_bad_config_is_refused():
         make_params(0.01, 0, -9.81, 0, 1, 1, 1, 2.0, True)
     assert np.array_equal(make_params(0.01, 0, -9.81, 0, 1, 1, 1, 1, True, 0.2, 0.5, 0.5, 0.1),
                           S.params(0.01, 0, -9.81, 0, 1, 1, 1, 1, True, 0.2, 0.5, 0.5, 0.1))
+
+
+@pytest.mark.parametrize("solver", ["until done mu=0.5", "until done", "grid averaged omega=1"])
+def test_gpu_the_reference_pile_matches_the_oracle(solver):
+    """The reference's own sphere benchmark scene (its sweep's large pile, 4,096 spheres) with each of the solver
+    settings it publishes times for: 60 frames, through the drop onto the floor, every field equal to the oracle's."""
+    from oracle.sphere import OracleSphereWorld
+    from vxr import scenes
+    from vxr.sphere_simulation import SphereSimulation
+    sc = scenes.sphere_pile(solver=solver)
+    n = sc["spheres"]
+    g = SphereSimulation(n, sc["substeps"], sc["iterations"], sc["grid"], sc["solve"])
+    g.start(sc["x"], sc["y"], sc["z"], sc["u"], sc["v"], sc["w"], sc["r"], sc["im"], sc["params"])
+    g.friction(sc["friction"])
+    o = OracleSphereWorld(n, sc["substeps"], sc["iterations"], sc["solve"], sc["grid"])
+    for k in ("x", "y", "z", "u", "v", "w", "r", "im"):
+        o.set_field(k, sc[k])
+    o.set_shown(S.shown_at_start(sc["x"], sc["y"], sc["z"], sc["r"]))
+    o.set_params(sc["params"], sc["friction"])
+    g.step_and_wait(60)
+    o.step(60)
+    for name in S.FIELDS:
+        assert np.array_equal(g.field(name).view(np.int32), o.field(name).view(np.int32)), name
+    assert np.array_equal(g.read_shown().view(np.int32), o.shown().view(np.int32))
+    g.close()
+    o.close()

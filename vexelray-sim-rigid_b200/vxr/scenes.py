@@ -198,3 +198,59 @@ def sphere_lattice(seed: int = 1, nx: int = 16, ny: int = 8, nz: int = 8, spacin
 
 def fields(scene: dict) -> list:
     return [scene[k] for k in FIELDS]
+
+
+def _java_doubles(seed: int):
+    """java.util.Random(seed).nextDouble(), again and again: the Java SE API's documented 48-bit linear
+    congruential generator, nextDouble = ((next(26) << 27) + next(27)) * 2^-53."""
+    mult, mask = 0x5DEECE66D, (1 << 48) - 1
+    state = (seed ^ mult) & mask
+
+    def nxt(bits):
+        nonlocal state
+        state = (state * mult + 0xB) & mask
+        return state >> (48 - bits)
+
+    while True:
+        yield ((nxt(26) << 27) + nxt(27)) * (1.0 / (1 << 53))
+
+
+# The reference's sphere sweep's solver settings (core tests, sphere/SphereSweepTest.java:20-48, :74-91): the name,
+# substeps, solve ("gs" Gauss-Seidel over the contact list run until done, "jacobi" on the grid), averaged, mu.
+PILE_SOLVERS = {
+    "until done mu=0.5": (10, "gs", False, 0.5),
+    "until done": (10, "gs", False, 0.0),
+    "grid averaged omega=1": (10, "jacobi", True, 0.0),
+}
+
+
+def sphere_pile(side: int = 16, seed: int = 7, solver: str = "until done mu=0.5") -> dict:
+    """The reference's sphere pile (core tests, sphere/SphereSweepTest.java:118-144, the large pile at side 16):
+    side^3 spheres of radius 3 cm and mass 0.1 kg dropped as a loose lattice into a box 0.08 + 0.06 side wide and
+    deep and 0.5 + 0.07 side tall, column x and row z jittered by java.util.Random(seed) (x drawn before z), layers
+    0.07 m apart from 0.3 m up; dt 1/60 s, one pass a substep, gravity -9.81, no restitution. `solver` is one of
+    PILE_SOLVERS. The reference times it over 240 frames at 60 Hz, after 2."""
+    from . import spheres as S
+    substeps, kind, averaged, mu = PILE_SOLVERS[solver]
+    solve = S.GAUSS_SEIDEL_BY_CONTACT if kind == "gs" else S.JACOBI
+    n = side ** 3
+    rnd = _java_doubles(seed)
+    x, y, z = np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32)
+    k = 0
+    for i in range(side):
+        for j in range(side):
+            for l_ in range(side):
+                x[k] = np.float32(0.07 + 0.06 * i + 0.005 * next(rnd))
+                y[k] = np.float32(0.3 + 0.07 * j)
+                z[k] = np.float32(0.07 + 0.06 * l_ + 0.005 * next(rnd))
+                k += 1
+    sx = sz = 0.08 + 0.06 * side
+    sy = 0.5 + 0.07 * side
+    dt = 1 / 60
+    r = np.full(n, np.float32(0.03), np.float32)
+    return {"x": x, "y": y, "z": z, "u": np.zeros(n, np.float32), "v": np.zeros(n, np.float32),
+            "w": np.zeros(n, np.float32), "r": r, "im": np.full(n, np.float32(1 / 0.1), np.float32),
+            "spheres": n, "walls": (sx, sy, sz), "dt": dt, "substeps": substeps, "iterations": 1, "solve": solve,
+            "friction": mu > 0, "grid": S.covering(sx, sy, sz, 0.06),
+            "params": S.params(dt / substeps, 0.0, -9.81, 0.0, sx, sy, sz, 1.0, averaged, 0.0, mu, mu, 0.0),
+            "frames": 240, "name": f"sphere pile {side}^3 = {n} spheres, r 3 cm, {solver}, seed {seed}"}
