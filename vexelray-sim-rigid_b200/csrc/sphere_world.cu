@@ -91,6 +91,7 @@ struct Kernel {
     int* cell_start;   // [cells + 1]
     int* claims;       // [3 n]
     int* list_count;   // [n]
+    int* part;         // [blocks] each block's slice total in a scan the blocks share
     int* list_start;   // [n + 1]
     ListGen gen[2];
     Counts* counts;
@@ -812,11 +813,13 @@ __device__ __forceinline__ void contact_round(const Kernel& K, const ListGen& L,
 
 __device__ __forceinline__ int position(int k) { return k == 0 ? 0 : 1 + (k - 1) % CYCLE; }
 
-// Exclusive scan of in[0..m) into out[0..m], out[m] the total, by the threads of one block.
-__device__ void block_scan(const int* in, int* out, int m) {
+// Exclusive scan of in[lo..hi) into out[lo..hi), starting from zero, by the threads of one block; returns the range's
+// total to every thread.
+__device__ int block_scan_range(const int* in, int* out, int lo, int hi) {
     __shared__ int warp_sums[32];
+    const int m = hi - lo;
     const int per = (m + blockDim.x - 1) / blockDim.x;
-    const int begin = min(m, (int)threadIdx.x * per), end = min(m, begin + per);
+    const int begin = lo + min(m, (int)threadIdx.x * per), end = min(hi, begin + per);
     int sum = 0;
     for (int i = begin; i < end; i++) sum += in[i];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -844,8 +847,29 @@ __device__ void block_scan(const int* in, int* out, int m) {
         out[i] = run;
         run += v;
     }
-    if (threadIdx.x == blockDim.x - 1) out[m] = warp_sums[(blockDim.x >> 5) - 1];
+    const int total = warp_sums[(blockDim.x >> 5) - 1];
     __syncthreads();
+    return total;
+}
+
+// The first half of a scan every block shares: block b scans its slice of in[0..m) into out, and posts the slice's
+// total. After a barrier, scan_finish adds the totals of the slices before it; out[m] is the whole total.
+__device__ __forceinline__ void scan_slices(const Kernel& K, const int* in, int* out, int m) {
+    const int per = (m + gridDim.x - 1) / gridDim.x;
+    const int lo = min(m, (int)blockIdx.x * per), hi = min(m, lo + per);
+    const int total = block_scan_range(in, out, lo, hi);
+    if (threadIdx.x == 0) K.part[blockIdx.x] = total;
+}
+__device__ __forceinline__ int scan_finish(const Kernel& K, int* out, int m) {
+    const int per = (m + gridDim.x - 1) / gridDim.x;
+    const int lo = min(m, (int)blockIdx.x * per), hi = min(m, lo + per);
+    int offset = 0;
+    for (int b = 0; b < (int)blockIdx.x; b++) offset += *(const volatile int*)&K.part[b];
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) out[i] += offset;
+    int whole = 0;
+    for (int b = 0; b < (int)gridDim.x; b++) whole += *(const volatile int*)&K.part[b];
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[m] = whole;
+    return whole;
 }
 
 __device__ __forceinline__ int read_int(const int* p) { return *(const volatile int*)p; }
@@ -906,7 +930,9 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
             }
             SYNC();
             if (K.gridded) {
-                if (blockIdx.x == 0) block_scan(K.cell_count, K.cell_start, K.cells);
+                scan_slices(K, K.cell_count, K.cell_start, K.cells);
+                SYNC();
+                scan_finish(K, K.cell_start, K.cells);
                 SYNC();
                 // a place in its cell for each sphere; the counts return to zero for the next substep
                 for (int s = gtid; s < n; s += gsize) {
@@ -933,9 +959,11 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
             if (gs) {
                 for (int a = gtid; a < n; a += gsize) K.list_count[a] = count_near(K, a);
                 SYNC();
-                if (blockIdx.x == 0) {
-                    block_scan(K.list_count, K.list_start, n);
-                    if (threadIdx.x == 0) K.counts->count[LISTED] = K.list_start[n];
+                scan_slices(K, K.list_count, K.list_start, n);
+                SYNC();
+                {
+                    const int whole = scan_finish(K, K.list_start, n);
+                    if (gtid == 0) K.counts->count[LISTED] = whole;
                 }
                 SYNC();
                 cur ^= 1;
@@ -1123,6 +1151,7 @@ struct vxr_sphere_world {
     float4* wall = nullptr;
     float* shown = nullptr;
     int *keys = nullptr, *order = nullptr, *cell_count = nullptr, *cell_start = nullptr;
+    int* part = nullptr;  // [blocks] the blocks' slice totals of a shared scan
     int *claims = nullptr, *list_count = nullptr, *list_start = nullptr;
     ListGen gen[2]{};
     Counts* counts = nullptr;
@@ -1256,6 +1285,7 @@ Kernel kernel_of(vxr_sphere_world* w, int steps) {
     K.claims = w->claims;
     K.list_count = w->list_count;
     K.list_start = w->list_start;
+    K.part = w->part;
     K.gen[0] = w->gen[0];
     K.gen[1] = w->gen[1];
     K.counts = w->counts;
@@ -1486,6 +1516,7 @@ vxr_sphere_world* vxr_sphere_create(const vxr_sphere_config* cfg, int32_t* statu
         w->blocks = cluster;
         w->cluster = 1;
     }
+    if (salloc(w, &w->part, (size_t)std::max(w->blocks, 1)) != VXR_OK) return bad(VXR_ECUDA);
     // the stepper's batch sizing starts at BATCH a pass (SphereStepper.java:59-64)
     std::vector<int> batch(w->iterations, BATCH);
     if (cudaMemcpy(w->opening, batch.data(), sizeof(int) * w->iterations, cudaMemcpyHostToDevice) != cudaSuccess)
