@@ -98,6 +98,43 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
+class Reports:
+    """The step reports of a timed loop, gathered over its periodic syncs. vxr_box_sync hands over the totals of the
+    steps since the sync before and zeroes them, so a sync with no step since reports nothing: the last step's
+    counts are kept from the last sync that covered a step, and the totals summed over all of them."""
+
+    def __init__(self):
+        self.last = None
+        self.unplaced_total = 0
+        self.unlisted_total = 0
+        self.most_rounds = 0
+        self.steps = 0
+
+    def add(self, rep):
+        if rep.steps > 0:
+            self.last = rep
+            self.unplaced_total += int(rep.unplaced_total)
+            self.unlisted_total += int(rep.unlisted_total)
+            self.most_rounds = max(self.most_rounds, int(rep.most_rounds))
+            self.steps += int(rep.steps)
+        return rep
+
+    def finish(self, world, synced_every: int, steps: int):
+        """The final sync, made only where steps ran since the loop's last periodic one."""
+        if steps % synced_every or self.last is None:
+            self.add(world.sync())
+        return self
+
+    def last_step(self) -> dict:
+        r = self.last
+        if r is None:
+            return {"touching": 0, "points": 0, "rounds": 0, "unplaced": 0, "unlisted": 0}
+        return {"touching": int(r.touching), "points": int(r.points), "rounds": int(r.rounds),
+                "unplaced": int(r.unplaced), "unlisted": int(r.unlisted), "most_rounds": self.most_rounds,
+                "unplaced_total": self.unplaced_total, "unlisted_total": self.unlisted_total,
+                "steps_reported": self.steps}
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -584,6 +621,7 @@ def run_batched(args):
     launches0 = sim.launches()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(pairs)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(pairs)]
+    reports = Reports()
     barrier(pg)
     torch.cuda.synchronize()
     with Clocks(local) as clocks:
@@ -595,8 +633,8 @@ def run_batched(args):
             with torch.cuda.stream(stream):
                 ends[k].record(stream)
             if k % 10 == 9:
-                sim.sync()
-        rep = sim.sync()
+                reports.add(sim.sync())
+        reports.finish(sim, 10, pairs)
     torch.cuda.synchronize()
     barrier(pg)
     launches = sim.launches() - launches0
@@ -646,7 +684,7 @@ def run_batched(args):
                    "parallelism": f"scenes shared out over {world_size} ranks" if world_size > 1 else "single"},
         "phase_ms_per_step": {"broad": phases[0] / 10, "narrow": phases[1] / 10, "colour": phases[2] / 10,
                               "solve": solve_ms},
-        "last_step": {"touching": rep.touching, "points": rep.points, "rounds": rep.rounds, **activity},
+        "last_step": {**reports.last_step(), **activity},
         "roofline": {"bound": "hbm", "kernel": "k_solve", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None, "peak_source": which, "bytes_per_launch": b_solve,
                      "ms_per_launch": solve_ms},
@@ -711,6 +749,7 @@ def run_towers(args):
     w.profile(True)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    reports = Reports()
     barrier(pg)
     torch.cuda.synchronize()
     with Clocks(local) as clocks:
@@ -722,8 +761,8 @@ def run_towers(args):
             with torch.cuda.stream(stream):
                 ends[k].record(stream)
             if k % 20 == 19:
-                w.sync()
-        rep = w.sync()
+                reports.add(w.sync())
+        reports.finish(w, 20, args.steps)
     torch.cuda.synchronize()
     barrier(pg)
     phases = w.profile(False)
@@ -751,7 +790,7 @@ def run_towers(args):
         "picture": pic,
         "phase_ms_per_step": {"broad": phases[0] / args.steps, "narrow": phases[1] / args.steps,
                               "colour": phases[2] / args.steps, "solve": solve_ms},
-        "last_step": {"touching": rep.touching, "points": rep.points, "rounds": rep.rounds, **activity},
+        "last_step": {**reports.last_step(), **activity},
         "roofline": {"bound": "hbm", "kernel": "k_solve", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None, "peak_source": which, "bytes_per_launch": b_solve,
                      "ms_per_launch": solve_ms},
@@ -886,6 +925,7 @@ def main():
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     sampled = []
+    reports = Reports()
     barrier(pg)
     torch.cuda.synchronize()
     with Clocks(local) as clocks:
@@ -897,13 +937,13 @@ def main():
             with torch.cuda.stream(stream):
                 ends[k].record(stream)
             if k % 20 == 19:
-                rep = w.sync()
+                reports.add(w.sync())
                 # the solve's algorithmic bytes, sampled every 20th step at the sync the loop makes anyway
                 a = w.activity()
                 sampled.append(algorithmic_solve_bytes(scene["bodies"], scene["substeps"], scene["sweeps"],
                                                        a["touching"], a["points"], a["bodies_active"],
                                                        a["wall_records"]))
-        rep = w.sync()
+        reports.finish(w, 20, args.steps)
     torch.cuda.synchronize()
     barrier(pg)
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
@@ -1008,8 +1048,7 @@ def main():
         "phase_ms_per_step": {"broad": phases[0] / args.steps, "narrow": phases[1] / args.steps,
                               "colour": phases[2] / args.steps, "solve": phases[3] / args.steps},
         "windows": windows,
-        "last_step": {"touching": rep.touching, "points": rep.points, "rounds": rep.rounds,
-                      "unplaced": rep.unplaced, "unlisted": rep.unlisted, **activity},
+        "last_step": {**reports.last_step(), **activity},
         "roofline": {"bound": "hbm", "kernel": "k_solve", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": LATE_SOLVE_TRAFFIC["dram_bytes"] if args.bodies == BODIES
                      else None, "peak_source": which, "bytes_per_launch": b_solve, "ms_per_launch": solve_ms,

@@ -22,7 +22,7 @@ extern "C" {
 #endif
 
 /* Status codes. The reference throws IllegalArgumentException for bad parameters or sizes
- * (core/box/Boxes.java:212-226, core/box/BoxStep.java:118-121) and IllegalStateException for a pass that never
+ * (core/box/Boxes.java:212-226, core/box/BoxStep.java:82-85) and IllegalStateException for a pass that never
  * ends (core/sphere/SphereStepper.java:86-88); soft failures it counts in its reports. */
 #define VXR_OK 0
 #define VXR_EINVAL 1     /* bad argument: IllegalArgumentException in the reference */
@@ -35,7 +35,7 @@ extern "C" {
 #define VXR_PARAM_COUNT 18   /* core/box/Boxes.java:101 */
 #define VXR_SHOWN_STRIDE 20  /* core/box/Boxes.java:781 */
 #define VXR_SLOTS 32         /* core/box/BoxBroad.java:60 */
-#define VXR_MOST_ROUNDS 32   /* core/box/BoxStep.java:81 */
+#define VXR_MOST_ROUNDS 32   /* core/box/BoxStep.java:45 */
 #define VXR_BOX_SHAPE 0.0f   /* core/box/Boxes.java:154 */
 #define VXR_SPHERE_SHAPE 1.0f
 
@@ -47,7 +47,7 @@ typedef struct {
 } vxr_grid;
 
 /* A world's shape, fixed at creation: the reference's BoxStep(boxes, substeps, sweeps, symmetric, grid)
- * (core/box/BoxStep.java:117-198). */
+ * (core/box/BoxStep.java:81-162). */
 typedef struct {
     int32_t bodies;
     int32_t substeps;
@@ -64,7 +64,7 @@ typedef struct {
     int32_t solve_blocks_per_sm; /* blocks of the solve kernel an SM runs; 0 = as many as fit (the autotuner's knob) */
 } vxr_box_config;
 
-/* What a step took: core/box/BoxStepper.java:308-311 (Report), plus the totals over a vxr_box_step call. */
+/* What a step took: core/box/BoxStepper.java:40 (Report), plus the totals over a vxr_box_step call. */
 typedef struct {
     int32_t touching;  /* pairs whose manifolds have points (last step) */
     int32_t points;    /* their points */
@@ -93,7 +93,7 @@ int32_t vxr_box_make_grid(double sx, double sy, double sz, double widest_half_di
 typedef struct vxr_box_world vxr_box_world;
 
 /* A world on the GPU: replaces new BoxStep(...) + new BoxSimulation(context, step)
- * (core/box/BoxStep.java:117-198, gui/BoxSimulation.java:34-50). NULL on failure, *status says why. */
+ * (core/box/BoxStep.java:81-162, gui/BoxSimulation.java:34-50). NULL on failure, *status says why. */
 vxr_box_world* vxr_box_create(const vxr_box_config* config, int32_t* status);
 
 /* Releases the world: replaces BoxSimulation.close (gui/BoxSimulation.java:183-188). */
@@ -119,7 +119,7 @@ int32_t vxr_box_load_state(vxr_box_world* world, const float* const* fields18, c
 int32_t vxr_box_params(vxr_box_world* world, const int32_t* params18);
 
 /* `steps` steps, waited for: replaces BoxSimulation.stepAndWait (gui/BoxSimulation.java:115-142), which runs
- * BoxStepper.step (core/box/BoxStepper.java:324-368). The report is the last step's, with totals. */
+ * BoxStepper.step (core/box/BoxStepper.java:56-100). The report is the last step's, with totals. */
 int32_t vxr_box_step(vxr_box_world* world, int32_t steps, vxr_box_report* report);
 
 /* `steps` steps enqueued on the world's stream, not waited for; vxr_box_sync waits and reports. Replaces the
@@ -138,7 +138,7 @@ int32_t vxr_box_state(vxr_box_world* world, float* const* out13);
 int32_t vxr_box_read_shown(vxr_box_world* world, float* out);
 
 /* The last step's touching pairs in slot order (the order BoxStepper reads `contacts`,
- * core/box/BoxStepper.java:339-358): first and second body, point count, the manifold in the reference's 40-word
+ * core/box/BoxStepper.java:71-90): first and second body, point count, the manifold in the reference's 40-word
  * layout (core/box/BoxContact.java:85-96) and the impulses in its 28-word layout (core/box/BoxPairs.java:48-50).
  * Any output may be NULL. Returns the number of touching pairs, or minus a status. */
 int32_t vxr_box_touching(vxr_box_world* world, int32_t* first, int32_t* second, int32_t* points, float* manifold40,
@@ -159,7 +159,7 @@ int32_t vxr_box_colour_waves(vxr_box_world* world);
  * cold_start = 1 starts every step's pair impulses from zero instead of carrying them (BoxPairs.carry,
  * core/box/BoxPairs.java:191-267) — the plain solver with no warm start, for comparison; sweeps (1 .. the count the
  * world was created with; 0 = that count) sets the sweeps of the solve and of the relax a substep runs, as the
- * reference's BoxStep sweeps (core/box/BoxStep.java:86); tolerance > 0 (with residual = 1, barrier schedule) stops a
+ * reference's BoxStep sweeps (core/box/BoxStep.java:49-50); tolerance > 0 (with residual = 1, barrier schedule) stops a
  * substep's solve sweeps, and its relax sweeps, once a sweep's residual is at or below it. */
 int32_t vxr_box_measure(vxr_box_world* world, int32_t residual, int32_t cold_start, int32_t sweeps, float tolerance);
 
@@ -200,27 +200,29 @@ int32_t vxr_collide(int32_t bodies, const float* const* fields18, const int32_t*
 /* The broad phase with no allocation. No counterpart in the reference: it exists for callers that cannot allocate
  * device memory while they step bodies — a host that owns all device memory through its own pool, or code that
  * must not allocate (an allocation synchronises the device) between the launches it is recording or under a
- * frame deadline. It runs the same bin, stable counting sort, neighbourhood list and compaction as a world's step
- * (core/box/BoxBroad.java:74-164 is what those replace) and writes the candidate pairs, sorted by (first, second),
- * to the caller's device arrays first_out and second_out (capacity entries each). All its scratch lives in one array
- * of about 6 MiB in this library's device memory, which every GPU that loads the library holds until the process
- * exits; nothing is allocated.
+ * frame deadline. It runs the same bin, stable counting sort, neighbourhood list and compaction kernels as a
+ * world's step and writes the candidate pairs, sorted by (first, second), to the caller's device arrays first_out
+ * and second_out (capacity entries each). All its scratch lives in one array of about 6 MiB in this library's
+ * device memory, which every GPU that loads the library holds until the process exits; nothing is allocated.
  *   Limits: at most 16384 bodies and 262144 grid cells a call; beyond them the call returns VXR_ECAPACITY and does
  *   nothing.
+ *   reach_cells: the neighbourhood's half-width in cells, 0 or 1 for the 27 cells, at most the grid's widest side
+ *   (max of nx, ny, nz: a wider reach finds no more pairs); a negative or wider value returns VXR_EINVAL.
  *   fields11: device pointers to x y z qx qy qz qw hx hy hz shape (bodies floats each).
  *   result3: a device array that receives [candidate pairs found (may exceed capacity), partners beyond 32 slots,
  *   VXR_OK or VXR_ECAPACITY (more pairs than capacity: the first capacity are written)].
  *   stream: the cudaStream_t to run on (NULL: the default stream); the call does not wait.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress) and should come before
- * any stream capture. Every call shares the array and it keeps the last call's contents: calls whose work overlaps
- * on the GPU (other streams, other host threads) race, so order them on one stream. */
+ * Every call looks up the array's address on the current device (cudaGetSymbolAddress, which allocates nothing), so
+ * the address stays right after cudaDeviceReset. The first call on a device may load the library's kernels onto it
+ * and should come before any stream capture. Every call shares the array and it keeps the last call's contents:
+ * calls whose work overlaps on the GPU (other streams, other host threads) race, so order them on one stream. */
 int32_t vxr_box_broadphase_static(int32_t bodies, const float* const* fields11, vxr_grid grid, int32_t reach_cells,
                                   float margin, int32_t* first_out, int32_t* second_out, int32_t capacity,
                                   int32_t* result3, void* stream);
 
 /* ---- Batched scenes -----------------------------------------------------------------------------------------------
  * Many independent scenes stepped as one world: no reference counterpart (the reference runs one BoxStep a scene,
- * core/box/BoxStep.java:117-198). Bodies are numbered scene after scene; each scene has its own grid (cells in one
+ * core/box/BoxStep.java:81-162). Bodies are numbered scene after scene; each scene has its own grid (cells in one
  * key space, end to end, so no body meets another scene's) and its own gravity, walls and friction. The substep,
  * margin, softness and push are one for the batch. Every scene's step is the one a world of that scene alone would
  * take, bit for bit: greedy colouring gives each scene's pairs the rounds they get alone. */

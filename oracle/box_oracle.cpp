@@ -311,7 +311,7 @@ void roll(Sweep sweep, Moving* first, Moving& second, float radius, const float*
 }
 
 // ------------------------------------------------------------------------------------------------------
-// The world: the reference's buffers (BoxStep.java :117-198).
+// The world: the reference's buffers (BoxStep.java :81-162).
 struct World {
     int n, substeps, sweeps, symmetric;
     int nx, ny, nz;
@@ -1119,7 +1119,7 @@ void solveRound(World& w, Sweep sweep, bool reverse, int round) {
     }
 }
 
-// BoxStep.sweep :253-267.
+// BoxStep.sweep :217-231.
 void sweepAll(World& w, Sweep kind, bool reverse, int rounds) {
     if (reverse) walls(w, kind, true);
     for (int order = 0; order < rounds; order++) {
@@ -1129,7 +1129,7 @@ void sweepAll(World& w, Sweep kind, bool reverse, int rounds) {
     if (!reverse) walls(w, kind, false);
 }
 
-// BoxStepper.step :324-368 with the collide list (BoxStep :174-189) and the substeps (BoxStep.build :235-250).
+// BoxStepper.step :56-100 with the collide list (BoxStep :141-158) and the substeps (BoxStep.build :199-215).
 void stepOnce(World& w) {
     int used = 0;
     for (int k = 0; k < 5; k++) w.report[k] = 0;

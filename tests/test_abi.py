@@ -56,3 +56,15 @@ def test_grid_matches_the_reference_rule():
     ref = B.grid(128.0, 70.0, 128.0, 1.0392304845, 0.005)
     assert (g.nx, g.ny, g.nz) == (ref.nx, ref.ny, ref.nz)
     assert np.float32(g.cell) == np.float32(ref.cell)
+
+
+def test_static_broad_phase_refuses_a_reach_beyond_the_grid():
+    """vxr_box_broadphase_static refuses a negative reach or one wider than the grid's widest side before it touches
+    a device: an unbounded reach would only lengthen every thread's neighbourhood walk."""
+    import ctypes
+    L = _lib.lib()
+    g = _lib.Grid(4, 6, 5, 1.0)
+    dummy = (ctypes.c_void_p * 11)(*([1] * 11))  # never read: the arguments are refused first
+    one = ctypes.c_void_p(1)
+    for reach in (-1, 7, 645, 1 << 30):
+        assert L.vxr_box_broadphase_static(8, dummy, g, reach, 0.0, one, one, 0, one, None) == _lib.VXR_EINVAL

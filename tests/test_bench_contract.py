@@ -51,3 +51,40 @@ def test_a_world_without_a_gpu_fails_loudly():
     from vxr.box_simulation import BoxSimulation
     with pytest.raises((VxrError, RuntimeError, OSError)):
         BoxSimulation(8, 1, 1, False, B.grid(1.0, 1.0, 1.0, 0.1, 0.005))
+
+
+class _Rep:
+    def __init__(self, steps, touching=0, rounds=0, unplaced=0, unlisted=0):
+        self.steps, self.touching, self.points, self.rounds = steps, touching, 2 * touching, rounds
+        self.unplaced, self.unlisted, self.most_rounds = unplaced, unlisted, rounds
+        self.unplaced_total, self.unlisted_total = unplaced * steps, unlisted * steps
+
+
+class _World:
+    """A world whose sync reports nothing when no step ran since the sync before, as vxr_box_sync does."""
+
+    def __init__(self):
+        self.pending = 0
+
+    def step(self, k):
+        self.pending += k
+
+    def sync(self):
+        k, self.pending = self.pending, 0
+        return _Rep(k, 500, 7, 1, 2) if k else _Rep(0)
+
+
+@pytest.mark.parametrize("steps", [20, 40, 25, 7])
+def test_last_step_keeps_the_colouring_when_the_final_sync_has_nothing_new(steps):
+    import bench
+    w = _World()
+    reports = bench.Reports()
+    for k in range(steps):
+        w.step(1)
+        if k % 20 == 19:
+            reports.add(w.sync())
+    reports.finish(w, 20, steps)
+    last = reports.last_step()
+    assert last["touching"] > 0 and last["rounds"] > 0
+    assert last["steps_reported"] == steps
+    assert last["unplaced_total"] == steps and last["unlisted_total"] == 2 * steps

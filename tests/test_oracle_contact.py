@@ -2,7 +2,7 @@
 
 Restates vexelray-sim-rigid-core/src/test/java/dev/vexelray/sim/rigid/box/BoxContactTest.java: 11 hand-worked box
 cases, 6 sphere cases and 500 random pairs (java.util.Random(19)), with the reference's tolerances (normals to
-2e-6, points to 1e-5, depths to 2e-6). The same cases run against the CUDA kernel in test_gpu_parity.py.
+2e-6, points to 1e-5, depths to 2e-6). The same cases run against the CUDA kernel in test_gpu_box.py.
 """
 import math
 

@@ -1,5 +1,5 @@
 """The picture's hand-off ring: the reference's ShownRingTest (vexelray-sim-rigid-gui/src/test/java/dev/vexelray/sim/
-rigid/gui/ShownRingTest.java:23-118), run against the native ring with no device (generations of no bodies keep no
+rigid/gui/ShownRingTest.java:22-94), run against the native ring with no device (generations of no bodies keep no
 buffers); and, on the GPU, frames that carry the steps' pictures."""
 import numpy as np
 import pytest

@@ -3,9 +3,9 @@
 //
 // The step the reference runs (paths inside sibarum/vexelray-sim-rigid, core =
 // vexelray-sim-rigid-core/src/main/java/dev/vexelray/sim/rigid/):
-//   core/box/BoxStep.java:174-189  collide list: keep, bin, sort, list, collide, carry, counts
-//   core/box/BoxStepper.java:324-368  host wait, greedy colouring, rounds written, substeps run
-//   core/box/BoxStep.java:235-267  per substep: velocities, WARM sweep, sweeps x SOLVE, positions, sweeps x RELAX;
+//   core/box/BoxStep.java:141-158  collide list: keep, bin, sort, list, collide, carry, counts
+//   core/box/BoxStepper.java:56-100    host wait, greedy colouring, rounds written, substeps run
+//   core/box/BoxStep.java:199-231  per substep: velocities, WARM sweep, sweeps x SOLVE, positions, sweeps x RELAX;
 //                                  each sweep every round of pairs then the walls (reversed: walls first)
 // Here the same passes run as device kernels in one stream. What changes is the layout and the scheduling:
 //   * body state is five float4 arrays (pose+im, turn, half+shape, velocity, angular momentum);
@@ -23,7 +23,6 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -494,7 +493,7 @@ __global__ void k_carry(const int* __restrict__ touching_n, const int* __restric
 }
 
 // ------------------------------------------------------------------------------------------------------------
-// Colouring (BoxStepper.java:339-358), reproduced exactly on the device.
+// Colouring (BoxStepper.java:71-90), reproduced exactly on the device.
 //
 // The host's greedy pass puts each touching pair, in slot order, into the first of 32 rounds holding neither of
 // its bodies. So a pair's round is the least round not used by the lower-numbered touching pairs that share a
@@ -1176,7 +1175,7 @@ struct Tracer {
 // Rounds of at most this many pairs (one a thread of a block) are run by one block, without grid barriers.
 constexpr int SMALL_ROUND = SOLVE_THREADS;
 
-// One sweep (BoxStep.sweep :253-267): every round of pairs, then the walls; backward, the walls first and the
+// One sweep (BoxStep.sweep :217-231): every round of pairs, then the walls; backward, the walls first and the
 // rounds last to first.
 __device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsigned int& epoch, int kind, bool reverse,
                                           int rounds, int slot, bool fill, int index) {
@@ -2817,7 +2816,7 @@ constexpr size_t STATIC_BYTES = 4 * STATIC_F4 + 5 * STATIC_N + STATIC_N1 + STATI
 }  // namespace
 
 // The scratch of vxr_box_broadphase_static: about 6 MiB. Host code must not use this name as a device address; the
-// address comes from cudaGetSymbolAddress, once per device.
+// address comes from cudaGetSymbolAddress on the current device, every call.
 static __device__ __align__(256) unsigned char vxr_broadphase_scratch[STATIC_BYTES];
 
 namespace {
@@ -2843,9 +2842,6 @@ __global__ void k_static_result(int n, int capacity, const int* __restrict__ can
     result[2] = total > capacity ? VXR_ECAPACITY : VXR_OK;
 }
 
-std::mutex static_setup_lock;
-unsigned char* static_scratch_of_device[64] = {nullptr};
-
 }  // namespace
 
 extern "C" int32_t vxr_box_broadphase_static(int32_t bodies, const float* const* fields11, vxr_grid grid,
@@ -2857,21 +2853,16 @@ extern "C" int32_t vxr_box_broadphase_static(int32_t bodies, const float* const*
     for (int k = 0; k < 11; k++)
         if (!fields11[k]) return VXR_EINVAL;
     if (grid.nx < 1 || grid.ny < 1 || grid.nz < 1 || !(grid.cell > 0.0f)) return VXR_EINVAL;
+    // The reach: 0 or 1 is the 27 cells; wider than the grid's widest side finds no more pairs, and an unbounded one
+    // would only lengthen every thread's walk.
+    if (reach_cells < 0 || reach_cells > std::max(grid.nx, std::max(grid.ny, grid.nz))) return VXR_EINVAL;
     const long cells = (long)grid.nx * grid.ny * grid.nz;
     if (bodies > STATIC_MAX_BODIES || cells > STATIC_MAX_CELLS) return VXR_ECAPACITY;  // beyond the fixed scratch
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return VXR_ECUDA;
-    unsigned char* base = nullptr;
-    {
-        std::lock_guard<std::mutex> hold(static_setup_lock);
-        if (!static_scratch_of_device[device]) {
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, vxr_broadphase_scratch) != cudaSuccess || !p) return VXR_ECUDA;
-            static_scratch_of_device[device] = (unsigned char*)p;
-        }
-        base = static_scratch_of_device[device];
-    }
-    unsigned char* at = base;
+    // The array's address on the current device, looked up every call (no allocation): a cached one would go stale
+    // once cudaDeviceReset unloads the module.
+    void* symbol = nullptr;
+    if (cudaGetSymbolAddress(&symbol, vxr_broadphase_scratch) != cudaSuccess || !symbol) return VXR_ECUDA;
+    unsigned char* at = (unsigned char*)symbol;
     auto take = [&](size_t bytes) {
         unsigned char* r = at;
         at += bytes;
@@ -2901,7 +2892,7 @@ extern "C" int32_t vxr_box_broadphase_static(int32_t bodies, const float* const*
     if (cudaMemsetAsync(counters, 0, sizeof(Counters), st) != cudaSuccess) return VXR_ECUDA;
     StaticFields f{fields11[0], fields11[1], fields11[2], fields11[3], fields11[4], fields11[5],
                    fields11[6], fields11[7], fields11[8], fields11[9], fields11[10]};
-    GridDims g{grid.nx, grid.ny, grid.nz, grid.cell, reach_cells > 0 ? reach_cells : 1};
+    GridDims g{grid.nx, grid.ny, grid.nz, grid.cell, reach_cells > 0 ? reach_cells : 1};  // 0: the 27 cells
     k_pack_static<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, f, pose, turn, half);
     const SceneGrids none{nullptr, nullptr, nullptr};
     k_bin<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, g, none, pose, turn, half, keys, reach, cell_count);

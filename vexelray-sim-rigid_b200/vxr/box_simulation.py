@@ -2,7 +2,7 @@
 
 Mirrors gui/BoxSimulation.java (vexelray-sim-rigid-gui/src/main/java/dev/vexelray/sim/rigid/gui/BoxSimulation.java):
 ``start`` :77-108, ``params`` :111-113, ``step_and_wait`` :115-142, ``last`` :145-147, ``state`` :153-160,
-``read_shown`` :163-165, ``close`` :183-188; and the step shape of core/box/BoxStep.java:117-198. Every call goes
+``read_shown`` :163-165, ``close`` :183-188; and the step shape of core/box/BoxStep.java:81-162. Every call goes
 through libvxr.so; nothing here computes the step.
 """
 from __future__ import annotations
@@ -21,7 +21,7 @@ ALL_FIELDS = STATE_FIELDS + ["im", "hx", "hy", "hz", "shape"]
 
 @dataclass
 class Report:
-    """BoxStepper.Report (core/box/BoxStepper.java:308-311) of the last step, with totals over the call."""
+    """BoxStepper.Report (core/box/BoxStepper.java:40) of the last step, with totals over the call."""
     touching: int
     points: int
     rounds: int
