@@ -163,6 +163,18 @@ int32_t vxr_box_colour_waves(vxr_box_world* world);
  * substep's solve sweeps, and its relax sweeps, once a sweep's residual is at or below it. */
 int32_t vxr_box_measure(vxr_box_world* world, int32_t residual, int32_t cold_start, int32_t sweeps, float tolerance);
 
+/* How the substeps are scheduled, from the next step on; no reference counterpart, the results are the same either
+ * way (the reference's per-body order, core/box/BoxStep.java:199-231). enable = 1 (the default): the connected
+ * components of the placed touching pairs of at most 64 bodies are solved whole by one warp each, their rounds
+ * apart by warp barriers, and bodies in no placed pair by a thread each; only larger components go through the
+ * grid-wide phases. enable = 0: every body goes through the grid-wide phases. A measuring tolerance
+ * (vxr_box_measure) runs every body through the grid-wide phases whatever this says. */
+int32_t vxr_box_islands(vxr_box_world* world, int32_t enable);
+
+/* How the last step was scheduled: out4 = [bodies through the grid-wide phases, bodies in small components (island
+ * warps), bodies in no placed pair (a thread each), island groups]. With islands off: [bodies, 0, 0, 0]. */
+int32_t vxr_box_paths(vxr_box_world* world, int32_t* out4);
+
 /* The last step's per-sweep residuals, substep by substep: the warm sweep, the solve sweeps, the relax sweeps
  * (substeps * (2 sweeps + 1) values). A sweep's residual is the largest positional correction its updates made at any
  * contact point, h k (|change of the normal impulse| + |change of the tangential impulse|) in metres, k the point's

@@ -44,6 +44,18 @@ constexpr int SOLVE_THREADS = 256;
 // then two boxes by point count (1 to 4).
 constexpr int PAIR_KINDS = 6;
 constexpr int BUCKETS = (MOST_ROUNDS + 1) * PAIR_KINDS;
+// Pairs are bucketed by path, then round, then kind: path 0 the pairs the grid phases solve (bodies of a component
+// too large for one warp, and every unplaced pair), path 1 the pairs of the small components the island warps solve.
+constexpr int ALL_BUCKETS = 2 * BUCKETS;
+// Islands: connected components of the placed touching pairs. A component of at most ISLAND_MOST bodies is solved
+// whole by one warp, its rounds apart by warp barriers; larger ones go through the grid phases. Components are packed
+// into groups in order of their roots: a group takes components until GROUP_BASE bodies have been placed, so it holds
+// at most GROUP_BASE + ISLAND_MOST - 1 bodies.
+constexpr int ISLAND_MOST = 64;
+constexpr int GROUP_BASE = 64;
+constexpr int GROUP_CAP = 128;
+constexpr int GROUP_ROUNDS = MOST_ROUNDS;  // (group, round) lists: placed pairs only
+constexpr int ISLAND_WARPS = 4;            // groups a block of the island kernel runs at once
 
 // ------------------------------------------------------------------------------------------------------------
 // Device buffers of a world.
@@ -91,7 +103,10 @@ struct Counters {  // device-side counts of a step
     unsigned int bar_count, bar_gen;
     int remaining[3];
     int trace_len;
-    int pad[2];
+    int grid_rounds;  // rounds the grid phases' pairs (path 0) use
+    int grid_n;       // bodies the grid phases move (components beyond a warp)
+    int free_n;       // bodies in no placed pair
+    int work;         // the island kernel's work counter
 };
 
 struct Totals {  // accumulated over the steps of one vxr_box_step call
@@ -117,7 +132,7 @@ struct vxr_box_world {
     Params params{};
     std::string error;
     int sms = 148;
-    int solve_blocks = 0, colour_blocks = 0;
+    int solve_blocks = 0, colour_blocks = 0, island_blocks = 0;
     float last_ms = 0.0f;
 
     Bodies b{};
@@ -157,6 +172,22 @@ struct vxr_box_world {
     int *round_count = nullptr, *round_start = nullptr, *round_fill = nullptr;  // by (round, kind) bucket
     int* bucket_start = nullptr;
     int *bucket_most = nullptr, *bucket_pstart = nullptr;  // by bucket: most points of a pair, first point
+    // islands (connected components of the placed touching pairs), rebuilt every step
+    int islands = 1;                  // small components solved by warps (0: every body through the grid phases)
+    int groups_max = 0;               // groups the bodies can fill
+    int *parent = nullptr;            // [n] union-find parent
+    int *comp = nullptr;              // [n] each body's component: its root
+    int *isl_size = nullptr;          // [n] bodies of the component rooted here
+    int *isl_key = nullptr;           // [n] a small component's body count at its root, 0 elsewhere
+    int *isl_offset = nullptr;        // [n + 1] their exclusive sum: where each small component's bodies begin
+    int *isl_fill = nullptr;          // [n] bodies of the component placed so far
+    int *body_group = nullptr;        // [n] a small component's group; -1 in no placed pair; -2 on the grid phases
+    int *body_local = nullptr;        // [n] its place in the group
+    int *group_body = nullptr;        // [groups_max * GROUP_CAP] each group's bodies
+    int *group_count = nullptr;       // [groups_max]
+    int *gr_count = nullptr, *gr_start = nullptr, *gr_fill = nullptr;  // by (group, round)
+    int2* ilist = nullptr;            // [cap] island pairs by (group, round): round-order position, local ids
+    int *grid_list = nullptr, *free_list = nullptr;  // [n] bodies of the grid phases; bodies in no placed pair
     Counters* counters = nullptr;
     Totals* totals = nullptr;
     Totals* host_totals = nullptr;  // pinned
@@ -577,6 +608,103 @@ __global__ void __launch_bounds__(THREADS) k_colour(const int* __restrict__ touc
     }
 }
 
+
+// ------------------------------------------------------------------------------------------------------------
+// Islands. Two bodies joined by a chain of placed pairs form one component; bodies of different components share no
+// pair and no wall record, so what a component's bodies go through in a step depends on that component alone. The
+// reference's order of operations is a per-body order (each body: its pairs in round order, then its walls, sweep
+// by sweep), so a component may be solved apart from the others, by one warp with warp barriers between its rounds,
+// and give every bit the grid phases give. Components are found by union-find over the placed pairs (unplaced pairs
+// are never solved, so they join nothing).
+
+__device__ __forceinline__ int uf_find(int* parent, int x) {
+    int p = *(volatile int*)&parent[x];
+    while (p != x) {
+        const int up = *(volatile int*)&parent[p];
+        if (up != p) *(volatile int*)&parent[x] = up;  // halve the path: up is an ancestor of x
+        x = p;
+        p = up;
+    }
+    return x;
+}
+
+__global__ void k_uf_init(int n, int* __restrict__ parent, int* __restrict__ size, int* __restrict__ fill) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    parent[s] = s;
+    size[s] = 0;
+    fill[s] = 0;
+}
+
+// Each placed pair joins its bodies' components: the larger root is hooked under the smaller, so every parent is
+// at most its child and no chain can loop.
+__global__ void k_uf_link(const int* __restrict__ touching_n, const int* __restrict__ ta, const int* __restrict__ tb,
+                          const int* __restrict__ colour, int* parent) {
+    const int total = *touching_n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int c = colour[t];
+        if (c < 0 || c >= MOST_ROUNDS) continue;
+        int a = uf_find(parent, ta[t]), b = uf_find(parent, tb[t]);
+        while (a != b) {
+            const int hi = max(a, b), lo = min(a, b);
+            const int was = atomicCAS(&parent[hi], hi, lo);
+            if (was == hi) break;
+            a = uf_find(parent, was);
+            b = uf_find(parent, lo);
+        }
+    }
+}
+
+// Every body's root (the links are done: parents only read), and each component's body count.
+__global__ void k_uf_flatten(int n, const int* __restrict__ parent, int* __restrict__ comp, int* __restrict__ size) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int r = s;
+    for (int p = parent[r]; p != r; p = parent[r]) r = p;
+    comp[s] = r;
+    atomicAdd(&size[r], 1);
+}
+
+// Which path each body takes: a component of one body (no placed pair) alone, a component of at most ISLAND_MOST
+// bodies in a group, a larger one through the grid phases. A small component's root keys the packing.
+__global__ void k_classify(int n, const int* __restrict__ root, const int* __restrict__ size, int* __restrict__ key,
+                           int* __restrict__ body_group, int* __restrict__ grid_list, int* __restrict__ free_list,
+                           Counters* counters) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int r = root[s];
+    const int m = size[r];
+    int k = 0;
+    if (m == 1) {
+        body_group[s] = -1;
+        free_list[atomicAdd(&counters->free_n, 1)] = s;
+    } else if (m > ISLAND_MOST) {
+        body_group[s] = -2;
+        grid_list[atomicAdd(&counters->grid_n, 1)] = s;
+    } else if (r == s) {
+        k = m;
+    }
+    key[s] = k;
+}
+
+// A small component's bodies: the group its root's place falls in, and places in that group one after another.
+__global__ void k_assign(int n, const int* __restrict__ root, const int* __restrict__ size,
+                         const int* __restrict__ offset, int* __restrict__ fill, int* __restrict__ body_group,
+                         int* __restrict__ body_local, int* __restrict__ group_body, int* __restrict__ group_count) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int r = root[s];
+    const int m = size[r];
+    if (m == 1 || m > ISLAND_MOST) return;
+    const int at = offset[r];
+    const int g = at / GROUP_BASE;
+    const int local = (at - g * GROUP_BASE) + atomicAdd(&fill[r], 1);
+    body_group[s] = g;
+    body_local[s] = local;
+    group_body[(long)g * GROUP_CAP + local] = s;
+    atomicMax(&group_count[g], local + 1);
+}
+
 __device__ __forceinline__ int pair_kind(float shapeA, float shapeB, int count) {
     const bool sa = shapeA > 0.5f, sb = shapeB > 0.5f;
     if (sa && sb) return 0;
@@ -584,11 +712,18 @@ __device__ __forceinline__ int pair_kind(float shapeA, float shapeB, int count) 
     return 1 + min(max(count, 1), 4);
 }
 
+// A pair's path: 1 where its first body is in a small component's group (its second then is too), else 0. Without
+// islands (body_group null) every pair takes the grid phases.
+__device__ __forceinline__ int path_of(const int* body_group, int a, int c) {
+    return body_group != nullptr && c < MOST_ROUNDS && body_group[a] >= 0 ? 1 : 0;
+}
+
 __global__ void k_round_count(const int* __restrict__ touching_n, const int* __restrict__ colour,
                               int* __restrict__ round_count, int* __restrict__ bucket_most, Counters* counters,
                               const int* __restrict__ ta, const int* __restrict__ tb,
                               unsigned* __restrict__ body_colours, const int* __restrict__ tcand,
-                              const float4* __restrict__ head, const float4* __restrict__ half) {
+                              const float4* __restrict__ head, const float4* __restrict__ half,
+                              const int* __restrict__ body_group, int* __restrict__ gr_count) {
     const int total = *touching_n;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         int c = colour[t];
@@ -598,10 +733,14 @@ __global__ void k_round_count(const int* __restrict__ touching_n, const int* __r
         }
         const int count = (int)head[tcand[t]].w;
         const int kind = pair_kind(half[ta[t]].w, half[tb[t]].w, count);
-        atomicAdd(&round_count[c * PAIR_KINDS + kind], 1);
-        atomicMax(&bucket_most[c * PAIR_KINDS + kind], min(max(count, 1), MOST_POINTS));
+        const int path = path_of(body_group, ta[t], c);
+        const int bucket = path * BUCKETS + c * PAIR_KINDS + kind;
+        atomicAdd(&round_count[bucket], 1);
+        atomicMax(&bucket_most[bucket], min(max(count, 1), MOST_POINTS));
+        if (path == 1) atomicAdd(&gr_count[body_group[ta[t]] * GROUP_ROUNDS + c], 1);
         if (c < MOST_ROUNDS) {
             atomicMax(&counters->rounds, c + 1);
+            if (path == 0) atomicMax(&counters->grid_rounds, c + 1);
             atomicOr(&body_colours[ta[t]], 1u << c);
             atomicOr(&body_colours[tb[t]], 1u << c);
         } else {
@@ -618,18 +757,26 @@ __global__ void k_order(const int* __restrict__ touching_n, const int* __restric
                         const int* __restrict__ bucket_pstart, int* __restrict__ round_fill, const int* __restrict__ ta,
                         const int* __restrict__ tcand, const Manifolds m, const float4* __restrict__ imp_t,
                         const float4* __restrict__ impr_t, PairGen now,
-                        const unsigned* __restrict__ body_colours, const float4* __restrict__ half) {
+                        const unsigned* __restrict__ body_colours, const float4* __restrict__ half,
+                        const int* __restrict__ body_group, const int* __restrict__ body_local,
+                        const int* __restrict__ gr_start, int* __restrict__ gr_fill, int2* __restrict__ ilist) {
     const int total = *touching_n;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         int c = colour[t];
         if (c < 0 || c > MOST_ROUNDS) c = MOST_ROUNDS;
         const int kind = pair_kind(half[ta[t]].w, half[now.tb[t]].w, (int)m.head[tcand[t]].w);
-        const int bucket = c * PAIR_KINDS + kind;
+        const int path = path_of(body_group, ta[t], c);
+        const int bucket = path * BUCKETS + c * PAIR_KINDS + kind;
         const int rank = atomicAdd(&round_fill[bucket], 1);
         const int p = bucket_start[bucket] + rank;
         const long first = bucket_pstart[bucket] + (long)rank * bucket_most[bucket];
         now.pos[t] = p;
         now.pstart[p] = (int)first;
+        if (path == 1) {  // the island warps' list: by (group, round), each pair's position and its bodies' places
+            const int gr = body_group[ta[t]] * GROUP_ROUNDS + c;
+            ilist[gr_start[gr] + atomicAdd(&gr_fill[gr], 1)] =
+                make_int2(p, body_local[ta[t]] | body_local[now.tb[t]] << 16);
+        }
         const int cd = tcand[t];
         const float4 head = m.head[cd];
         const int count = (int)head.w;
@@ -651,21 +798,22 @@ __global__ void k_order(const int* __restrict__ touching_n, const int* __restric
 }
 
 // Where each bucket's points begin: its pairs take `most` entries each (every pair of a box-box bucket has the
-// same point count, and sphere pairs have one point, so the points are packed). One thread: BUCKETS entries.
+// same point count, and sphere pairs have one point, so the points are packed). One thread: ALL_BUCKETS entries.
 __global__ void k_bucket_points(const int* __restrict__ round_count, const int* __restrict__ bucket_most,
                                 int* __restrict__ bucket_pstart) {
     if (threadIdx.x != 0) return;
     int at = 0;
-    for (int b = 0; b < BUCKETS; b++) {
+    for (int b = 0; b < ALL_BUCKETS; b++) {
         bucket_pstart[b] = at;
         at += round_count[b] * bucket_most[b];
     }
-    bucket_pstart[BUCKETS] = at;
+    bucket_pstart[ALL_BUCKETS] = at;
 }
 
 // Where each round begins: its first bucket's start.
 __global__ void k_round_starts(const int* __restrict__ bucket_start, int* __restrict__ round_start) {
-    const int r = threadIdx.x;  // bucket_start has BUCKETS + 1 entries: r * PAIR_KINDS <= BUCKETS for r <= 33
+    // The grid phases' rounds (path 0, which comes first): r * PAIR_KINDS <= BUCKETS for r <= 33.
+    const int r = threadIdx.x;
     if (r <= MOST_ROUNDS + 1) round_start[r] = bucket_start[r * PAIR_KINDS];
 }
 
@@ -697,7 +845,15 @@ struct SolveArgs {
     GridBarrier bar;
     unsigned long long* trace;  // null: not traced
     int trace_cap;
+    const int* grid_list;  // the bodies the grid phases move (the rest are the island kernel's); null: every body
+    const int* grid_n;     // their count (device)
 };
+
+// The i-th body of the grid phases, and how many there are.
+__device__ __forceinline__ int grid_bodies(const SolveArgs& A) {
+    return A.grid_list ? *(volatile const int*)A.grid_n : A.n;
+}
+__device__ __forceinline__ int grid_body(const SolveArgs& A, int i) { return A.grid_list ? A.grid_list[i] : i; }
 
 // Body state a solve phase reads and writes goes through L2 (ld/st .cg): under the dependency schedule one
 // body's consecutive items can run on different SMs.
@@ -712,27 +868,15 @@ __device__ __forceinline__ void store_held(const Held& h, const Bodies& b, int s
 
 __device__ __forceinline__ void list_wall_body(const SolveArgs& A, int s, float4 pose, int slot);
 
-// Boxes.positions :299-342, and the body listed for the relax sweeps' walls from where it now is.
-__device__ __forceinline__ void phase_positions(const SolveArgs& A, int slot) {
-    const int stride = gridDim.x * blockDim.x;
-    if (blockIdx.x == 0 && threadIdx.x == 0) A.counters->bar_gen = 0u;  // the dependency schedule's ticket
-    const float h = A.params.w[P_H];
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += stride) {
-        float4 p = __ldcg(&A.b.pose[s]);
-        const float im = p.w;
-        A.version[s] = 0;
-        A.listed[s] = 0;
-        if (!(im > 0.0f)) continue;
-        const float4 v = __ldcg(&A.b.vel[s]);
-        p.x = p.x + h * v.x;
-        p.y = p.y + h * v.y;
-        p.z = p.z + h * v.z;
-        __stcg(&A.b.pose[s], p);
-        const float4 tq = __ldcg(&A.b.turn[s]);
+// Boxes.positions :299-342 for one moving body: x += h v; the turn by the angular velocity at the half step.
+__device__ __forceinline__ void move_body(float4& p, float4& turn, float4 v, float4 l, float4 inv, float h) {
+    p.x = p.x + h * v.x;
+    p.y = p.y + h * v.y;
+    p.z = p.z + h * v.z;
+    {
+        const float4 tq = turn;
         const float q[4] = {tq.x, tq.y, tq.z, tq.w};
-        const float4 l = __ldcg(&A.b.mom[s]);
         const float momentum[3] = {l.x, l.y, l.z};
-        const float4 inv = __ldg(&A.b.inv[s]);
         const float inverse[3] = {inv.x, inv.y, inv.z};
         float omega[3], mid[4], omega_mid[3], end[4];
         {
@@ -754,7 +898,27 @@ __device__ __forceinline__ void phase_positions(const SolveArgs& A, int slot) {
             rotate_by(mid, tw, scaled, omega_mid);
         }
         turned(q, omega_mid, h, end);
-        __stcg(&A.b.turn[s], make_float4(end[0], end[1], end[2], end[3]));
+        turn = make_float4(end[0], end[1], end[2], end[3]);
+    }
+}
+
+// Boxes.positions :299-342, and the body listed for the relax sweeps' walls from where it now is.
+__device__ __forceinline__ void phase_positions(const SolveArgs& A, int slot) {
+    const int stride = gridDim.x * blockDim.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) A.counters->bar_gen = 0u;  // the dependency schedule's ticket
+    const float h = A.params.w[P_H];
+    const int count = grid_bodies(A);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const int s = grid_body(A, i);
+        float4 p = __ldcg(&A.b.pose[s]);
+        const float im = p.w;
+        A.version[s] = 0;
+        A.listed[s] = 0;
+        if (!(im > 0.0f)) continue;
+        float4 turn = __ldcg(&A.b.turn[s]);
+        move_body(p, turn, __ldcg(&A.b.vel[s]), __ldcg(&A.b.mom[s]), __ldg(&A.b.inv[s]), h);
+        __stcg(&A.b.pose[s], p);
+        __stcg(&A.b.turn[s], turn);
         list_wall_body(A, s, p, slot);
     }
 }
@@ -803,7 +967,9 @@ __device__ __forceinline__ void phase_velocities_and_list(const SolveArgs& A, in
     const int stride = gridDim.x * blockDim.x;
     if (blockIdx.x == 0 && threadIdx.x == 0) A.counters->bar_gen = 0u;  // the dependency schedule's ticket
     const float h = A.params.w[P_H];
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += stride) {
+    const int count = grid_bodies(A);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        const int s = grid_body(A, i);
         const float4 pose = A.b.pose[s];
         A.version[s] = 0;
         A.listed[s] = 0;
@@ -972,14 +1138,12 @@ __device__ __forceinline__ void phase_walls(const SolveArgs& A, int sweep, bool 
 // fill: the first sweep of a substep's half (positions fixed until the next positions phase): each point's anchors
 // in the world's frame, its gap and its normal's generalised inverse mass are worked out and kept; the later
 // sweeps of that half read them back (the same values the reference works out again every sweep).
-__device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4, int sweep, bool reverse, bool fill,
-                                           unsigned* track) {
+// solve_points: the pair's points with both bodies held (loaded by the caller, stored after).
+__device__ __forceinline__ void solve_points(const SolveArgs& A, long k, int4 rec4, Held& first, Held& second,
+                                             int sweep, bool reverse, bool fill, unsigned* track) {
     const Params& P = A.params;
     const float4 head = __ldg(&A.pairs.normal[k]);
-    const int ia = rec4.x, ib = rec4.y, count = rec4.z;
-    Held first, second;
-    load_held(first, A.b, ia);
-    load_held(second, A.b, ib);
+    const int ia = rec4.x, count = rec4.z;
     Soft soft(P, false);
     if (first.im == 0.0f || second.im == 0.0f) {
         soft.bias = P.w[P_STATIC_BIAS];
@@ -1059,8 +1223,16 @@ __device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4
             if (sweep != WARM) __stcg(&A.pairs.impr[at], rr);
         }
     }
-    store_held(first, A.b, ia);
-    store_held(second, A.b, ib);
+}
+
+__device__ __forceinline__ void solve_pair(const SolveArgs& A, long k, int4 rec4, int sweep, bool reverse, bool fill,
+                                           unsigned* track) {
+    Held first, second;
+    load_held(first, A.b, rec4.x);
+    load_held(second, A.b, rec4.y);
+    solve_points(A, k, rec4, first, second, sweep, reverse, fill, track);
+    store_held(first, A.b, rec4.x);
+    store_held(second, A.b, rec4.y);
 }
 
 // One round of pairs that share no body (the barrier schedule). A round's pairs lie in kind order (sphere pairs
@@ -1232,7 +1404,12 @@ __device__ __forceinline__ bool converged(const SolveArgs& A, int index) {
 }
 
 __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_solve(SolveArgs A) {
-    const int rounds = *(volatile int*)&A.counters->rounds;
+    const int rounds = *(volatile int*)&A.counters->grid_rounds;
+    if (A.grid_list && grid_bodies(A) == 0) {  // every body is the island kernel's: nothing for the grid phases
+        if (A.used && blockIdx.x == 0 && threadIdx.x == 0)
+            for (int sub = 0; sub < A.substeps; sub++) A.used[2 * sub] = A.used[2 * sub + 1] = A.sweeps;
+        return;
+    }
     Tracer tr{A.trace, A.trace_cap, 0};
     unsigned int epoch = 0;
     tr.mark(TR_START);
@@ -1283,6 +1460,245 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_solve(SolveArgs A) {
         }
     }
     if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) A.counters->trace_len = tr.len;
+}
+
+
+// ------------------------------------------------------------------------------------------------------------
+// The island kernel: whole substeps of the small components, a warp a group, the group's bodies held in shared
+// memory for the step; and the bodies in no placed pair, a thread each. Every operation is the one the grid phases
+// make, in each body's order (velocities; the warm sweep and the solve sweeps, each its rounds then its walls, or
+// backward the walls then the rounds; positions; the relax sweeps), so the results are theirs to the bit.
+
+constexpr int ISLAND_THREADS = 32 * ISLAND_WARPS;
+
+struct IslandArgs {
+    const int* group_body;   // [groups * GROUP_CAP]
+    const int* group_count;  // [groups]
+    const int* gr_start;     // [groups * GROUP_ROUNDS + 1] each (group, round)'s first entry of ilist
+    const int2* ilist;       // position, local ids of first | second << 16
+    const int* free_list;    // bodies in no placed pair
+    const int* island_n;     // bodies in small components
+    int* work;               // items handed out: groups, then runs of 32 lone bodies
+};
+
+struct GroupBodies {  // one warp's group, for the step
+    float4 pose[GROUP_CAP], turn[GROUP_CAP], vel[GROUP_CAP], mom[GROUP_CAP];
+    int id[GROUP_CAP];
+    unsigned listed[GROUP_CAP / 32];  // bodies the walls' sweeps visit until positions next change
+};
+
+__device__ __forceinline__ void load_local(Held& h, const GroupBodies& G, const Bodies& b, int i) {
+    const int s = G.id[i];
+    h.load(G.pose[i], G.turn[i], __ldg(&b.half[s]), G.vel[i], G.mom[i], __ldg(&b.inv[s]));
+}
+__device__ __forceinline__ void store_local(const Held& h, GroupBodies& G, int i) {
+    G.vel[i] = make_float4(h.velocity[0], h.velocity[1], h.velocity[2], 0.0f);
+    G.mom[i] = make_float4(h.momentum[0], h.momentum[1], h.momentum[2], 0.0f);
+}
+
+// Whether the walls' sweeps visit a body until positions next change: as list_wall_body decides.
+__device__ __forceinline__ bool wall_listed(const SolveArgs& A, int s, float4 pose, float4 hw) {
+    const int sc = scene_of(A, s);
+    const float extent[3] = {word_of(A, sc, P_SX), word_of(A, sc, P_SY), word_of(A, sc, P_SZ)};
+    return __ldcg(&A.wmask[s]) != 0ull || near_walls(pose, hw, A.params.w[P_MARGIN], extent) != 0u;
+}
+
+__device__ __forceinline__ void group_velocities(const SolveArgs& A, GroupBodies& G, int nb, float h) {
+    const int lane = threadIdx.x & 31;
+    for (int j = 0; j * 32 < nb; j++) {
+        const int i = j * 32 + lane;
+        bool list = false;
+        if (i < nb) {
+            const int s = G.id[i];
+            const float4 pose = G.pose[i];
+            if (pose.w > 0.0f) {
+                float4 v = G.vel[i];
+                const int sc = scene_of(A, s);
+                v.x = v.x + h * word_of(A, sc, P_GX);
+                v.y = v.y + h * word_of(A, sc, P_GY);
+                v.z = v.z + h * word_of(A, sc, P_GZ);
+                G.vel[i] = v;
+                list = wall_listed(A, s, pose, __ldg(&A.b.half[s]));
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, list);
+        if (lane == 0) G.listed[j] = m;
+    }
+}
+
+__device__ __forceinline__ void group_positions(const SolveArgs& A, GroupBodies& G, int nb, float h) {
+    const int lane = threadIdx.x & 31;
+    for (int j = 0; j * 32 < nb; j++) {
+        const int i = j * 32 + lane;
+        bool list = false;
+        if (i < nb) {
+            const int s = G.id[i];
+            float4 p = G.pose[i];
+            if (p.w > 0.0f) {
+                float4 turn = G.turn[i];
+                move_body(p, turn, G.vel[i], G.mom[i], __ldg(&A.b.inv[s]), h);
+                G.pose[i] = p;
+                G.turn[i] = turn;
+                list = wall_listed(A, s, p, __ldg(&A.b.half[s]));
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, list);
+        if (lane == 0) G.listed[j] = m;
+    }
+}
+
+__device__ __forceinline__ void group_walls(const SolveArgs& A, GroupBodies& G, int nb, int kind, bool reverse,
+                                            unsigned* track) {
+    const int lane = threadIdx.x & 31;
+    for (int j = 0; j * 32 < nb; j++) {
+        const int i = j * 32 + lane;
+        if (i < nb && ((G.listed[j] >> lane) & 1u)) {
+            Held box;
+            load_local(box, G, A.b, i);
+            if (walls_of(A, box, G.id[i], kind, reverse, track)) store_local(box, G, i);
+        }
+    }
+}
+
+// One sweep of a group: its rounds in order, a warp barrier after each (a round's pairs share no body), then the
+// walls; backward, the walls first and the rounds last to first.
+__device__ __forceinline__ void group_sweep(const SolveArgs& A, const IslandArgs& I, GroupBodies& G, int nb,
+                                            const int* gs, unsigned present, int kind, bool reverse, bool fill,
+                                            int index) {
+    const int lane = threadIdx.x & 31;
+    unsigned* track = A.residual ? A.residual + index : nullptr;
+    if (reverse) {
+        group_walls(A, G, nb, kind, true, track);
+        __syncwarp();
+    }
+    for (unsigned left = present; left;) {
+        const int r = reverse ? 31 - __clz(left) : __ffs(left) - 1;
+        left &= ~(1u << r);
+        const int hi = gs[r + 1];
+        for (int idx = gs[r] + lane; idx < hi; idx += 32) {
+            const int2 e = I.ilist[idx];
+            const int la = e.y & 0xffff, lb = e.y >> 16;
+            Held first, second;
+            load_local(first, G, A.b, la);
+            load_local(second, G, A.b, lb);
+            solve_points(A, e.x, __ldg(&A.pairs.pair[e.x]), first, second, kind, reverse, fill, track);
+            store_local(first, G, la);
+            store_local(second, G, lb);
+        }
+        __syncwarp();
+    }
+    if (!reverse) {
+        group_walls(A, G, nb, kind, false, track);
+        __syncwarp();
+    }
+}
+
+__device__ __forceinline__ void run_group(const SolveArgs& A, const IslandArgs& I, GroupBodies& G, int g) {
+    const int lane = threadIdx.x & 31;
+    const int nb = I.group_count[g];
+    for (int i = lane; i < nb; i += 32) {
+        const int s = I.group_body[(long)g * GROUP_CAP + i];
+        G.id[i] = s;
+        G.pose[i] = __ldcg(&A.b.pose[s]);
+        G.turn[i] = __ldcg(&A.b.turn[s]);
+        G.vel[i] = __ldcg(&A.b.vel[s]);
+        G.mom[i] = __ldcg(&A.b.mom[s]);
+    }
+    const int* gs = I.gr_start + (long)g * GROUP_ROUNDS;
+    const unsigned present = __ballot_sync(0xffffffffu, lane < GROUP_ROUNDS && gs[lane + 1] > gs[lane]);
+    __syncwarp();
+    const float h = A.params.w[P_H];
+    const int stride = 2 * A.sweeps + 1;  // residual words a substep
+    for (int sub = 0; sub < A.substeps; sub++) {
+        group_velocities(A, G, nb, h);
+        __syncwarp();
+        const int base = sub * stride;
+        group_sweep(A, I, G, nb, gs, present, WARM, false, true, base);
+        for (int sw = 0; sw < A.sweeps; sw++)
+            group_sweep(A, I, G, nb, gs, present, SOLVE, A.symmetric && sw % 2 == 1, false, base + 1 + sw);
+        group_positions(A, G, nb, h);
+        __syncwarp();
+        const int relax = base + 1 + A.sweeps;
+        for (int sw = 0; sw < A.sweeps; sw++)
+            group_sweep(A, I, G, nb, gs, present, RELAX, A.symmetric && sw % 2 == 1, sw == 0, relax + sw);
+    }
+    for (int i = lane; i < nb; i += 32) {
+        const int s = G.id[i];
+        __stcg(&A.b.pose[s], G.pose[i]);
+        __stcg(&A.b.turn[s], G.turn[i]);
+        __stcg(&A.b.vel[s], G.vel[i]);
+        __stcg(&A.b.mom[s], G.mom[i]);
+    }
+    __syncwarp();  // the shared memory is the next group's
+}
+
+// A body in no placed pair, all substeps in one thread: velocities, its walls in every sweep it is listed for,
+// positions. A fixed body (no inverse mass) is neither moved nor listed.
+__device__ __forceinline__ void walls_alone(const SolveArgs& A, int s, float4 pose, float4 turn, float4 hw, float4& vel,
+                                            float4& mom, float4 inv, int kind, bool reverse, unsigned* track) {
+    Held box;
+    box.load(pose, turn, hw, vel, mom, inv);
+    if (walls_of(A, box, s, kind, reverse, track)) {
+        vel = make_float4(box.velocity[0], box.velocity[1], box.velocity[2], 0.0f);
+        mom = make_float4(box.momentum[0], box.momentum[1], box.momentum[2], 0.0f);
+    }
+}
+
+__device__ __forceinline__ void run_alone(const SolveArgs& A, int s) {
+    float4 pose = __ldcg(&A.b.pose[s]);
+    if (!(pose.w > 0.0f)) return;
+    float4 turn = __ldcg(&A.b.turn[s]), vel = __ldcg(&A.b.vel[s]), mom = __ldcg(&A.b.mom[s]);
+    const float4 hw = __ldg(&A.b.half[s]), inv = __ldg(&A.b.inv[s]);
+    const int sc = scene_of(A, s);
+    const float h = A.params.w[P_H];
+    const float g[3] = {word_of(A, sc, P_GX), word_of(A, sc, P_GY), word_of(A, sc, P_GZ)};
+    const int stride = 2 * A.sweeps + 1;
+    unsigned* res = A.residual;
+    for (int sub = 0; sub < A.substeps; sub++) {
+        vel.x = vel.x + h * g[0];
+        vel.y = vel.y + h * g[1];
+        vel.z = vel.z + h * g[2];
+        const int base = sub * stride;
+        if (wall_listed(A, s, pose, hw)) {
+            walls_alone(A, s, pose, turn, hw, vel, mom, inv, WARM, false, res ? res + base : nullptr);
+            for (int sw = 0; sw < A.sweeps; sw++)
+                walls_alone(A, s, pose, turn, hw, vel, mom, inv, SOLVE, A.symmetric && sw % 2 == 1,
+                            res ? res + base + 1 + sw : nullptr);
+        }
+        move_body(pose, turn, vel, mom, inv, h);
+        if (wall_listed(A, s, pose, hw)) {
+            const int relax = base + 1 + A.sweeps;
+            for (int sw = 0; sw < A.sweeps; sw++)
+                walls_alone(A, s, pose, turn, hw, vel, mom, inv, RELAX, A.symmetric && sw % 2 == 1,
+                            res ? res + relax + sw : nullptr);
+        }
+    }
+    __stcg(&A.b.pose[s], pose);
+    __stcg(&A.b.turn[s], turn);
+    __stcg(&A.b.vel[s], vel);
+    __stcg(&A.b.mom[s], mom);
+}
+
+// Warps take items from a counter: the groups first (the longer chains), then runs of 32 lone bodies.
+__global__ void __launch_bounds__(ISLAND_THREADS, 4) k_islands(SolveArgs A, IslandArgs I) {
+    __shared__ GroupBodies groups[ISLAND_WARPS];
+    GroupBodies& G = groups[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int ngroups = (*I.island_n + GROUP_BASE - 1) / GROUP_BASE;
+    const int nfree = *(volatile const int*)&A.counters->free_n;
+    const int items = ngroups + (nfree + 31) / 32;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(I.work, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= items) break;
+        if (item < ngroups) {
+            run_group(A, I, G, item);
+        } else {
+            const int f = (item - ngroups) * 32 + lane;
+            if (f < nfree) run_alone(A, I.free_list[f]);
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------------------------------
@@ -1647,6 +2063,12 @@ int mark(vxr_box_world* w, int which) {
 // Launches per step, counted as they are made.
 #define LAUNCHED(k) (w->launches += (k))
 
+// Whether a step solves its small components by island warps: on by default; off where a substep's sweep count
+// depends on a residual over every contact (the measuring tolerance), which only the grid phases gather.
+bool islands_on(const vxr_box_world* w) {
+    return w->islands && w->has_grid && !(w->measure && w->tolerance > 0.0f);
+}
+
 // One whole step, enqueued on the world's stream.
 int enqueue_step(vxr_box_world* w) {
     cudaStream_t st = w->stream;
@@ -1714,20 +2136,46 @@ int enqueue_step(vxr_box_world* w) {
             int rc = launch_cooperative(w, (const void*)k_colour, w->colour_blocks, THREADS, args);
             if (rc) return rc;
         }
-        VXR_CUDA(cudaMemsetAsync(w->round_count, 0, sizeof(int) * BUCKETS, st));
-        VXR_CUDA(cudaMemsetAsync(w->bucket_most, 0, sizeof(int) * BUCKETS, st));
-        VXR_CUDA(cudaMemsetAsync(w->round_fill, 0, sizeof(int) * BUCKETS, st));
+        // islands: the components of the placed pairs, the small ones packed into groups
+        const bool isl = islands_on(w);
+        if (isl) {
+            const int* tn = now.tstart + n;
+            k_uf_init<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->parent, w->isl_size, w->isl_fill);
+            k_uf_link<<<tblocks, THREADS, 0, st>>>(tn, w->ta, now.tb, w->colour, w->parent);
+            k_uf_flatten<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->parent, w->comp, w->isl_size);
+            k_classify<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_key,
+                                                                  w->body_group, w->grid_list, w->free_list,
+                                                                  w->counters);
+            exclusive_scan(w->isl_key, w->isl_offset, n, w->scan_tiles, st);
+            VXR_CUDA(cudaMemsetAsync(w->group_count, 0, sizeof(int) * w->groups_max, st));
+            k_assign<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_offset, w->isl_fill,
+                                                                w->body_group, w->body_local, w->group_body,
+                                                                w->group_count);
+            VXR_CUDA(cudaMemsetAsync(w->gr_count, 0, sizeof(int) * (size_t)w->groups_max * GROUP_ROUNDS, st));
+            VXR_CUDA(cudaMemsetAsync(w->gr_fill, 0, sizeof(int) * (size_t)w->groups_max * GROUP_ROUNDS, st));
+            LAUNCHED(5 + 3);  // init, link, flatten, classify, assign, scan
+        }
+        VXR_CUDA(cudaMemsetAsync(w->round_count, 0, sizeof(int) * ALL_BUCKETS, st));
+        VXR_CUDA(cudaMemsetAsync(w->bucket_most, 0, sizeof(int) * ALL_BUCKETS, st));
+        VXR_CUDA(cudaMemsetAsync(w->round_fill, 0, sizeof(int) * ALL_BUCKETS, st));
         VXR_CUDA(cudaMemsetAsync(w->body_colours, 0, sizeof(unsigned) * n, st));
+        const int* groups_of = isl ? w->body_group : nullptr;
         k_round_count<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->round_count, w->bucket_most,
                                                   w->counters, w->ta,
-                                                  now.tb, w->body_colours, w->tcand, w->man.head, w->b.half);
-        exclusive_scan(w->round_count, w->bucket_start, BUCKETS, w->scan_tiles, st);
+                                                  now.tb, w->body_colours, w->tcand, w->man.head, w->b.half,
+                                                  groups_of, w->gr_count);
+        exclusive_scan(w->round_count, w->bucket_start, ALL_BUCKETS, w->scan_tiles, st);
+        if (isl) {
+            exclusive_scan(w->gr_count, w->gr_start, w->groups_max * GROUP_ROUNDS, w->scan_tiles, st);
+            LAUNCHED(3);
+        }
         k_round_starts<<<1, 64, 0, st>>>(w->bucket_start, w->round_start);
         k_bucket_points<<<1, 32, 0, st>>>(w->round_count, w->bucket_most, w->bucket_pstart);
         k_order<<<tblocks, THREADS, 0, st>>>(now.tstart + n, w->colour, w->bucket_start, w->bucket_most,
                                             w->bucket_pstart, w->round_fill, w->ta,
                                             w->tcand, w->man, w->imp_t, w->impr_t, now,
-                                            w->body_colours, w->b.half);
+                                            w->body_colours, w->b.half, groups_of, w->body_local, w->gr_start,
+                                            w->gr_fill, w->ilist);
         LAUNCHED(1 + 3 + 1 + 1 + 1 + 3 + 1 + 1 + 1);  // inc count, scan, inc fill, colour, round count, scan,
                                                     // starts, bucket points, order
         if (w->learn_mode > 0) {
@@ -1781,6 +2229,21 @@ int enqueue_step(vxr_box_world* w) {
         A.bar = barrier_of(w);
         A.trace = w->tracing ? w->trace : nullptr;
         A.trace_cap = w->trace_cap;
+        const bool isl = islands_on(w);
+        A.grid_list = isl ? w->grid_list : nullptr;
+        A.grid_n = isl ? &w->counters->grid_n : nullptr;
+        if (isl) {  // the small components and the lone bodies, then the grid phases for the rest
+            IslandArgs I;
+            I.group_body = w->group_body;
+            I.group_count = w->group_count;
+            I.gr_start = w->gr_start;
+            I.ilist = w->ilist;
+            I.free_list = w->free_list;
+            I.island_n = w->isl_offset + n;
+            I.work = &w->counters->work;
+            k_islands<<<w->island_blocks, ISLAND_THREADS, 0, st>>>(A, I);
+            LAUNCHED(1);
+        }
         VXR_CUDA(cudaMemsetAsync(&w->counters->bar_count, 0, 2 * sizeof(unsigned int), st));
         void* args[] = {(void*)&A};
         int rc = launch_cooperative(w, (const void*)k_solve, w->solve_blocks, SOLVE_THREADS, args);
@@ -1992,12 +2455,15 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     rc |= alloc(w, &w->shown, (size_t)n * SHOWN_STRIDE);
     rc |= alloc(w, &w->counters, 1);
     rc |= alloc(w, &w->totals, 1);
-    rc |= alloc(w, &w->scan_tiles, scan_tiles_for(std::max(n, w->cells)) + 1);
-    rc |= alloc(w, &w->round_count, BUCKETS);
+    // groups the bodies can fill: one a GROUP_BASE placed, plus the last part-filled one
+    w->groups_max = n / GROUP_BASE + 2;
+    rc |= alloc(w, &w->scan_tiles,
+                scan_tiles_for(std::max(std::max(n, w->cells), w->groups_max * GROUP_ROUNDS + 1)) + 1);
+    rc |= alloc(w, &w->round_count, ALL_BUCKETS);
     rc |= alloc(w, &w->round_start, MOST_ROUNDS + 2);
-    rc |= alloc(w, &w->bucket_start, BUCKETS + 1);
-    rc |= alloc(w, &w->bucket_most, BUCKETS);
-    rc |= alloc(w, &w->bucket_pstart, BUCKETS + 1);
+    rc |= alloc(w, &w->bucket_start, ALL_BUCKETS + 1);
+    rc |= alloc(w, &w->bucket_most, ALL_BUCKETS);
+    rc |= alloc(w, &w->bucket_pstart, ALL_BUCKETS + 1);
     rc |= alloc(w, &w->wall_list, n);
     rc |= alloc(w, &w->wall_count, 4 * (size_t)w->substeps);
     rc |= alloc(w, &w->version, n);
@@ -2005,7 +2471,7 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     rc |= alloc(w, &w->body_colours, n);
     rc |= alloc(w, &w->residual, (size_t)w->substeps * (2 * w->sweeps + 1));
     rc |= alloc(w, &w->used, 2 * (size_t)w->substeps);
-    rc |= alloc(w, &w->round_fill, BUCKETS);
+    rc |= alloc(w, &w->round_fill, ALL_BUCKETS);
     if (w->has_grid) {
         rc |= alloc(w, &w->keys, n);
         rc |= alloc(w, &w->cell_count, w->cells);
@@ -2054,6 +2520,22 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
         rc |= alloc(w, &w->inc_start, (size_t)n + 1);
         rc |= alloc(w, &w->inc_fill, n);
         rc |= alloc(w, &w->inc_list, (size_t)w->cap * 2);
+        rc |= alloc(w, &w->parent, n);
+        rc |= alloc(w, &w->comp, n);
+        rc |= alloc(w, &w->isl_size, n);
+        rc |= alloc(w, &w->isl_key, n);
+        rc |= alloc(w, &w->isl_offset, (size_t)n + 1);
+        rc |= alloc(w, &w->isl_fill, n);
+        rc |= alloc(w, &w->body_group, n);
+        rc |= alloc(w, &w->body_local, n);
+        rc |= alloc(w, &w->group_body, (size_t)w->groups_max * GROUP_CAP);
+        rc |= alloc(w, &w->group_count, w->groups_max);
+        rc |= alloc(w, &w->gr_count, (size_t)w->groups_max * GROUP_ROUNDS);
+        rc |= alloc(w, &w->gr_start, (size_t)w->groups_max * GROUP_ROUNDS + 1);
+        rc |= alloc(w, &w->gr_fill, (size_t)w->groups_max * GROUP_ROUNDS);
+        rc |= alloc(w, &w->ilist, w->cap);
+        rc |= alloc(w, &w->grid_list, n);
+        rc |= alloc(w, &w->free_list, n);
     }
     if (rc) return bad(VXR_ECUDA);
     if (cudaMallocHost(&w->host_totals, sizeof(Totals)) != cudaSuccess) return bad(VXR_ECUDA);
@@ -2065,6 +2547,8 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     w->solve_blocks = per_sm * w->sms;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_colour, THREADS, 0);
     w->colour_blocks = std::max(1, per_sm) * w->sms;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_islands, ISLAND_THREADS, 0);
+    w->island_blocks = std::max(1, per_sm) * w->sms;
     // Everything starts at zero, as the reference's buffers do; every orientation the identity.
     cudaStream_t st = w->stream;
     cudaMemsetAsync(w->b.pose, 0, sizeof(float4) * n, st);
@@ -2656,6 +3140,13 @@ int32_t vxr_box_measure(vxr_box_world* w, int32_t residual, int32_t cold_start, 
     return VXR_OK;
 }
 
+int32_t vxr_box_islands(vxr_box_world* w, int32_t enable) {
+    if (!w) return VXR_EINVAL;
+    drop_graph(w);
+    w->islands = enable ? 1 : 0;
+    return VXR_OK;
+}
+
 int32_t vxr_box_residuals(vxr_box_world* w, float* out, int32_t capacity, int32_t* used) {
     if (!w) return -VXR_EINVAL;
     const int count = w->substeps * (2 * w->active_sweeps + 1);
@@ -2694,6 +3185,22 @@ int32_t vxr_box_activity(vxr_box_world* w, int64_t* out4) {
     out4[1] = c.points;
     out4[2] = host[0];
     out4[3] = host[1];
+    return VXR_OK;
+}
+
+int32_t vxr_box_paths(vxr_box_world* w, int32_t* out4) {
+    if (!w || !out4) return VXR_EINVAL;
+    Counters c;
+    int island = 0;
+    VXR_CUDA(cudaMemcpyAsync(&c, w->counters, sizeof(Counters), cudaMemcpyDeviceToHost, w->stream));
+    if (w->has_grid)
+        VXR_CUDA(cudaMemcpyAsync(&island, w->isl_offset + w->n, sizeof(int), cudaMemcpyDeviceToHost, w->stream));
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    const bool isl = islands_on(w);
+    out4[0] = isl ? c.grid_n : w->n;
+    out4[1] = isl ? island : 0;
+    out4[2] = isl ? c.free_n : 0;
+    out4[3] = isl ? (island + GROUP_BASE - 1) / GROUP_BASE : 0;
     return VXR_OK;
 }
 

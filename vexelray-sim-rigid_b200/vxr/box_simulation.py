@@ -281,6 +281,18 @@ class BoxSimulation:
                                            float(tolerance)))
         self.active_sweeps = sweeps or self.sweeps
 
+    def islands(self, enable: bool = True) -> None:
+        """Small components solved by island warps (the default), or every body through the grid-wide phases; the
+        results are the same either way."""
+        self._check(self.L.vxr_box_islands(self.h, int(bool(enable))))
+
+    def paths(self) -> dict:
+        """How the last step was scheduled: bodies through the grid-wide phases, in small components (island warps),
+        in no placed pair (a thread each), and the island groups."""
+        out = np.zeros(4, np.int32)
+        self._check(self.L.vxr_box_paths(self.h, ptr(out)))
+        return {"grid": int(out[0]), "islands": int(out[1]), "alone": int(out[2]), "groups": int(out[3])}
+
     def residuals(self):
         """The last step's per-sweep residuals, shape (substeps, 2 sweeps + 1) (warm, solve..., relax...), and the
         sweeps each half-substep ran, shape (substeps, 2)."""
