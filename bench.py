@@ -194,12 +194,13 @@ LATE_SOLVE_TRAFFIC = {"step": 481, "dram_bytes": 5.17e9, "dram_read_bytes": 3.76
                       "algorithmic_bytes": 7.85e9, "ms": 18.85, "source": "ncu, one launch"}
 
 
-def make_world(scene, device, max_pairs=0, schedule=0, solve_blocks_per_sm=0):
+def make_world(scene, device, max_pairs=0, schedule=0, solve_blocks_per_sm=0, islands=True):
     from vxr.box_simulation import BoxSimulation
     # room for the iteration count measurement's sweeps; the steps run the scene's own
     w = BoxSimulation(scene["bodies"], scene["substeps"], max(scene["sweeps"], ITERATION_CAP), False, scene["grid"],
                       device=device, max_pairs=max_pairs, schedule=schedule, solve_blocks_per_sm=solve_blocks_per_sm)
     w.measure(residual=False, sweeps=scene["sweeps"])
+    w.islands(islands)
     l = [scene["lx"], scene["ly"], scene["lz"]]
     q = [scene["qx"], scene["qy"], scene["qz"], scene["qw"]]
     h = [scene["hx"], scene["hy"], scene["hz"]]
@@ -609,6 +610,7 @@ def run_batched(args):
                               schedule=tune["schedule"], solve_blocks_per_sm=tune["solve_blocks_per_sm"])
         sim.load_state([b[k] for k in scenes.FIELDS], None)
         sim.scene_params(b["params"])
+        sim.islands(tune.get("islands", True))
         return sim
 
     sim = make()
@@ -680,7 +682,8 @@ def run_batched(args):
         "config": {"workload": BATCH_WORKLOAD, "scenes": b["scenes"], "bodies": b["bodies"],
                    "timed_steps": f"{args.warmup + 2}..{args.warmup + 1 + steps}, as {pairs} replays of a two-step graph",
                    "l2": "flushed (256 MiB write) before every replay",
-                   "autotuned": {k: tune[k] for k in ("cell_scale", "solve_blocks_per_sm", "schedule", "cached")},
+                   "autotuned": {k: tune.get(k) for k in ("cell_scale", "solve_blocks_per_sm", "schedule", "islands",
+                                                          "cached")},
                    "parallelism": f"scenes shared out over {world_size} ranks" if world_size > 1 else "single"},
         "phase_ms_per_step": {"broad": phases[0] / 10, "narrow": phases[1] / 10, "colour": phases[2] / 10,
                               "solve": solve_ms},
@@ -876,6 +879,8 @@ def main():
     ap.add_argument("--load-state", default="", help="large scene: start from a state saved by --save-state")
     ap.add_argument("--solve-blocks-per-sm", type=int, default=0, help="solve blocks an SM (0: the library's choice)")
     ap.add_argument("--max-pairs", type=int, default=0, help="pair capacity of the world (0: 32 a body)")
+    ap.add_argument("--no-islands", action="store_true",
+                    help="every body through the grid-wide phases (small components not solved by island warps)")
     ap.add_argument("--workload", default="large-mixed",
                     choices=["large-mixed", "sphere-lattice", "batched-scenes", "towers", "sphere-pile"])
     args = ap.parse_args()
@@ -901,7 +906,7 @@ def main():
         scene = scenes.large_mixed(args.bodies, seed=1 + rank)
     else:  # a smaller case of the same scene: the same body density over a smaller footprint
         scene = scenes.sub_volume(BODIES, args.bodies / BODIES, seed=1 + rank)
-    w = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm)
+    w = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm, not args.no_islands)
     if args.load_state:  # a state saved by --save-state: the 13 moving fields; shapes, masses and params the scene's
         z = np.load(args.load_state)
         moving = [z[f"arr_{i}"] for i in range(13)]
@@ -1014,7 +1019,7 @@ def main():
 
     e2e = None
     if not args.no_e2e:
-        w2 = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm)
+        w2 = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm, not args.no_islands)
         # the step's result read into pinned host arrays, reused every step
         pinned = [torch.empty(scene["bodies"], dtype=torch.float32, pin_memory=True).numpy() for _ in range(13)]
         for _ in range(args.warmup):

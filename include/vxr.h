@@ -114,6 +114,8 @@ int32_t vxr_box_start(vxr_box_world* world, const float* x, const float* y, cons
  * momentum, as core/box/BoxStep.java keeps it; the reference's test fixture writes these buffers directly,
  * vexelray-sim-rigid-core/src/test/java/dev/vexelray/sim/rigid/box/BoxScene.java:141-166). Clears every impulse. */
 int32_t vxr_box_load_state(vxr_box_world* world, const float* const* fields18, const int32_t* params18);
+/* Both starts refuse a state holding a NaN or an infinity with VXR_ENONFINITE and load nothing: such a state is
+ * what the reference's diagnostics flag as broken (core/sphere/SphereDiagnostics.java:48-50). */
 
 /* New parameters from the next step on: replaces BoxSimulation.params (gui/BoxSimulation.java:111-113). */
 int32_t vxr_box_params(vxr_box_world* world, const int32_t* params18);
@@ -169,6 +171,12 @@ int32_t vxr_box_measure(vxr_box_world* world, int32_t residual, int32_t cold_sta
  * apart by warp barriers, and bodies in no placed pair by a thread each; only larger components go through the
  * grid-wide phases. enable = 0: every body goes through the grid-wide phases. A measuring tolerance
  * (vxr_box_measure) runs every body through the grid-wide phases whatever this says. */
+/* The longest a device-wide wait of a step (a grid barrier, a dependency wait) may last, from the next step on; ns
+ * <= 0 restores the default of 2 s. A wait that runs out stops the step: the call returns VXR_ETIMEOUT and the GPU
+ * stays usable (the world's state is then part-way through a step; load a state before stepping again). No
+ * reference counterpart: the reference's host waits on its runner (core/box/BoxStepper.java:62). */
+int32_t vxr_box_wait_limit(vxr_box_world* world, int64_t ns);
+
 int32_t vxr_box_islands(vxr_box_world* world, int32_t enable);
 
 /* How the last step was scheduled: out4 = [bodies through the grid-wide phases, bodies in small components (island
@@ -387,10 +395,18 @@ int32_t vxr_sphere_start(vxr_sphere_world* world, const float* x, const float* y
  * (Spheres.SPHERE order: x y z u v w r im cx cy cz dx dy dz ax ay az tx ty tz qx qy qz qw; a null entry leaves it
  * zero, qw one) and the parameters; the picture's buffer zero. */
 int32_t vxr_sphere_load_state(vxr_sphere_world* world, const float* const* fields24, const int32_t* params13);
+/* Both starts refuse a state holding a NaN or an infinity with VXR_ENONFINITE and load nothing: such a state is
+ * what the reference's diagnostics flag as broken (core/sphere/SphereDiagnostics.java:48-50). */
 /* SphereSimulation.params(int[]) (gui/SphereSimulation.java:181-184): from the next step on. */
 int32_t vxr_sphere_params(vxr_sphere_world* world, const int32_t* params13);
 /* SphereStepper.friction(boolean) (core/sphere/SphereStepper.java:106-112): whether passes run friction rounds. */
 int32_t vxr_sphere_friction(vxr_sphere_world* world, int32_t on);
+/* The rounds a Gauss-Seidel pass run until done may take before the step stops with VXR_EROUNDS, "a pass is still
+ * open" (core/sphere/SphereStepper.java:79,86-88); 0 (the default) is the reference's limit, the list's capacity
+ * plus two cycles of rounds. Each round solves at least the open contact of highest priority, so an honest pass
+ * never reaches the default; a lower limit makes a pass that needs more rounds an error, as the reference's test
+ * does with a runner that never closes (ctest/sphere/SphereStepperTest.java:163-166). */
+int32_t vxr_sphere_round_limit(vxr_sphere_world* world, int32_t rounds);
 
 /* SphereSimulation.stepAndWait() (gui/SphereSimulation.java:196-199): `steps` steps, waiting for them. */
 int32_t vxr_sphere_step(vxr_sphere_world* world, int32_t steps, vxr_sphere_report* report);

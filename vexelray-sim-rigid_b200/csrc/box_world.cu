@@ -174,6 +174,7 @@ struct vxr_box_world {
     int *bucket_most = nullptr, *bucket_pstart = nullptr;  // by bucket: most points of a pair, first point
     // islands (connected components of the placed touching pairs), rebuilt every step
     int islands = 1;                  // small components solved by warps (0: every body through the grid phases)
+    unsigned long long wait_limit_ns = 2000000000ull;  // the longest a device-wide wait may last
     int groups_max = 0;               // groups the bodies can fill
     int *parent = nullptr;            // [n] union-find parent
     int *comp = nullptr;              // [n] each body's component: its root
@@ -2043,7 +2044,7 @@ GridBarrier barrier_of(vxr_box_world* w) {
     g.generation = &w->counters->bar_gen;
     g.abort = &w->counters->abort;
     g.status = &w->counters->status;
-    g.limit_ns = 2000000000ull;  // 2 s: far above any barrier's honest wait
+    g.limit_ns = w->wait_limit_ns;  // 2 s unless set: far above any barrier's honest wait
     return g;
 }
 
@@ -2842,10 +2843,22 @@ int32_t vxr_box_step_graph(vxr_box_world* w, int32_t pairs) {
     return VXR_OK;
 }
 
+// Whether every value of the given host arrays is finite (the state a step may start from).
+bool all_finite(const float* const* fields, int count, int n) {
+    for (int k = 0; k < count; k++)
+        for (int s = 0; s < n; s++)
+            if (!std::isfinite(fields[k][s])) return false;
+    return true;
+}
+
 int32_t vxr_box_load_state(vxr_box_world* w, const float* const* f, const int32_t* params) {
     if (!w || !f) return VXR_EINVAL;
     for (int k = 0; k < 18; k++)
         if (!f[k]) return VXR_EINVAL;
+    if (!all_finite(f, 18, w->n)) {
+        w->error = "a non-finite value in the state: nothing was loaded";
+        return VXR_ENONFINITE;
+    }
     cudaSetDevice(w->device);
     int rc = clear_dynamic(w);
     if (rc) return rc;
@@ -3137,6 +3150,13 @@ int32_t vxr_box_measure(vxr_box_world* w, int32_t residual, int32_t cold_start, 
     w->cold = cold_start ? 1 : 0;
     w->active_sweeps = sweeps > 0 ? sweeps : w->sweeps;
     w->tolerance = tolerance;
+    return VXR_OK;
+}
+
+int32_t vxr_box_wait_limit(vxr_box_world* w, int64_t ns) {
+    if (!w) return VXR_EINVAL;
+    drop_graph(w);
+    w->wait_limit_ns = ns > 0 ? (unsigned long long)ns : 2000000000ull;
     return VXR_OK;
 }
 

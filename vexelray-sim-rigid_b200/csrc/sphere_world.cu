@@ -80,6 +80,7 @@ struct Counts {
 struct Kernel {
     int n, cap, substeps, iterations, solve, rounds, gridded, nx, ny, nz, cells, friction, steps;
     int cluster;  // the blocks form one thread-block cluster: passes are separated by the cluster's barrier
+    int limit;    // rounds a pass may take before it is an error (SphereStepper.step :79)
     float cell;
     SParams p;
     State s;
@@ -901,7 +902,7 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
     unsigned int epoch = 0;
     int cur = read_int(&K.counts->cur);
     const bool gs = K.solve != 0;
-    const int limit = K.cap + 2 * CYCLE;
+    const int limit = K.limit;
     for (int step = 0; step < K.steps; step++) {
         if (gtid == 0) {
             for (int k = 0; k < 4; k++) K.counts->last[k] = 0;
@@ -1163,6 +1164,7 @@ struct vxr_sphere_world {
     std::vector<void*> allocations;
     long long launches = 0;
     int pending = 0;  // a call of steps is in flight
+    int round_limit = 0;  // rounds a pass may take; 0: the reference's, the list's capacity + 2 cycles
 };
 
 namespace {
@@ -1273,6 +1275,7 @@ Kernel kernel_of(vxr_sphere_world* w, int steps) {
     K.friction = w->friction;
     K.steps = steps;
     K.cluster = w->cluster;
+    K.limit = w->round_limit > 0 ? w->round_limit : w->cap + 2 * CYCLE;
     K.cell = w->cell;
     K.p = w->params;
     K.s = w->s;
@@ -1535,9 +1538,23 @@ static int rubs_of(const int32_t* params) {
     return (f[MU_STATIC] + f[MU_KINETIC]) + f[MU_ROLLING] > 0.0f ? 1 : 0;
 }
 
+// Whether every value of the given host arrays (null ones skipped) is finite.
+static bool finite_fields(const float* const* fields, int count, int n) {
+    for (int k = 0; k < count; k++)
+        if (fields[k])
+            for (int s = 0; s < n; s++)
+                if (!std::isfinite(fields[k][s])) return false;
+    return true;
+}
+
 int32_t vxr_sphere_start(vxr_sphere_world* w, const float* x, const float* y, const float* z, const float* u,
                          const float* v, const float* wv, const float* r, const float* im, const int32_t* params) {
     if (!w || !x || !y || !z || !u || !v || !wv || !r || !im || !params) return sfail(w, VXR_EINVAL, "null argument");
+    {
+        const float* given[8] = {x, y, z, u, v, wv, r, im};
+        if (!finite_fields(given, 8, w->n))
+            return sfail(w, VXR_ENONFINITE, "a non-finite value in the state: nothing was loaded");
+    }
     if (w->pending) finish(w, nullptr);
     const float* fields[24] = {x, y, z, u, v, wv, r, im};
     std::vector<float> shown((size_t)w->n * SHOWN, 0.0f);
@@ -1556,6 +1573,8 @@ int32_t vxr_sphere_start(vxr_sphere_world* w, const float* x, const float* y, co
 
 int32_t vxr_sphere_load_state(vxr_sphere_world* w, const float* const* fields24, const int32_t* params) {
     if (!w || !fields24 || !params) return sfail(w, VXR_EINVAL, "null argument");
+    if (!finite_fields(fields24, 24, w->n))
+        return sfail(w, VXR_ENONFINITE, "a non-finite value in the state: nothing was loaded");
     if (w->pending) finish(w, nullptr);
     std::memcpy(w->params.w, params, sizeof(float) * P_COUNT);
     w->friction = rubs_of(params);
@@ -1566,6 +1585,12 @@ int32_t vxr_sphere_params(vxr_sphere_world* w, const int32_t* params) {
     if (!w || !params) return sfail(w, VXR_EINVAL, "null argument");
     std::memcpy(w->params.w, params, sizeof(float) * P_COUNT);
     w->friction = rubs_of(params);
+    return VXR_OK;
+}
+
+int32_t vxr_sphere_round_limit(vxr_sphere_world* w, int32_t rounds) {
+    if (!w || rounds < 0) return sfail(w, VXR_EINVAL, "a round limit is at least 0");
+    w->round_limit = rounds;
     return VXR_OK;
 }
 

@@ -1,6 +1,10 @@
-"""The autotuner for batched scenes: which cell size, solve block shape and colouring schedule step a batch
-fastest on this GPU. No reference counterpart (the reference fixes its cell by BoxBroad.grid's rule,
-core/box/BoxBroad.java:66-68, and has one schedule).
+"""The autotuner for batched scenes: which cell size, solve block shape and schedule of the coloured rounds step a
+batch fastest on this GPU. No reference counterpart (the reference fixes its cell by BoxBroad.grid's rule,
+core/box/BoxBroad.java:66-68, and runs its rounds one dispatch after another, core/box/BoxStep.java:217-231).
+
+The schedule of the rounds has two knobs: whether the small connected components of the placed pairs are solved
+whole by one warp each (islands) or go through the grid-wide phases with the rest, and whether the grid-wide phases
+run each round behind a grid barrier or as a stream of items each waiting for its own bodies (dependency).
 
 The search is timed, not modelled: the batch is stepped once to a representative state (bodies landed and piling),
 then every candidate steps from that same state, a few steps to warm the pair impulses and a few timed with CUDA
@@ -10,7 +14,8 @@ $VXR_TUNE_CACHE, default ~/.cache/vxr-b200/tune.json), so a second run of the sa
 The candidates cannot change a result, only its speed: every cell size is at least the reference's rule (the
 27-cell neighbourhood still holds every pair), and both schedules and every block shape keep each body's order of
 operations. (The one exception, stated for completeness: a body with more than 32 partners keeps the first 32 the
-neighbourhood walk finds, and cell size changes the walk's order.)
+neighbourhood walk finds, and cell size changes the walk's order.) The colouring itself is the reference's greedy
+one in every candidate: its rounds are the reference's, so they are not a knob.
 """
 from __future__ import annotations
 
@@ -27,6 +32,12 @@ from . import boxes as B
 CELL_SCALES = (1.0, 1.25)
 BLOCKS_PER_SM = (1, 2)
 SCHEDULES = (0, 1)
+ISLANDS = (True, False)
+
+
+def candidates():
+    """Every (cell scale, solve blocks an SM, grid schedule, islands) the search times."""
+    return list(itertools.product(CELL_SCALES, BLOCKS_PER_SM, SCHEDULES, ISLANDS))
 
 
 def cache_path() -> str:
@@ -57,11 +68,23 @@ def _fields(batch: dict, state=None):
     return f
 
 
+def make_batch(batch: dict, cand, state=None, device: int = 0):
+    """A batched world of `batch` set up as candidate `cand` (cell scale, solve blocks an SM, grid schedule,
+    islands), from the batch's start or from `state` (its 13 moving fields)."""
+    from .box_simulation import BatchSimulation
+    scale, per_sm, schedule, islands = cand
+    sim = BatchSimulation(batch["counts"], scaled_grids(batch, scale), batch["substeps"], batch["sweeps"],
+                          device=device, schedule=schedule, solve_blocks_per_sm=per_sm)
+    sim.load_state(_fields(batch, state), None)
+    sim.scene_params(batch["params"])
+    sim.islands(islands)
+    return sim
+
+
 def tune_batch(batch: dict, device: int = 0, settle_steps: int = 120, warm_steps: int = 4, timed_steps: int = 6,
                use_cache: bool = True, verbose: bool = False) -> dict:
     """The fastest of CELL_SCALES x BLOCKS_PER_SM x SCHEDULES for this batch on this GPU (cached)."""
     import torch
-    from .box_simulation import BatchSimulation
     name = torch.cuda.get_device_name(device)
     key = _key(batch, name)
     path = cache_path()
@@ -75,21 +98,15 @@ def tune_batch(batch: dict, device: int = 0, settle_steps: int = 120, warm_steps
         if key in cache:
             return dict(cache[key], cached=True)
 
-    def make(scale, per_sm, schedule, state):
-        sim = BatchSimulation(batch["counts"], scaled_grids(batch, scale), batch["substeps"], batch["sweeps"],
-                              device=device, schedule=schedule, solve_blocks_per_sm=per_sm)
-        sim.load_state(_fields(batch, state), None)
-        sim.scene_params(batch["params"])
-        return sim
-
     # a representative state: the batch stepped until its bodies have landed
-    sim = make(1.0, 0, 0, None)
+    sim = make_batch(batch, (1.0, 0, 0, True), None, device)
     sim.step_and_wait(settle_steps)
     state = sim.state()
     sim.close()
     trials = []
-    for scale, per_sm, schedule in itertools.product(CELL_SCALES, BLOCKS_PER_SM, SCHEDULES):
-        sim = make(scale, per_sm, schedule, state)
+    for cand in candidates():
+        scale, per_sm, schedule, islands = cand
+        sim = make_batch(batch, cand, state, device)
         sim.step_and_wait(warm_steps)
         stream = torch.cuda.ExternalStream(sim.stream)
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -100,12 +117,14 @@ def tune_batch(batch: dict, device: int = 0, settle_steps: int = 120, warm_steps
         torch.cuda.synchronize()
         ms = start.elapsed_time(end) / timed_steps
         sim.close()
-        trials.append({"cell_scale": scale, "solve_blocks_per_sm": per_sm, "schedule": schedule, "ms_per_step": ms})
+        trials.append({"cell_scale": scale, "solve_blocks_per_sm": per_sm, "schedule": schedule, "islands": islands,
+                       "ms_per_step": ms})
         if verbose:
             print(trials[-1])
     best = min(trials, key=lambda t: t["ms_per_step"])
     result = {"cell_scale": best["cell_scale"], "solve_blocks_per_sm": best["solve_blocks_per_sm"],
-              "schedule": best["schedule"], "ms_per_step": best["ms_per_step"], "trials": trials,
+              "schedule": best["schedule"], "islands": best["islands"], "ms_per_step": best["ms_per_step"],
+              "trials": trials,
               "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
     if use_cache:
         cache[key] = result

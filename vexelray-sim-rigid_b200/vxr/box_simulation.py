@@ -281,6 +281,11 @@ class BoxSimulation:
                                            float(tolerance)))
         self.active_sweeps = sweeps or self.sweeps
 
+    def wait_limit(self, ns: int = 0) -> None:
+        """The longest a device-wide wait of a step may last (0: the default of 2 s); past it the step stops with
+        VXR_ETIMEOUT."""
+        self._check(self.L.vxr_box_wait_limit(self.h, int(ns)))
+
     def islands(self, enable: bool = True) -> None:
         """Small components solved by island warps (the default), or every body through the grid-wide phases; the
         results are the same either way."""

@@ -72,6 +72,11 @@ class SphereSimulation:
     def friction(self, on: bool) -> None:
         self._check(lib().vxr_sphere_friction(self._h, int(bool(on))))
 
+    def round_limit(self, rounds: int = 0) -> None:
+        """The rounds a pass run until done may take before the step is an error (VXR_EROUNDS); 0: the
+        reference's limit, the list's capacity plus two cycles."""
+        self._check(lib().vxr_sphere_round_limit(self._h, int(rounds)))
+
     def step_and_wait(self, steps: int = 1) -> Report:
         r = SphereReport()
         self._check(lib().vxr_sphere_step(self._h, steps, ctypes.byref(r)))
