@@ -179,9 +179,10 @@ int32_t vxr_box_wait_limit(vxr_box_world* world, int64_t ns);
 
 int32_t vxr_box_islands(vxr_box_world* world, int32_t enable);
 
-/* How the last step was scheduled: out4 = [bodies through the grid-wide phases, bodies in small components (island
- * warps), bodies in no placed pair (a thread each), island groups]. With islands off: [bodies, 0, 0, 0]. */
-int32_t vxr_box_paths(vxr_box_world* world, int32_t* out4);
+/* How the last step was scheduled: out5 = [bodies through the grid-wide phases, bodies in small components (island
+ * warps), bodies in no placed pair (a thread each), island groups, bodies of the largest component]. With islands
+ * off: [bodies, 0, 0, 0, 0]. */
+int32_t vxr_box_paths(vxr_box_world* world, int32_t* out5);
 
 /* The last step's per-sweep residuals, substep by substep: the warm sweep, the solve sweeps, the relax sweeps
  * (substeps * (2 sweeps + 1) values). A sweep's residual is the largest positional correction its updates made at any

@@ -107,6 +107,7 @@ struct Counters {  // device-side counts of a step
     int grid_n;       // bodies the grid phases move (components beyond a warp)
     int free_n;       // bodies in no placed pair
     int work;         // the island kernel's work counter
+    int largest;      // bodies of the largest component
 };
 
 struct Totals {  // accumulated over the steps of one vxr_box_step call
@@ -186,6 +187,7 @@ struct vxr_box_world {
     int *body_local = nullptr;        // [n] its place in the group
     int *group_body = nullptr;        // [groups_max * GROUP_CAP] each group's bodies
     int *group_count = nullptr;       // [groups_max]
+    int *group_base = nullptr;        // [groups_max] the place of each group's first component
     int *gr_count = nullptr, *gr_start = nullptr, *gr_fill = nullptr;  // by (group, round)
     int2* ilist = nullptr;            // [cap] island pairs by (group, round): round-order position, local ids
     int *grid_list = nullptr, *free_list = nullptr;  // [n] bodies of the grid phases; bodies in no placed pair
@@ -675,6 +677,7 @@ __global__ void k_classify(int n, const int* __restrict__ root, const int* __res
     if (s >= n) return;
     const int r = root[s];
     const int m = size[r];
+    if (r == s && m > 1) atomicMax(&counters->largest, m);
     int k = 0;
     if (m == 1) {
         body_group[s] = -1;
@@ -688,10 +691,24 @@ __global__ void k_classify(int n, const int* __restrict__ root, const int* __res
     key[s] = k;
 }
 
-// A small component's bodies: the group its root's place falls in, and places in that group one after another.
+// Where each group's bodies begin: the place of its first component (a component that began in the group before may
+// reach past the group's GROUP_BASE boundary, so a group's places start at its own first component, not there).
+__global__ void k_group_base(int n, const int* __restrict__ root, const int* __restrict__ size,
+                             const int* __restrict__ offset, int* __restrict__ group_base) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n || root[s] != s) return;
+    const int m = size[s];
+    if (m == 1 || m > ISLAND_MOST) return;
+    const int at = offset[s];
+    atomicMin(&group_base[at / GROUP_BASE], at);
+}
+
+// A small component's bodies: the group its root's place falls in, and places in that group one after another from
+// the group's first (the group's components lie end to end: its places are 0 .. its body count - 1).
 __global__ void k_assign(int n, const int* __restrict__ root, const int* __restrict__ size,
-                         const int* __restrict__ offset, int* __restrict__ fill, int* __restrict__ body_group,
-                         int* __restrict__ body_local, int* __restrict__ group_body, int* __restrict__ group_count) {
+                         const int* __restrict__ offset, const int* __restrict__ group_base, int* __restrict__ fill,
+                         int* __restrict__ body_group, int* __restrict__ body_local, int* __restrict__ group_body,
+                         int* __restrict__ group_count) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const int r = root[s];
@@ -699,7 +716,7 @@ __global__ void k_assign(int n, const int* __restrict__ root, const int* __restr
     if (m == 1 || m > ISLAND_MOST) return;
     const int at = offset[r];
     const int g = at / GROUP_BASE;
-    const int local = (at - g * GROUP_BASE) + atomicAdd(&fill[r], 1);
+    const int local = (at - group_base[g]) + atomicAdd(&fill[r], 1);
     body_group[s] = g;
     body_local[s] = local;
     group_body[(long)g * GROUP_CAP + local] = s;
@@ -935,6 +952,20 @@ __device__ __forceinline__ float word_of(const SolveArgs& A, int sc, int i) {
     return sc < 0 ? A.params.w[i] : __ldg(&A.scene_params[sc].w[i]);
 }
 
+// Wall, roll and contact-point records: a record one thread alone reads and writes for a whole step (OWN, the island
+// kernel's) goes through L1 with plain accesses; one that consecutive items of a step may take on different SMs (the
+// grid phases') goes through L2 (ld/st .cg).
+template <bool OWN, class T>
+__device__ __forceinline__ T ld_rec(const T* p) {
+    if (OWN) return *p;
+    return __ldcg(p);
+}
+template <bool OWN, class T>
+__device__ __forceinline__ void st_rec(T* p, T v) {
+    if (OWN) *p = v;
+    else __stcg(p, v);
+}
+
 // Which walls a body may touch: bit w set where the body's bounding sphere comes within the margin of wall w
 // (a bound that holds through f32 rounding: every corner's gap to a wall not in the set exceeds the margin).
 __device__ __forceinline__ unsigned near_walls(float4 pose, float4 hw, float margin, const float* extent) {
@@ -988,6 +1019,7 @@ __device__ __forceinline__ void phase_velocities_and_list(const SolveArgs& A, in
 // Boxes.walls :357-416 for one body held in registers: its corners (a sphere: its nearest point) against the six
 // walls. A wall the body is far from, with no impulse held against it, is skipped: its contacts would neither
 // start nor apply. Returns whether anything was applied (the caller then stores the body).
+template <bool OWN = false>
 __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, int sweep, bool reverse,
                                          unsigned* track = nullptr) {
     const Params& P = A.params;
@@ -995,7 +1027,7 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
     const int sc = scene_of(A, s);
     const float extent[3] = {word_of(A, sc, P_SX), word_of(A, sc, P_SY), word_of(A, sc, P_SZ)};
     const float mu_rolling = word_of(A, sc, P_MU_ROLLING);
-    unsigned long long mask = __ldcg(&A.wmask[s]);
+    unsigned long long mask = ld_rec<OWN>(&A.wmask[s]);
     const float4 pose = make_float4(box.at[0], box.at[1], box.at[2], box.im);
     const float4 hw = make_float4(box.half[0], box.half[1], box.half[2], box.shape);
     const bool sphere = hw.w > 0.5f;
@@ -1032,19 +1064,19 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
             float4 rec = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             const long at = (long)s * WALL_RECORDS + wall * 8;
             if (need) {
-                rec = held ? __ldcg(&A.wall[at]) : rec;
+                rec = held ? ld_rec<OWN>(&A.wall[at]) : rec;
                 contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft, -1.0f, track);
                 if (sweep != WARM) {
-                    __stcg(&A.wall[at], rec);
+                    st_rec<OWN>(&A.wall[at], rec);
                     mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
                 }
                 touched = true;
             }
             if (rolled || (sweep != WARM && nonzero_bits(rec))) {
-                float4 rr = rolled ? __ldcg(&A.wroll[(long)s * 6 + wall]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                float4 rr = rolled ? ld_rec<OWN>(&A.wroll[(long)s * 6 + wall]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 roll<false>(sweep, box, box, box.half[0], rec.x, rr, mu_rolling);
                 if (sweep != WARM) {
-                    __stcg(&A.wroll[(long)s * 6 + wall], rr);
+                    st_rec<OWN>(&A.wroll[(long)s * 6 + wall], rr);
                     mask = nonzero_bits(rr) ? (mask | (1ull << rbit)) : (mask & ~(1ull << rbit));
                 }
                 touched = true;
@@ -1086,14 +1118,14 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
         };
         bit = next_bit(todo);
         float4 ahead = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (bit >= 0 && ((mask >> bit) & 1ull)) ahead = __ldcg(&A.wall[(long)s * WALL_RECORDS + bit]);
+        if (bit >= 0 && ((mask >> bit) & 1ull)) ahead = ld_rec<OWN>(&A.wall[(long)s * WALL_RECORDS + bit]);
         while (bit >= 0) {
             todo &= ~(1ull << bit);
             const int wall = bit / 8, c = bit % 8;
             const bool held = (mask >> bit) & 1ull;
             const float4 loaded = held ? ahead : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             const int after = next_bit(todo);
-            if (after >= 0 && ((mask >> after) & 1ull)) ahead = __ldcg(&A.wall[(long)s * WALL_RECORDS + after]);
+            if (after >= 0 && ((mask >> after) & 1ull)) ahead = ld_rec<OWN>(&A.wall[(long)s * WALL_RECORDS + after]);
             const int axis = wall / 2;
             const bool high = wall % 2 == 1;
             float n[3];
@@ -1106,14 +1138,14 @@ __device__ __forceinline__ bool walls_of(const SolveArgs& A, Held& box, int s, i
             float4 rec = loaded;
             contact<false>(sweep, gap, n, box, nullptr, box, r, rec, soft, -1.0f, track);
             if (sweep != WARM) {
-                __stcg(&A.wall[(long)s * WALL_RECORDS + bit], rec);
+                st_rec<OWN>(&A.wall[(long)s * WALL_RECORDS + bit], rec);
                 mask = nonzero_bits(rec) ? (mask | (1ull << bit)) : (mask & ~(1ull << bit));
             }
             touched = true;
             bit = after;
         }
     }
-    if (touched) __stcg(&A.wmask[s], mask);
+    if (touched) st_rec<OWN>(&A.wmask[s], mask);
     return touched;
 }
 
@@ -1140,6 +1172,7 @@ __device__ __forceinline__ void phase_walls(const SolveArgs& A, int sweep, bool 
 // in the world's frame, its gap and its normal's generalised inverse mass are worked out and kept; the later
 // sweeps of that half read them back (the same values the reference works out again every sweep).
 // solve_points: the pair's points with both bodies held (loaded by the caller, stored after).
+template <bool OWN = false>
 __device__ __forceinline__ void solve_points(const SolveArgs& A, long k, int4 rec4, Held& first, Held& second,
                                              int sweep, bool reverse, bool fill, unsigned* track) {
     const Params& P = A.params;
@@ -1167,9 +1200,9 @@ __device__ __forceinline__ void solve_points(const SolveArgs& A, long k, int4 re
     float4 next_a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), next_b = next_a, next_imp = next_a;
     if (!fill && count > 0) {
         const long at0 = base + (reverse ? count - 1 : 0);
-        next_a = __ldcg(&A.pairs.prepA[at0]);
-        next_b = __ldcg(&A.pairs.prepB[at0]);
-        next_imp = __ldcg(&A.pairs.imp[at0]);
+        next_a = ld_rec<OWN>(&A.pairs.prepA[at0]);
+        next_b = ld_rec<OWN>(&A.pairs.prepB[at0]);
+        next_imp = ld_rec<OWN>(&A.pairs.imp[at0]);
     }
     for (int order = 0; order < MOST_POINTS; order++) {
         const int slot = reverse ? MOST_POINTS - 1 - order : order;
@@ -1196,32 +1229,32 @@ __device__ __forceinline__ void solve_points(const SolveArgs& A, long k, int4 re
                   ((second.at[1] + rB[1]) - (first.at[1] + rA[1])) * n[1];
             gap = gap + ((second.at[2] + rB[2]) - (first.at[2] + rA[2])) * n[2];
             kn = mass_along<true>(first, rA, second, rB, n);
-            __stcg(&A.pairs.prepA[at], make_float4(rA[0], rA[1], rA[2], gap));
-            __stcg(&A.pairs.prepB[at], make_float4(rB[0], rB[1], rB[2], kn));
-            rec = __ldcg(&A.pairs.imp[at]);
+            st_rec<OWN>(&A.pairs.prepA[at], make_float4(rA[0], rA[1], rA[2], gap));
+            st_rec<OWN>(&A.pairs.prepB[at], make_float4(rB[0], rB[1], rB[2], kn));
+            rec = ld_rec<OWN>(&A.pairs.imp[at]);
         } else {
             const float4 pa = next_a, pb = next_b;
             rec = next_imp;
             const int later = reverse ? slot - 1 : slot + 1;
             if (later >= 0 && later < count) {
                 const long at1 = base + later;
-                next_a = __ldcg(&A.pairs.prepA[at1]);
-                next_b = __ldcg(&A.pairs.prepB[at1]);
-                next_imp = __ldcg(&A.pairs.imp[at1]);
+                next_a = ld_rec<OWN>(&A.pairs.prepA[at1]);
+                next_b = ld_rec<OWN>(&A.pairs.prepB[at1]);
+                next_imp = ld_rec<OWN>(&A.pairs.imp[at1]);
             }
             rA[0] = pa.x; rA[1] = pa.y; rA[2] = pa.z; gap = pa.w;
             rB[0] = pb.x; rB[1] = pb.y; rB[2] = pb.z; kn = pb.w;
         }
         contact<true>(sweep, gap, n, first, rA, second, rB, rec, soft, kn, track);
-        if (sweep != WARM) __stcg(&A.pairs.imp[at], rec);
+        if (sweep != WARM) st_rec<OWN>(&A.pairs.imp[at], rec);
         if (anySphere) {
             float radius = second.half[0];
             if (first.sphere()) radius = first.half[0];
             if (first.sphere() && second.sphere())
                 radius = (first.half[0] * second.half[0]) / (first.half[0] + second.half[0]);
-            float4 rr = __ldcg(&A.pairs.impr[at]);
+            float4 rr = ld_rec<OWN>(&A.pairs.impr[at]);
             roll<true>(sweep, first, second, radius, rec.x, rr, mu_rolling);
-            if (sweep != WARM) __stcg(&A.pairs.impr[at], rr);
+            if (sweep != WARM) st_rec<OWN>(&A.pairs.impr[at], rr);
         }
     }
 }
@@ -1556,7 +1589,7 @@ __device__ __forceinline__ void group_walls(const SolveArgs& A, GroupBodies& G, 
         if (i < nb && ((G.listed[j] >> lane) & 1u)) {
             Held box;
             load_local(box, G, A.b, i);
-            if (walls_of(A, box, G.id[i], kind, reverse, track)) store_local(box, G, i);
+            if (walls_of<true>(A, box, G.id[i], kind, reverse, track)) store_local(box, G, i);
         }
     }
 }
@@ -1577,12 +1610,12 @@ __device__ __forceinline__ void group_sweep(const SolveArgs& A, const IslandArgs
         left &= ~(1u << r);
         const int hi = gs[r + 1];
         for (int idx = gs[r] + lane; idx < hi; idx += 32) {
-            const int2 e = I.ilist[idx];
+            const int2 e = __ldg(&I.ilist[idx]);
             const int la = e.y & 0xffff, lb = e.y >> 16;
             Held first, second;
             load_local(first, G, A.b, la);
             load_local(second, G, A.b, lb);
-            solve_points(A, e.x, __ldg(&A.pairs.pair[e.x]), first, second, kind, reverse, fill, track);
+            solve_points<true>(A, e.x, __ldg(&A.pairs.pair[e.x]), first, second, kind, reverse, fill, track);
             store_local(first, G, la);
             store_local(second, G, lb);
         }
@@ -1639,7 +1672,7 @@ __device__ __forceinline__ void walls_alone(const SolveArgs& A, int s, float4 po
                                             float4& mom, float4 inv, int kind, bool reverse, unsigned* track) {
     Held box;
     box.load(pose, turn, hw, vel, mom, inv);
-    if (walls_of(A, box, s, kind, reverse, track)) {
+    if (walls_of<true>(A, box, s, kind, reverse, track)) {
         vel = make_float4(box.velocity[0], box.velocity[1], box.velocity[2], 0.0f);
         mom = make_float4(box.momentum[0], box.momentum[1], box.momentum[2], 0.0f);
     }
@@ -2149,12 +2182,15 @@ int enqueue_step(vxr_box_world* w) {
                                                                   w->counters);
             exclusive_scan(w->isl_key, w->isl_offset, n, w->scan_tiles, st);
             VXR_CUDA(cudaMemsetAsync(w->group_count, 0, sizeof(int) * w->groups_max, st));
-            k_assign<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_offset, w->isl_fill,
-                                                                w->body_group, w->body_local, w->group_body,
-                                                                w->group_count);
+            VXR_CUDA(cudaMemsetAsync(w->group_base, 0x7f, sizeof(int) * w->groups_max, st));
+            k_group_base<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_offset,
+                                                                    w->group_base);
+            k_assign<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_offset,
+                                                                w->group_base, w->isl_fill, w->body_group,
+                                                                w->body_local, w->group_body, w->group_count);
             VXR_CUDA(cudaMemsetAsync(w->gr_count, 0, sizeof(int) * (size_t)w->groups_max * GROUP_ROUNDS, st));
             VXR_CUDA(cudaMemsetAsync(w->gr_fill, 0, sizeof(int) * (size_t)w->groups_max * GROUP_ROUNDS, st));
-            LAUNCHED(5 + 3);  // init, link, flatten, classify, assign, scan
+            LAUNCHED(6 + 3);  // init, link, flatten, classify, group base, assign, scan
         }
         VXR_CUDA(cudaMemsetAsync(w->round_count, 0, sizeof(int) * ALL_BUCKETS, st));
         VXR_CUDA(cudaMemsetAsync(w->bucket_most, 0, sizeof(int) * ALL_BUCKETS, st));
@@ -2531,6 +2567,7 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
         rc |= alloc(w, &w->body_local, n);
         rc |= alloc(w, &w->group_body, (size_t)w->groups_max * GROUP_CAP);
         rc |= alloc(w, &w->group_count, w->groups_max);
+        rc |= alloc(w, &w->group_base, w->groups_max);
         rc |= alloc(w, &w->gr_count, (size_t)w->groups_max * GROUP_ROUNDS);
         rc |= alloc(w, &w->gr_start, (size_t)w->groups_max * GROUP_ROUNDS + 1);
         rc |= alloc(w, &w->gr_fill, (size_t)w->groups_max * GROUP_ROUNDS);
@@ -3208,8 +3245,9 @@ int32_t vxr_box_activity(vxr_box_world* w, int64_t* out4) {
     return VXR_OK;
 }
 
-int32_t vxr_box_paths(vxr_box_world* w, int32_t* out4) {
-    if (!w || !out4) return VXR_EINVAL;
+int32_t vxr_box_paths(vxr_box_world* w, int32_t* out5) {
+    if (!w || !out5) return VXR_EINVAL;
+    int32_t* out4 = out5;
     Counters c;
     int island = 0;
     VXR_CUDA(cudaMemcpyAsync(&c, w->counters, sizeof(Counters), cudaMemcpyDeviceToHost, w->stream));
@@ -3221,6 +3259,7 @@ int32_t vxr_box_paths(vxr_box_world* w, int32_t* out4) {
     out4[1] = isl ? island : 0;
     out4[2] = isl ? c.free_n : 0;
     out4[3] = isl ? (island + GROUP_BASE - 1) / GROUP_BASE : 0;
+    out5[4] = isl ? c.largest : 0;
     return VXR_OK;
 }
 

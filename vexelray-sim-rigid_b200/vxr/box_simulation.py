@@ -294,9 +294,10 @@ class BoxSimulation:
     def paths(self) -> dict:
         """How the last step was scheduled: bodies through the grid-wide phases, in small components (island warps),
         in no placed pair (a thread each), and the island groups."""
-        out = np.zeros(4, np.int32)
+        out = np.zeros(5, np.int32)
         self._check(self.L.vxr_box_paths(self.h, ptr(out)))
-        return {"grid": int(out[0]), "islands": int(out[1]), "alone": int(out[2]), "groups": int(out[3])}
+        return {"grid": int(out[0]), "islands": int(out[1]), "alone": int(out[2]), "groups": int(out[3]),
+                "largest": int(out[4])}
 
     def residuals(self):
         """The last step's per-sweep residuals, shape (substeps, 2 sweeps + 1) (warm, solve..., relax...), and the
