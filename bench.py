@@ -880,7 +880,7 @@ def main():
     ap.add_argument("--solve-blocks-per-sm", type=int, default=0, help="solve blocks an SM (0: the library's choice)")
     ap.add_argument("--max-pairs", type=int, default=0, help="pair capacity of the world (0: 32 a body)")
     ap.add_argument("--no-islands", action="store_true",
-                    help="every body through the grid-wide phases (small components not solved by island warps)")
+                    help="every body through the grid-wide phases (small components not solved by island blocks)")
     ap.add_argument("--workload", default="large-mixed",
                     choices=["large-mixed", "sphere-lattice", "batched-scenes", "towers", "sphere-pile"])
     args = ap.parse_args()

@@ -167,9 +167,9 @@ int32_t vxr_box_measure(vxr_box_world* world, int32_t residual, int32_t cold_sta
 
 /* How the substeps are scheduled, from the next step on; no reference counterpart, the results are the same either
  * way (the reference's per-body order, core/box/BoxStep.java:199-231). enable = 1 (the default): the connected
- * components of the placed touching pairs of at most 64 bodies are solved whole by one warp each, their rounds
- * apart by warp barriers, and bodies in no placed pair by a thread each; only larger components go through the
- * grid-wide phases. enable = 0: every body goes through the grid-wide phases. A measuring tolerance
+ * components of the placed touching pairs of at most 256 bodies are solved whole by one thread block each (several
+ * components a block, up to 511 bodies, held in shared memory for the step), their rounds apart by block barriers,
+ * and bodies in no placed pair by a thread each; only larger components go through the grid-wide phases. enable = 0: every body goes through the grid-wide phases. A measuring tolerance
  * (vxr_box_measure) runs every body through the grid-wide phases whatever this says. */
 /* The longest a device-wide wait of a step (a grid barrier, a dependency wait) may last, from the next step on; ns
  * <= 0 restores the default of 2 s. A wait that runs out stops the step: the call returns VXR_ETIMEOUT and the GPU
@@ -180,7 +180,7 @@ int32_t vxr_box_wait_limit(vxr_box_world* world, int64_t ns);
 int32_t vxr_box_islands(vxr_box_world* world, int32_t enable);
 
 /* How the last step was scheduled: out5 = [bodies through the grid-wide phases, bodies in small components (island
- * warps), bodies in no placed pair (a thread each), island groups, bodies of the largest component]. With islands
+ * blocks), bodies in no placed pair (a thread each), island groups, bodies of the largest component]. With islands
  * off: [bodies, 0, 0, 0, 0]. */
 int32_t vxr_box_paths(vxr_box_world* world, int32_t* out5);
 

@@ -1,11 +1,11 @@
-"""Islands: the small connected components of a step's placed touching pairs solved whole by one warp each (and
-bodies in no placed pair by a thread each), apart from the grid-wide phases that the larger components go through.
+"""Islands: the small connected components of a step's placed touching pairs solved whole by one thread block each
+(and bodies in no placed pair by a thread each), apart from the grid-wide phases that the larger components go through.
 
 The reference's order of operations is a per-body order (core/box/BoxStep.java:199-231: each sweep every round,
 then the walls), and bodies of different components share no pair, so the schedule changes no result. Checked to the
 bit: the large mixed scene's own generator on a 16,384-body part of its volume, stepped with islands and without,
 through the drop (small islands in the air, lone bodies on the floor and at the walls); a crowded drop in which a
-pile larger than a warp's component forms beside small islands; and against the oracle over the first steps.
+pile larger than a block's component forms beside small islands; and against the oracle over the first steps.
 """
 import numpy as np
 import pytest
@@ -69,7 +69,7 @@ def test_islands_and_grid_phases_agree_through_the_drop():
 
 
 def test_a_pile_beside_islands_matches_the_grid_phases():
-    """A crowded drop into a low box: a pile larger than a warp's component forms within a few steps beside small
+    """A crowded drop into a low box: a pile larger than a block's component forms within a few steps beside small
     islands and lone bodies, so both schedules run in the same step; equal to the bit."""
     sc = scenes.large_mixed(4096, seed=9, volume=(24.0, 6.0, 24.0), height=12.0)
     a = gpu_world(sc, islands=True)

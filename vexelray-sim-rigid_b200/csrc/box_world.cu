@@ -45,17 +45,18 @@ constexpr int SOLVE_THREADS = 256;
 constexpr int PAIR_KINDS = 6;
 constexpr int BUCKETS = (MOST_ROUNDS + 1) * PAIR_KINDS;
 // Pairs are bucketed by path, then round, then kind: path 0 the pairs the grid phases solve (bodies of a component
-// too large for one warp, and every unplaced pair), path 1 the pairs of the small components the island warps solve.
+// too large for one block, and every unplaced pair), path 1 the pairs of the small components the island blocks solve.
 constexpr int ALL_BUCKETS = 2 * BUCKETS;
 // Islands: connected components of the placed touching pairs. A component of at most ISLAND_MOST bodies is solved
-// whole by one warp, its rounds apart by warp barriers; larger ones go through the grid phases. Components are packed
-// into groups in order of their roots: a group takes components until GROUP_BASE bodies have been placed, so it holds
-// at most GROUP_BASE + ISLAND_MOST - 1 bodies.
-constexpr int ISLAND_MOST = 64;
-constexpr int GROUP_BASE = 64;
-constexpr int GROUP_CAP = 128;
-constexpr int GROUP_ROUNDS = MOST_ROUNDS;  // (group, round) lists: placed pairs only
-constexpr int ISLAND_WARPS = 4;            // groups a block of the island kernel runs at once
+// whole by one block, its bodies in shared memory, its rounds apart by block barriers; larger ones go through the grid
+// phases. Components are packed into groups in order of their roots: a group takes components until GROUP_BASE bodies
+// have been placed, so it holds at most GROUP_BASE + ISLAND_MOST - 1 bodies.
+constexpr int ISLAND_MOST = 256;
+constexpr int GROUP_BASE = 256;
+constexpr int GROUP_CAP = 512;
+constexpr int GROUP_ROUNDS = MOST_ROUNDS;                // placed pairs only
+constexpr int GROUP_LISTS = GROUP_ROUNDS * PAIR_KINDS;  // a group's pairs listed by (round, kind)
+constexpr int ISLAND_THREADS = 256;                      // a block a group
 
 // ------------------------------------------------------------------------------------------------------------
 // Device buffers of a world.
@@ -188,8 +189,8 @@ struct vxr_box_world {
     int *group_body = nullptr;        // [groups_max * GROUP_CAP] each group's bodies
     int *group_count = nullptr;       // [groups_max]
     int *group_base = nullptr;        // [groups_max] the place of each group's first component
-    int *gr_count = nullptr, *gr_start = nullptr, *gr_fill = nullptr;  // by (group, round)
-    int2* ilist = nullptr;            // [cap] island pairs by (group, round): round-order position, local ids
+    int *gr_count = nullptr, *gr_start = nullptr, *gr_fill = nullptr;  // by (group, round, kind)
+    int2* ilist = nullptr;            // [cap] island pairs by (group, round, kind): round-order position, local ids
     int *grid_list = nullptr, *free_list = nullptr;  // [n] bodies of the grid phases; bodies in no placed pair
     Counters* counters = nullptr;
     Totals* totals = nullptr;
@@ -616,7 +617,7 @@ __global__ void __launch_bounds__(THREADS) k_colour(const int* __restrict__ touc
 // Islands. Two bodies joined by a chain of placed pairs form one component; bodies of different components share no
 // pair and no wall record, so what a component's bodies go through in a step depends on that component alone. The
 // reference's order of operations is a per-body order (each body: its pairs in round order, then its walls, sweep
-// by sweep), so a component may be solved apart from the others, by one warp with warp barriers between its rounds,
+// by sweep), so a component may be solved apart from the others, by one block with block barriers between its rounds,
 // and give every bit the grid phases give. Components are found by union-find over the placed pairs (unplaced pairs
 // are never solved, so they join nothing).
 
@@ -755,7 +756,7 @@ __global__ void k_round_count(const int* __restrict__ touching_n, const int* __r
         const int bucket = path * BUCKETS + c * PAIR_KINDS + kind;
         atomicAdd(&round_count[bucket], 1);
         atomicMax(&bucket_most[bucket], min(max(count, 1), MOST_POINTS));
-        if (path == 1) atomicAdd(&gr_count[body_group[ta[t]] * GROUP_ROUNDS + c], 1);
+        if (path == 1) atomicAdd(&gr_count[(body_group[ta[t]] * GROUP_ROUNDS + c) * PAIR_KINDS + kind], 1);
         if (c < MOST_ROUNDS) {
             atomicMax(&counters->rounds, c + 1);
             if (path == 0) atomicMax(&counters->grid_rounds, c + 1);
@@ -790,8 +791,8 @@ __global__ void k_order(const int* __restrict__ touching_n, const int* __restric
         const long first = bucket_pstart[bucket] + (long)rank * bucket_most[bucket];
         now.pos[t] = p;
         now.pstart[p] = (int)first;
-        if (path == 1) {  // the island warps' list: by (group, round), each pair's position and its bodies' places
-            const int gr = body_group[ta[t]] * GROUP_ROUNDS + c;
+        if (path == 1) {  // the island list: by (group, round, kind), each pair's position and its bodies' places
+            const int gr = (body_group[ta[t]] * GROUP_ROUNDS + c) * PAIR_KINDS + kind;
             ilist[gr_start[gr] + atomicAdd(&gr_fill[gr], 1)] =
                 make_int2(p, body_local[ta[t]] | body_local[now.tb[t]] << 16);
         }
@@ -1498,27 +1499,30 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_solve(SolveArgs A) {
 
 
 // ------------------------------------------------------------------------------------------------------------
-// The island kernel: whole substeps of the small components, a warp a group, the group's bodies held in shared
-// memory for the step; and the bodies in no placed pair, a thread each. Every operation is the one the grid phases
-// make, in each body's order (velocities; the warm sweep and the solve sweeps, each its rounds then its walls, or
-// backward the walls then the rounds; positions; the relax sweeps), so the results are theirs to the bit.
-
-constexpr int ISLAND_THREADS = 32 * ISLAND_WARPS;
+// The island kernel: whole substeps of the small components, a block a group, the group's bodies held in shared memory
+// for the step; and the bodies in no placed pair, a thread each. Every operation is the one the grid phases make, in
+// each body's order (velocities; the warm sweep and the solve sweeps, each its rounds then its walls, or backward the
+// walls then the rounds; positions; the relax sweeps), so the results are theirs to the bit. As in the grid phases, a
+// round's pairs lie in kind order and the walls' bodies are listed spheres first and boxes last, so a warp's lanes
+// mostly take one path.
 
 struct IslandArgs {
     const int* group_body;   // [groups * GROUP_CAP]
     const int* group_count;  // [groups]
-    const int* gr_start;     // [groups * GROUP_ROUNDS + 1] each (group, round)'s first entry of ilist
+    const int* gr_start;     // [groups * GROUP_LISTS + 1] each (group, round, kind)'s first entry of ilist
     const int2* ilist;       // position, local ids of first | second << 16
     const int* free_list;    // bodies in no placed pair
     const int* island_n;     // bodies in small components
-    int* work;               // items handed out: groups, then runs of 32 lone bodies
+    int* work;               // items handed out: groups, then runs of ISLAND_THREADS lone bodies
 };
 
-struct GroupBodies {  // one warp's group, for the step
+struct GroupBodies {  // a block's group, for the step
     float4 pose[GROUP_CAP], turn[GROUP_CAP], vel[GROUP_CAP], mom[GROUP_CAP];
     int id[GROUP_CAP];
-    unsigned listed[GROUP_CAP / 32];  // bodies the walls' sweeps visit until positions next change
+    short wall_list[GROUP_CAP];  // bodies the walls' sweeps visit until positions next change: spheres, then boxes
+    int wall_count[2];           // spheres (from the front), boxes (from the back)
+    unsigned present;            // the rounds the group has pairs in
+    int item;
 };
 
 __device__ __forceinline__ void load_local(Held& h, const GroupBodies& G, const Bodies& b, int i) {
@@ -1537,79 +1541,72 @@ __device__ __forceinline__ bool wall_listed(const SolveArgs& A, int s, float4 po
     return __ldcg(&A.wmask[s]) != 0ull || near_walls(pose, hw, A.params.w[P_MARGIN], extent) != 0u;
 }
 
+__device__ __forceinline__ void group_list_wall(GroupBodies& G, int i, float4 hw) {
+    if (hw.w > 0.5f) G.wall_list[atomicAdd(&G.wall_count[0], 1)] = (short)i;
+    else G.wall_list[GROUP_CAP - 1 - atomicAdd(&G.wall_count[1], 1)] = (short)i;
+}
+
 __device__ __forceinline__ void group_velocities(const SolveArgs& A, GroupBodies& G, int nb, float h) {
-    const int lane = threadIdx.x & 31;
-    for (int j = 0; j * 32 < nb; j++) {
-        const int i = j * 32 + lane;
-        bool list = false;
-        if (i < nb) {
-            const int s = G.id[i];
-            const float4 pose = G.pose[i];
-            if (pose.w > 0.0f) {
-                float4 v = G.vel[i];
-                const int sc = scene_of(A, s);
-                v.x = v.x + h * word_of(A, sc, P_GX);
-                v.y = v.y + h * word_of(A, sc, P_GY);
-                v.z = v.z + h * word_of(A, sc, P_GZ);
-                G.vel[i] = v;
-                list = wall_listed(A, s, pose, __ldg(&A.b.half[s]));
-            }
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, list);
-        if (lane == 0) G.listed[j] = m;
+    if (threadIdx.x == 0) G.wall_count[0] = G.wall_count[1] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        const int s = G.id[i];
+        const float4 pose = G.pose[i];
+        if (!(pose.w > 0.0f)) continue;
+        float4 v = G.vel[i];
+        const int sc = scene_of(A, s);
+        v.x = v.x + h * word_of(A, sc, P_GX);
+        v.y = v.y + h * word_of(A, sc, P_GY);
+        v.z = v.z + h * word_of(A, sc, P_GZ);
+        G.vel[i] = v;
+        const float4 hw = __ldg(&A.b.half[s]);
+        if (wall_listed(A, s, pose, hw)) group_list_wall(G, i, hw);
     }
+    __syncthreads();
 }
 
 __device__ __forceinline__ void group_positions(const SolveArgs& A, GroupBodies& G, int nb, float h) {
-    const int lane = threadIdx.x & 31;
-    for (int j = 0; j * 32 < nb; j++) {
-        const int i = j * 32 + lane;
-        bool list = false;
-        if (i < nb) {
-            const int s = G.id[i];
-            float4 p = G.pose[i];
-            if (p.w > 0.0f) {
-                float4 turn = G.turn[i];
-                move_body(p, turn, G.vel[i], G.mom[i], __ldg(&A.b.inv[s]), h);
-                G.pose[i] = p;
-                G.turn[i] = turn;
-                list = wall_listed(A, s, p, __ldg(&A.b.half[s]));
-            }
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, list);
-        if (lane == 0) G.listed[j] = m;
+    if (threadIdx.x == 0) G.wall_count[0] = G.wall_count[1] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        const int s = G.id[i];
+        float4 p = G.pose[i];
+        if (!(p.w > 0.0f)) continue;
+        float4 turn = G.turn[i];
+        move_body(p, turn, G.vel[i], G.mom[i], __ldg(&A.b.inv[s]), h);
+        G.pose[i] = p;
+        G.turn[i] = turn;
+        const float4 hw = __ldg(&A.b.half[s]);
+        if (wall_listed(A, s, p, hw)) group_list_wall(G, i, hw);
     }
+    __syncthreads();
 }
 
-__device__ __forceinline__ void group_walls(const SolveArgs& A, GroupBodies& G, int nb, int kind, bool reverse,
+__device__ __forceinline__ void group_walls(const SolveArgs& A, GroupBodies& G, int kind, bool reverse,
                                             unsigned* track) {
-    const int lane = threadIdx.x & 31;
-    for (int j = 0; j * 32 < nb; j++) {
-        const int i = j * 32 + lane;
-        if (i < nb && ((G.listed[j] >> lane) & 1u)) {
-            Held box;
-            load_local(box, G, A.b, i);
-            if (walls_of<true>(A, box, G.id[i], kind, reverse, track)) store_local(box, G, i);
-        }
+    const int spheres = G.wall_count[0], listed = spheres + G.wall_count[1];
+    for (int k = threadIdx.x; k < listed; k += blockDim.x) {
+        const int i = G.wall_list[k < spheres ? k : GROUP_CAP - 1 - (k - spheres)];
+        Held box;
+        load_local(box, G, A.b, i);
+        if (walls_of<true>(A, box, G.id[i], kind, reverse, track)) store_local(box, G, i);
     }
 }
 
-// One sweep of a group: its rounds in order, a warp barrier after each (a round's pairs share no body), then the
+// One sweep of a group: its rounds in order, a block barrier after each (a round's pairs share no body), then the
 // walls; backward, the walls first and the rounds last to first.
-__device__ __forceinline__ void group_sweep(const SolveArgs& A, const IslandArgs& I, GroupBodies& G, int nb,
-                                            const int* gs, unsigned present, int kind, bool reverse, bool fill,
-                                            int index) {
-    const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void group_sweep(const SolveArgs& A, const IslandArgs& I, GroupBodies& G, const int* gs,
+                                            int kind, bool reverse, bool fill, int index) {
     unsigned* track = A.residual ? A.residual + index : nullptr;
     if (reverse) {
-        group_walls(A, G, nb, kind, true, track);
-        __syncwarp();
+        group_walls(A, G, kind, true, track);
+        __syncthreads();
     }
-    for (unsigned left = present; left;) {
+    for (unsigned left = G.present; left;) {
         const int r = reverse ? 31 - __clz(left) : __ffs(left) - 1;
         left &= ~(1u << r);
-        const int hi = gs[r + 1];
-        for (int idx = gs[r] + lane; idx < hi; idx += 32) {
+        const int hi = gs[(r + 1) * PAIR_KINDS];
+        for (int idx = gs[r * PAIR_KINDS] + threadIdx.x; idx < hi; idx += blockDim.x) {
             const int2 e = __ldg(&I.ilist[idx]);
             const int la = e.y & 0xffff, lb = e.y >> 16;
             Held first, second;
@@ -1619,18 +1616,17 @@ __device__ __forceinline__ void group_sweep(const SolveArgs& A, const IslandArgs
             store_local(first, G, la);
             store_local(second, G, lb);
         }
-        __syncwarp();
+        __syncthreads();
     }
     if (!reverse) {
-        group_walls(A, G, nb, kind, false, track);
-        __syncwarp();
+        group_walls(A, G, kind, false, track);
+        __syncthreads();
     }
 }
 
 __device__ __forceinline__ void run_group(const SolveArgs& A, const IslandArgs& I, GroupBodies& G, int g) {
-    const int lane = threadIdx.x & 31;
     const int nb = I.group_count[g];
-    for (int i = lane; i < nb; i += 32) {
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
         const int s = I.group_body[(long)g * GROUP_CAP + i];
         G.id[i] = s;
         G.pose[i] = __ldcg(&A.b.pose[s]);
@@ -1638,32 +1634,34 @@ __device__ __forceinline__ void run_group(const SolveArgs& A, const IslandArgs& 
         G.vel[i] = __ldcg(&A.b.vel[s]);
         G.mom[i] = __ldcg(&A.b.mom[s]);
     }
-    const int* gs = I.gr_start + (long)g * GROUP_ROUNDS;
-    const unsigned present = __ballot_sync(0xffffffffu, lane < GROUP_ROUNDS && gs[lane + 1] > gs[lane]);
-    __syncwarp();
+    const int* gs = I.gr_start + (long)g * GROUP_LISTS;
+    if (threadIdx.x < 32) {
+        const int r = threadIdx.x;
+        const unsigned present = __ballot_sync(0xffffffffu, gs[(r + 1) * PAIR_KINDS] > gs[r * PAIR_KINDS]);
+        if (r == 0) G.present = present;
+    }
+    __syncthreads();
     const float h = A.params.w[P_H];
     const int stride = 2 * A.sweeps + 1;  // residual words a substep
     for (int sub = 0; sub < A.substeps; sub++) {
         group_velocities(A, G, nb, h);
-        __syncwarp();
         const int base = sub * stride;
-        group_sweep(A, I, G, nb, gs, present, WARM, false, true, base);
+        group_sweep(A, I, G, gs, WARM, false, true, base);
         for (int sw = 0; sw < A.sweeps; sw++)
-            group_sweep(A, I, G, nb, gs, present, SOLVE, A.symmetric && sw % 2 == 1, false, base + 1 + sw);
+            group_sweep(A, I, G, gs, SOLVE, A.symmetric && sw % 2 == 1, false, base + 1 + sw);
         group_positions(A, G, nb, h);
-        __syncwarp();
         const int relax = base + 1 + A.sweeps;
         for (int sw = 0; sw < A.sweeps; sw++)
-            group_sweep(A, I, G, nb, gs, present, RELAX, A.symmetric && sw % 2 == 1, sw == 0, relax + sw);
+            group_sweep(A, I, G, gs, RELAX, A.symmetric && sw % 2 == 1, sw == 0, relax + sw);
     }
-    for (int i = lane; i < nb; i += 32) {
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
         const int s = G.id[i];
         __stcg(&A.b.pose[s], G.pose[i]);
         __stcg(&A.b.turn[s], G.turn[i]);
         __stcg(&A.b.vel[s], G.vel[i]);
         __stcg(&A.b.mom[s], G.mom[i]);
     }
-    __syncwarp();  // the shared memory is the next group's
+    __syncthreads();  // the shared memory is the next group's
 }
 
 // A body in no placed pair, all substeps in one thread: velocities, its walls in every sweep it is listed for,
@@ -1713,23 +1711,22 @@ __device__ __forceinline__ void run_alone(const SolveArgs& A, int s) {
     __stcg(&A.b.mom[s], mom);
 }
 
-// Warps take items from a counter: the groups first (the longer chains), then runs of 32 lone bodies.
-__global__ void __launch_bounds__(ISLAND_THREADS, 4) k_islands(SolveArgs A, IslandArgs I) {
-    __shared__ GroupBodies groups[ISLAND_WARPS];
-    GroupBodies& G = groups[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
+// Blocks take items from a counter: the groups first (the longer chains), then runs of lone bodies, one a thread.
+__global__ void __launch_bounds__(ISLAND_THREADS, 2) k_islands(SolveArgs A, IslandArgs I) {
+    __shared__ GroupBodies G;
     const int ngroups = (*I.island_n + GROUP_BASE - 1) / GROUP_BASE;
     const int nfree = *(volatile const int*)&A.counters->free_n;
-    const int items = ngroups + (nfree + 31) / 32;
+    const int items = ngroups + (nfree + ISLAND_THREADS - 1) / ISLAND_THREADS;
     for (;;) {
-        int item = 0;
-        if (lane == 0) item = atomicAdd(I.work, 1);
-        item = __shfl_sync(0xffffffffu, item, 0);
+        if (threadIdx.x == 0) G.item = atomicAdd(I.work, 1);
+        __syncthreads();
+        const int item = G.item;
+        __syncthreads();
         if (item >= items) break;
         if (item < ngroups) {
             run_group(A, I, G, item);
         } else {
-            const int f = (item - ngroups) * 32 + lane;
+            const int f = (item - ngroups) * ISLAND_THREADS + threadIdx.x;
             if (f < nfree) run_alone(A, I.free_list[f]);
         }
     }
@@ -2097,7 +2094,7 @@ int mark(vxr_box_world* w, int which) {
 // Launches per step, counted as they are made.
 #define LAUNCHED(k) (w->launches += (k))
 
-// Whether a step solves its small components by island warps: on by default; off where a substep's sweep count
+// Whether a step solves its small components by island blocks: on by default; off where a substep's sweep count
 // depends on a residual over every contact (the measuring tolerance), which only the grid phases gather.
 bool islands_on(const vxr_box_world* w) {
     return w->islands && w->has_grid && !(w->measure && w->tolerance > 0.0f);
@@ -2188,8 +2185,8 @@ int enqueue_step(vxr_box_world* w) {
             k_assign<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_offset,
                                                                 w->group_base, w->isl_fill, w->body_group,
                                                                 w->body_local, w->group_body, w->group_count);
-            VXR_CUDA(cudaMemsetAsync(w->gr_count, 0, sizeof(int) * (size_t)w->groups_max * GROUP_ROUNDS, st));
-            VXR_CUDA(cudaMemsetAsync(w->gr_fill, 0, sizeof(int) * (size_t)w->groups_max * GROUP_ROUNDS, st));
+            VXR_CUDA(cudaMemsetAsync(w->gr_count, 0, sizeof(int) * (size_t)w->groups_max * GROUP_LISTS, st));
+            VXR_CUDA(cudaMemsetAsync(w->gr_fill, 0, sizeof(int) * (size_t)w->groups_max * GROUP_LISTS, st));
             LAUNCHED(6 + 3);  // init, link, flatten, classify, group base, assign, scan
         }
         VXR_CUDA(cudaMemsetAsync(w->round_count, 0, sizeof(int) * ALL_BUCKETS, st));
@@ -2203,7 +2200,7 @@ int enqueue_step(vxr_box_world* w) {
                                                   groups_of, w->gr_count);
         exclusive_scan(w->round_count, w->bucket_start, ALL_BUCKETS, w->scan_tiles, st);
         if (isl) {
-            exclusive_scan(w->gr_count, w->gr_start, w->groups_max * GROUP_ROUNDS, w->scan_tiles, st);
+            exclusive_scan(w->gr_count, w->gr_start, w->groups_max * GROUP_LISTS, w->scan_tiles, st);
             LAUNCHED(3);
         }
         k_round_starts<<<1, 64, 0, st>>>(w->bucket_start, w->round_start);
@@ -2495,7 +2492,7 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     // groups the bodies can fill: one a GROUP_BASE placed, plus the last part-filled one
     w->groups_max = n / GROUP_BASE + 2;
     rc |= alloc(w, &w->scan_tiles,
-                scan_tiles_for(std::max(std::max(n, w->cells), w->groups_max * GROUP_ROUNDS + 1)) + 1);
+                scan_tiles_for(std::max(std::max(n, w->cells), w->groups_max * GROUP_LISTS + 1)) + 1);
     rc |= alloc(w, &w->round_count, ALL_BUCKETS);
     rc |= alloc(w, &w->round_start, MOST_ROUNDS + 2);
     rc |= alloc(w, &w->bucket_start, ALL_BUCKETS + 1);
@@ -2568,9 +2565,9 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
         rc |= alloc(w, &w->group_body, (size_t)w->groups_max * GROUP_CAP);
         rc |= alloc(w, &w->group_count, w->groups_max);
         rc |= alloc(w, &w->group_base, w->groups_max);
-        rc |= alloc(w, &w->gr_count, (size_t)w->groups_max * GROUP_ROUNDS);
-        rc |= alloc(w, &w->gr_start, (size_t)w->groups_max * GROUP_ROUNDS + 1);
-        rc |= alloc(w, &w->gr_fill, (size_t)w->groups_max * GROUP_ROUNDS);
+        rc |= alloc(w, &w->gr_count, (size_t)w->groups_max * GROUP_LISTS);
+        rc |= alloc(w, &w->gr_start, (size_t)w->groups_max * GROUP_LISTS + 1);
+        rc |= alloc(w, &w->gr_fill, (size_t)w->groups_max * GROUP_LISTS);
         rc |= alloc(w, &w->ilist, w->cap);
         rc |= alloc(w, &w->grid_list, n);
         rc |= alloc(w, &w->free_list, n);

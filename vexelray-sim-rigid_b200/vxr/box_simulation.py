@@ -287,12 +287,12 @@ class BoxSimulation:
         self._check(self.L.vxr_box_wait_limit(self.h, int(ns)))
 
     def islands(self, enable: bool = True) -> None:
-        """Small components solved by island warps (the default), or every body through the grid-wide phases; the
+        """Small components solved by island blocks (the default), or every body through the grid-wide phases; the
         results are the same either way."""
         self._check(self.L.vxr_box_islands(self.h, int(bool(enable))))
 
     def paths(self) -> dict:
-        """How the last step was scheduled: bodies through the grid-wide phases, in small components (island warps),
+        """How the last step was scheduled: bodies through the grid-wide phases, in small components (island blocks),
         in no placed pair (a thread each), and the island groups."""
         out = np.zeros(5, np.int32)
         self._check(self.L.vxr_box_paths(self.h, ptr(out)))
