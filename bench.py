@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -198,7 +199,8 @@ def make_world(scene, device, max_pairs=0, schedule=0, solve_blocks_per_sm=0, is
     from vxr.box_simulation import BoxSimulation
     # room for the iteration count measurement's sweeps; the steps run the scene's own
     w = BoxSimulation(scene["bodies"], scene["substeps"], max(scene["sweeps"], ITERATION_CAP), False, scene["grid"],
-                      device=device, max_pairs=max_pairs, schedule=schedule, solve_blocks_per_sm=solve_blocks_per_sm)
+                      reach_cells=scene.get("reach_cells", 1), device=device, max_pairs=max_pairs, schedule=schedule,
+                      solve_blocks_per_sm=solve_blocks_per_sm)
     w.measure(residual=False, sweeps=scene["sweeps"])
     w.islands(islands)
     l = [scene["lx"], scene["ly"], scene["lz"]]
@@ -207,6 +209,17 @@ def make_world(scene, device, max_pairs=0, schedule=0, solve_blocks_per_sm=0, is
     w.start_momentum(scene["x"], scene["y"], scene["z"], scene["u"], scene["v"], scene["w"], l, q, h,
                      scene["shape"], scene["im"], scene["params"])
     return w
+
+
+def with_cell(scene, cell):
+    """The scene on a grid of `cell`-wide cells; where that is narrower than the reference's rule (BoxBroad.grid),
+    the neighbourhood walk widens to as many cells each way as the rule's cell spans."""
+    from vxr import boxes as B
+    sx, sy, sz = scene["walls"]
+    rule = scene["grid"].cell
+    scene["grid"] = B.covering(sx, sy, sz, cell)
+    scene["reach_cells"] = max(1, math.ceil(rule / scene["grid"].cell))
+    return scene
 
 
 def algorithmic_solve_bytes(n, substeps, sweeps, touching, points, active, wall_records):
@@ -879,6 +892,9 @@ def main():
     ap.add_argument("--load-state", default="", help="large scene: start from a state saved by --save-state")
     ap.add_argument("--solve-blocks-per-sm", type=int, default=0, help="solve blocks an SM (0: the library's choice)")
     ap.add_argument("--max-pairs", type=int, default=0, help="pair capacity of the world (0: 32 a body)")
+    ap.add_argument("--cell", type=float, default=0.0,
+                    help="large scene: grid cell in metres (0: the reference's rule, about 2.07 m); a narrower cell "
+                         "walks as many cells each way as the rule's width needs (1.6 m: 2, the 125 cells)")
     ap.add_argument("--no-islands", action="store_true",
                     help="every body through the grid-wide phases (small components not solved by island blocks)")
     ap.add_argument("--workload", default="large-mixed",
@@ -906,6 +922,8 @@ def main():
         scene = scenes.large_mixed(args.bodies, seed=1 + rank)
     else:  # a smaller case of the same scene: the same body density over a smaller footprint
         scene = scenes.sub_volume(BODIES, args.bodies / BODIES, seed=1 + rank)
+    if args.cell > 0:
+        with_cell(scene, args.cell)
     w = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm, not args.no_islands)
     if args.load_state:  # a state saved by --save-state: the 13 moving fields; shapes, masses and params the scene's
         z = np.load(args.load_state)
@@ -1046,6 +1064,7 @@ def main():
                    "bodies": scene["bodies"], "dt": scene["dt"], "substeps": scene["substeps"],
                    "sweeps": scene["sweeps"], "mu": scene["mu"], "mu_rolling": scene["mu_rolling"],
                    "grid": [scene["grid"].nx, scene["grid"].ny, scene["grid"].nz, scene["grid"].cell],
+                   "reach_cells": scene.get("reach_cells", 1),
                    "timed_steps": f"{args.warmup}..{args.warmup + args.steps - 1} of the drop",
                    "l2": "flushed (256 MiB write) before every timed step",
                    "schedule": args.schedule, "solve_blocks_per_sm": args.solve_blocks_per_sm,

@@ -38,6 +38,7 @@ def lib(threads: bool = False) -> ctypes.CDLL:
         L.orc_box_create.restype = vp
         L.orc_box_create.argtypes = [i, i, i, i, i, i, i, f, i]
         L.orc_box_destroy.argtypes = [vp]
+        L.orc_box_set_reach.argtypes = [vp, i]
         L.orc_box_set_field.argtypes = [vp, i, vp]
         L.orc_box_get_field.argtypes = [vp, i, vp]
         L.orc_box_set_params.argtypes = [vp, vp]
@@ -63,13 +64,14 @@ def _ptr(a: np.ndarray) -> ctypes.c_void_p:
 class OracleBoxWorld:
     """The oracle's box/mixed world: the same start / step / state surface as the CUDA library's BoxSimulation."""
 
-    def __init__(self, n, substeps, sweeps, symmetric, grid, threads=False):
+    def __init__(self, n, substeps, sweeps, symmetric, grid, threads=False, reach_cells=1):
         self.L = lib(threads)
         self.n = n
         g = grid
         self.h = self.L.orc_box_create(n, substeps, sweeps, int(bool(symmetric)), g.nx if g else 1,
                                        g.ny if g else 1, g.nz if g else 1, g.cell if g else 1.0,
                                        1 if g is not None else 0)
+        self.L.orc_box_set_reach(self.h, int(reach_cells))
 
     def close(self):
         if self.h:

@@ -316,6 +316,7 @@ struct World {
     int n, substeps, sweeps, symmetric;
     int nx, ny, nz;
     float cell;
+    int reach_cells = 1;  // neighbourhood half-width in cells: 1 is the reference's 27 cells
     int slots, width;
     std::vector<float> f[18];  // x y z u v w lx ly lz qx qy qz qw im hx hy hz shape
     float params[PARAM_COUNT];
@@ -955,7 +956,9 @@ void binAndSort(World& w) {
     for (int s = 0; s < w.n; s++) w.order[fill[w.keys[s]]++] = s;
 }
 
-// BoxBroad.list :103-164 with around :230-252.
+// BoxBroad.list :103-164 with around :230-252. With reach_cells r > 1 (cells narrower than BoxBroad.grid's rule,
+// :66-68) the walk widens to the (2r + 1)^3 cells around, in the same x-fastest order; at r = 1 it is the reference's
+// 27 cells in its order.
 void list(World& w) {
     const float margin = w.params[MARGIN];
     ORC_PARALLEL_FOR
@@ -971,8 +974,9 @@ void list(World& w) {
         int found = 0;
         int key = w.keys[s];
         int ix = key % w.nx, iy = (key / w.nx) % w.ny, iz = key / (w.nx * w.ny);
-        for (int nn = 0; nn < 27; nn++) {
-            int jx = ix + (nn % 3 - 1), jy = iy + ((nn / 3) % 3 - 1), jz = iz + (nn / 9 - 1);
+        const int r = w.reach_cells, side = 2 * r + 1;
+        for (int nn = 0; nn < side * side * side; nn++) {
+            int jx = ix + (nn % side - r), jy = iy + ((nn / side) % side - r), jz = iz + (nn / (side * side) - r);
             if (!(jx >= 0 && jx < w.nx && jy >= 0 && jy < w.ny && jz >= 0 && jz < w.nz)) continue;
             int cell = jx + w.nx * (jy + w.ny * jz);
             for (int k = w.starts[cell]; k < w.starts[cell + 1]; k++) {
@@ -1193,6 +1197,8 @@ void stepOnce(World& w) {
 extern "C" {
 
 // fields: 0 x 1 y 2 z 3 u 4 v 5 w 6 lx 7 ly 8 lz 9 qx 10 qy 11 qz 12 qw 13 im 14 hx 15 hy 16 hz 17 shape
+void orc_box_set_reach(void* h, int reach_cells) { ((World*)h)->reach_cells = reach_cells > 0 ? reach_cells : 1; }
+
 void* orc_box_create(int n, int substeps, int sweeps, int symmetric, int nx, int ny, int nz, float cell,
                      int grid) {
     World* w = new World();
