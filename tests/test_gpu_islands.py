@@ -68,20 +68,25 @@ def test_islands_and_grid_phases_agree_through_the_drop():
     b.close()
 
 
-def test_a_pile_beside_islands_matches_the_grid_phases():
-    """A crowded drop into a low box: a pile larger than a block's component forms within a few steps beside small
-    islands and lone bodies, so both schedules run in the same step; equal to the bit."""
+def test_a_pile_larger_than_a_block_sends_every_body_to_the_grid_phases():
+    """A crowded drop into a low box: once a component larger than a block's forms, every body of the step takes the
+    grid phases (their phase count is set by the rounds alone); before, the components take island blocks. Equal to
+    the bit throughout."""
     sc = scenes.large_mixed(4096, seed=9, volume=(24.0, 6.0, 24.0), height=12.0)
     a = gpu_world(sc, islands=True)
     b = gpu_world(sc, islands=False)
-    both = 0
-    for k in range(4):
-        a.step_and_wait(15)
-        b.step_and_wait(15)
+    seen = set()
+    for k in range(8):
+        a.step_and_wait(1 if k < 4 else 15)
+        b.step_and_wait(1 if k < 4 else 15)
         p = a.paths()
-        both += p["grid"] > 0 and (p["islands"] > 0 or p["alone"] > 0)
-        assert_same_worlds(a, b, f"after {15 * (k + 1)} steps")
-    assert both > 0
+        if p["largest"] > 256:
+            assert p["grid"] == sc["bodies"] and p["islands"] == 0 and p["alone"] == 0
+            seen.add("grid")
+        else:
+            seen.add("islands")
+        assert_same_worlds(a, b, f"after check {k}")
+    assert "grid" in seen
     a.close()
     b.close()
 

@@ -109,6 +109,7 @@ struct Counters {  // device-side counts of a step
     int free_n;       // bodies in no placed pair
     int work;         // the island kernel's work counter
     int largest;      // bodies of the largest component
+    int all_grid;     // a component too large for a block: every body through the grid phases
 };
 
 struct Totals {  // accumulated over the steps of one vxr_box_step call
@@ -669,8 +670,16 @@ __global__ void k_uf_flatten(int n, const int* __restrict__ parent, int* __restr
     atomicAdd(&size[r], 1);
 }
 
+// The largest component's body count.
+__global__ void k_largest(int n, const int* __restrict__ root, const int* __restrict__ size, Counters* counters) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n && root[s] == s && size[s] > 1) atomicMax(&counters->largest, size[s]);
+}
+
 // Which path each body takes: a component of one body (no placed pair) alone, a component of at most ISLAND_MOST
-// bodies in a group, a larger one through the grid phases. A small component's root keys the packing.
+// bodies in a group. Where any component is larger, every body goes through the grid phases: their phase count is
+// set by the rounds alone, so the small components cost them nothing more there, while beside them the island
+// blocks would only lengthen the step. A small component's root keys the packing.
 __global__ void k_classify(int n, const int* __restrict__ root, const int* __restrict__ size, int* __restrict__ key,
                            int* __restrict__ body_group, int* __restrict__ grid_list, int* __restrict__ free_list,
                            Counters* counters) {
@@ -678,16 +687,16 @@ __global__ void k_classify(int n, const int* __restrict__ root, const int* __res
     if (s >= n) return;
     const int r = root[s];
     const int m = size[r];
-    if (r == s && m > 1) atomicMax(&counters->largest, m);
     int k = 0;
-    if (m == 1) {
+    if (*(volatile const int*)&counters->largest > ISLAND_MOST) {
+        body_group[s] = -2;
+        if (s == 0) counters->all_grid = 1;
+    } else if (m == 1) {
         body_group[s] = -1;
         free_list[atomicAdd(&counters->free_n, 1)] = s;
-    } else if (m > ISLAND_MOST) {
-        body_group[s] = -2;
-        grid_list[atomicAdd(&counters->grid_n, 1)] = s;
-    } else if (r == s) {
-        k = m;
+    } else {
+        body_group[s] = -3;  // a small component's: its group comes from k_assign
+        if (r == s) k = m;
     }
     key[s] = k;
 }
@@ -695,11 +704,12 @@ __global__ void k_classify(int n, const int* __restrict__ root, const int* __res
 // Where each group's bodies begin: the place of its first component (a component that began in the group before may
 // reach past the group's GROUP_BASE boundary, so a group's places start at its own first component, not there).
 __global__ void k_group_base(int n, const int* __restrict__ root, const int* __restrict__ size,
-                             const int* __restrict__ offset, int* __restrict__ group_base) {
+                             const int* __restrict__ offset, const int* __restrict__ body_group,
+                             int* __restrict__ group_base) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n || root[s] != s) return;
+    if (s >= n || root[s] != s || body_group[s] == -2) return;
     const int m = size[s];
-    if (m == 1 || m > ISLAND_MOST) return;
+    if (m == 1) return;
     const int at = offset[s];
     atomicMin(&group_base[at / GROUP_BASE], at);
 }
@@ -714,7 +724,7 @@ __global__ void k_assign(int n, const int* __restrict__ root, const int* __restr
     if (s >= n) return;
     const int r = root[s];
     const int m = size[r];
-    if (m == 1 || m > ISLAND_MOST) return;
+    if (m == 1 || body_group[s] == -2) return;
     const int at = offset[r];
     const int g = at / GROUP_BASE;
     const int local = (at - group_base[g]) + atomicAdd(&fill[r], 1);
@@ -869,10 +879,13 @@ struct SolveArgs {
 };
 
 // The i-th body of the grid phases, and how many there are.
-__device__ __forceinline__ int grid_bodies(const SolveArgs& A) {
-    return A.grid_list ? *(volatile const int*)A.grid_n : A.n;
+__device__ __forceinline__ bool listed_grid(const SolveArgs& A) {
+    return A.grid_list && !*(volatile const int*)&A.counters->all_grid;
 }
-__device__ __forceinline__ int grid_body(const SolveArgs& A, int i) { return A.grid_list ? A.grid_list[i] : i; }
+__device__ __forceinline__ int grid_bodies(const SolveArgs& A) {
+    return listed_grid(A) ? *(volatile const int*)A.grid_n : A.n;
+}
+__device__ __forceinline__ int grid_body(const SolveArgs& A, int i) { return listed_grid(A) ? A.grid_list[i] : i; }
 
 // Body state a solve phase reads and writes goes through L2 (ld/st .cg): under the dependency schedule one
 // body's consecutive items can run on different SMs.
@@ -2174,6 +2187,7 @@ int enqueue_step(vxr_box_world* w) {
             k_uf_init<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->parent, w->isl_size, w->isl_fill);
             k_uf_link<<<tblocks, THREADS, 0, st>>>(tn, w->ta, now.tb, w->colour, w->parent);
             k_uf_flatten<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->parent, w->comp, w->isl_size);
+            k_largest<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->counters);
             k_classify<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_key,
                                                                   w->body_group, w->grid_list, w->free_list,
                                                                   w->counters);
@@ -2181,13 +2195,13 @@ int enqueue_step(vxr_box_world* w) {
             VXR_CUDA(cudaMemsetAsync(w->group_count, 0, sizeof(int) * w->groups_max, st));
             VXR_CUDA(cudaMemsetAsync(w->group_base, 0x7f, sizeof(int) * w->groups_max, st));
             k_group_base<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_offset,
-                                                                    w->group_base);
+                                                                    w->body_group, w->group_base);
             k_assign<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_offset,
                                                                 w->group_base, w->isl_fill, w->body_group,
                                                                 w->body_local, w->group_body, w->group_count);
             VXR_CUDA(cudaMemsetAsync(w->gr_count, 0, sizeof(int) * (size_t)w->groups_max * GROUP_LISTS, st));
             VXR_CUDA(cudaMemsetAsync(w->gr_fill, 0, sizeof(int) * (size_t)w->groups_max * GROUP_LISTS, st));
-            LAUNCHED(6 + 3);  // init, link, flatten, classify, group base, assign, scan
+            LAUNCHED(7 + 3);  // init, link, flatten, largest, classify, group base, assign, scan
         }
         VXR_CUDA(cudaMemsetAsync(w->round_count, 0, sizeof(int) * ALL_BUCKETS, st));
         VXR_CUDA(cudaMemsetAsync(w->bucket_most, 0, sizeof(int) * ALL_BUCKETS, st));
@@ -3251,12 +3265,12 @@ int32_t vxr_box_paths(vxr_box_world* w, int32_t* out5) {
     if (w->has_grid)
         VXR_CUDA(cudaMemcpyAsync(&island, w->isl_offset + w->n, sizeof(int), cudaMemcpyDeviceToHost, w->stream));
     VXR_CUDA(cudaStreamSynchronize(w->stream));
-    const bool isl = islands_on(w);
+    const bool isl = islands_on(w) && !c.all_grid;
     out4[0] = isl ? c.grid_n : w->n;
     out4[1] = isl ? island : 0;
     out4[2] = isl ? c.free_n : 0;
     out4[3] = isl ? (island + GROUP_BASE - 1) / GROUP_BASE : 0;
-    out5[4] = isl ? c.largest : 0;
+    out5[4] = islands_on(w) ? c.largest : 0;
     return VXR_OK;
 }
 

@@ -48,7 +48,7 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& b, unsigned int& ep
             unsigned int spins = 0;
             while (load_acquire(b.count) < target) {
                 if (*(volatile int*)b.abort) break;
-                if ((++spins & 255u) == 0u && global_ns() - start > b.limit_ns) {
+                if (((++spins & 255u) == 0u || spins == 1u) && global_ns() - start > b.limit_ns) {
                     atomicExch(b.abort, 1);
                     atomicCAS(b.status, ST_OK, ST_TIMEOUT);
                     break;
