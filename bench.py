@@ -191,6 +191,9 @@ ITERATION_CAP = 64
 # DRAM traffic of one k_solve launch of the large scene late in the drop, from an ncu capture (one pass:
 # dram__bytes_read.sum + dram__bytes_write.sum) of the step after step 480, the state saved at step 480 and loaded.
 # A late launch is where the pair records outgrow L2; that launch's own algorithmic bytes are given beside it.
+# The landed-pile window's first step: by then the bodies from the top of the 64 m volume have landed (a drop of 64 m
+# takes about 3.6 s, 430 steps of 1/120 s).
+LANDED_STEP = 480
 LATE_SOLVE_TRAFFIC = {"step": 481, "dram_bytes": 5.17e9, "dram_read_bytes": 3.76e9, "dram_write_bytes": 1.41e9,
                       "algorithmic_bytes": 7.85e9, "ms": 18.85, "source": "ncu, one launch"}
 
@@ -220,6 +223,57 @@ def with_cell(scene, cell):
     scene["grid"] = B.covering(sx, sy, sz, cell)
     scene["reach_cells"] = max(1, math.ceil(rule / scene["grid"].cell))
     return scene
+
+
+def window_quality(w, scene, steps):
+    """What `steps` more steps of `w` leave behind, at the scene's own sweep count: each substep's residual after
+    its last solve sweep and after its last relax sweep (the largest positional correction that sweep still made,
+    h k (|dlambda_n| + |dlambda_t|)), and each contact point's complementarity error at the step's end (the larger of
+    h max(0, -(vn + max(gap, 0) / h)) within the margin and the overlap max(0, -gap)). Measuring changes no result."""
+    sweeps = scene["sweeps"]
+    w.measure(residual=True, sweeps=sweeps)
+    solve_res, relax_res, errs_max, errs_p99, points = [], [], [], [], 0
+    for _ in range(steps):
+        w.step_and_wait(1)
+        res, _ = w.residuals()
+        solve_res.extend(res[:, sweeps].tolist())
+        relax_res.extend(res[:, 2 * sweeps].tolist())
+        e = w.contact_errors()
+        points += len(e)
+        if len(e):
+            errs_max.append(float(e.max()))
+            errs_p99.append(float(np.percentile(e, 99)))
+    w.measure(residual=False, sweeps=sweeps)
+    s, r = np.array(solve_res), np.array(relax_res)
+    return {"steps": steps, "sweeps": sweeps,
+            "update_residual_m": {"after_last_solve_sweep": {"max": float(s.max()), "p99": float(np.percentile(s, 99)),
+                                                             "median": float(np.median(s))},
+                                  "after_last_relax_sweep": {"max": float(r.max()), "p99": float(np.percentile(r, 99)),
+                                                             "median": float(np.median(r))},
+                                  "substeps_at_or_below_1e-4": float(np.mean(s <= 1e-4))},
+            "complementarity_m": {"max": max(errs_max) if errs_max else 0.0,
+                                  "p99_median_over_steps": float(np.median(errs_p99)) if errs_p99 else 0.0,
+                                  "points_per_step": points / max(steps, 1)},
+            "definitions": "update residual: a sweep's largest positional correction at any contact point; "
+                           "complementarity: per contact point at the step's end, "
+                           "max(h max(0, -(vn + max(gap,0)/h)) within the margin, max(0, -gap))"}
+
+
+def timed_steps(w, stream, flush, steps):
+    """`steps` steps of `w`, each timed with CUDA events on the world's stream, L2 flushed before each."""
+    import torch
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            starts[k].record(stream)
+        w.step_async(1)
+        with torch.cuda.stream(stream):
+            ends[k].record(stream)
+    w.sync()
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in zip(starts, ends)]
 
 
 def algorithmic_solve_bytes(n, substeps, sweeps, touching, points, active, wall_records):
@@ -895,6 +949,7 @@ def main():
     ap.add_argument("--cell", type=float, default=0.0,
                     help="large scene: grid cell in metres (0: the reference's rule, about 2.07 m); a narrower cell "
                          "walks as many cells each way as the rule's width needs (1.6 m: 2, the 125 cells)")
+    ap.add_argument("--no-landed", action="store_true", help="large scene: skip the landed-pile window")
     ap.add_argument("--no-islands", action="store_true",
                     help="every body through the grid-wide phases (small components not solved by island blocks)")
     ap.add_argument("--workload", default="large-mixed",
@@ -998,6 +1053,30 @@ def main():
     pic = picture_timing(w, 1, scene["bodies"], scene["walls"], local, squash=0.0,
                          cpu=rank == 0 and not args.no_cpu)
 
+    # The timed steps' quality: a second world along the same trajectory (the step is deterministic and measuring
+    # changes no result), stepped untimed to the timed window's start, then the same steps measured.
+    wq = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm, not args.no_islands)
+    wq.step_and_wait(args.warmup)
+    quality = window_quality(wq, scene, args.steps)
+    quality["same_trajectory_as_timed"] = all(np.array_equal(a.view(np.int32), b.view(np.int32))
+                                              for a, b in zip(wq.state(), w.state()))
+    wq.close()
+
+    # The landed pile: the scene stepped untimed to LANDED_STEP (bodies from the top of the volume land about then),
+    # then as many steps as the timed window, timed the same way, and their quality measured on the steps after.
+    landed, wl = None, None
+    if not args.no_landed:
+        wl = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm, not args.no_islands)
+        for _ in range(LANDED_STEP // 20):
+            wl.step_async(20)
+            wl.sync()
+        ms_l = timed_steps(wl, torch.cuda.ExternalStream(wl.stream), flush, args.steps)
+        slow_l = all_max(pg, float(sum(ms_l)))
+        landed = {"steps": f"{LANDED_STEP}..{LANDED_STEP + args.steps - 1}", "ms_per_step": slow_l / args.steps,
+                  "value": bodies_all * args.steps / (slow_l / 1e3), "touching": wl.last().touching,
+                  "rounds": wl.last().rounds, "paths": wl.paths(),
+                  "quality": window_quality(wl, scene, min(args.steps, 10))}
+
     # Iterations to residual: the same world, the pile as the timed steps left it, a substep's solve sweeps run until
     # a sweep's residual (the largest positional correction it makes at any contact point) is 1e-4 m or less, at most
     # 64; with the impulses carried from the step before (the reference's warm start), from zero, and from the learned
@@ -1022,6 +1101,8 @@ def main():
         losses = net.train(feats, targets, epochs=20, batch=4096, lr=1e-3, seed=8)
         train_s = time.perf_counter() - t1
         verdict = Lm.judge(w, net, steps=3, tolerance=1e-4, cap=ITERATION_CAP)
+        if wl is not None:
+            landed["iterations_to_residual"] = Lm.judge(wl, net, steps=3, tolerance=1e-4, cap=ITERATION_CAP)
         net.close()
         w.measure(residual=False, cold_start=False, sweeps=scene["sweeps"], tolerance=0.0)
         iters.update(verdict)
@@ -1031,6 +1112,8 @@ def main():
                              "data": "a second world of the same distribution (seed 101), settled as far; targets "
                                      "from the plain solver run to 1e-6 m (at most 64 sweeps)"}
 
+    if wl is not None:
+        wl.close()
     judged = None
     if not args.no_judge:
         judged = judged_run(scene, 500, 10, local)
@@ -1073,13 +1156,16 @@ def main():
                               "colour": phases[2] / args.steps, "solve": phases[3] / args.steps},
         "windows": windows,
         "last_step": {**reports.last_step(), **activity},
-        "roofline": {"bound": "hbm", "kernel": "k_solve", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "the solve (k_islands, then k_solve)", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": LATE_SOLVE_TRAFFIC["dram_bytes"] if args.bodies == BODIES
                      else None, "peak_source": which, "bytes_per_launch": b_solve, "ms_per_launch": solve_ms,
                      "bytes_per_launch_sampled": "every 20th timed step",
                      "traffic_launch": LATE_SOLVE_TRAFFIC if args.bodies == BODIES else None},
         "gpu_launches": int(launches),
         "iterations_to_residual": iters,
+        "quality": quality,
+        "landed_window": landed,
         "judged_500_steps": judged,
         "picture": pic,
         "e2e": e2e,

@@ -275,6 +275,14 @@ typedef struct {
 } vxr_box_diag;
 int32_t vxr_box_diagnostics(vxr_box_world* world, vxr_box_diag* out);
 
+/* The positional complementarity error (metres) at each contact point of the last step, from the state at its end:
+ * the larger of h max(0, -(vn + max(gap, 0) / h)) (for a point within the margin: how deep the relative normal
+ * velocity would close within a substep beyond the gap) and max(0, -gap) (the overlap). No reference counterpart:
+ * the reference has no residual; this is the measure a solve's quality is judged by. out receives 4 rows a touching
+ * pair (round order), -1 past a pair's point count. Returns the row count (out NULL: only the count), or minus a
+ * status. */
+int32_t vxr_box_contact_errors(vxr_box_world* world, float* out, int32_t capacity);
+
 /* `pairs` x 2 steps as replays of one CUDA graph holding two whole steps, enqueued without waiting (vxr_box_sync
  * waits and reports). The first call captures the graph; changing the parameters, the measuring switches or the
  * state captures it again at the next call. Profiling and tracing must be off. */

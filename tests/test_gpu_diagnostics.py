@@ -104,3 +104,49 @@ def test_gpu_box_towers_stand_without_penetration_or_energy_gain():
         assert d["kinetic"] + d["potential"] <= e0 * (1 + 1e-5)
     assert worst < 5e-3
     w.close()
+
+
+def host_contact_errors(w, sc, h, margin):
+    """Each contact point's complementarity error, in doubles from the state read back."""
+    x, y, z, u, v, wv, lx, ly, lz, qx, qy, qz, qw = [a.astype(np.float64) for a in w.state()]
+    at, vel, spun = np.stack([x, y, z]), np.stack([u, v, wv]), np.stack([lx, ly, lz])
+    q = np.stack([qx, qy, qz, qw])
+    half = np.stack([sc["hx"], sc["hy"], sc["hz"]]).astype(np.float64)
+    sphere = sc["shape"] > 0.5
+    m = 1.0 / sc["im"].astype(np.float64)
+    moment = np.where(sphere, 0.4 * m * half[0] ** 2, 0.0)
+    moments = np.stack([np.where(sphere, moment, m * (half[1] ** 2 + half[2] ** 2) / 3),
+                        np.where(sphere, moment, m * (half[0] ** 2 + half[2] ** 2) / 3),
+                        np.where(sphere, moment, m * (half[0] ** 2 + half[1] ** 2) / 3)])
+    conj = q * np.array([-1, -1, -1, 1.0])[:, None]
+    omega = rotate(q, rotate(conj, spun) / moments)
+    a, b, c, mf, _ = w.touching()
+    out = []
+    for t in range(len(a)):
+        n = mf[t, 0:3].astype(np.float64)
+        for i in range(c[t]):
+            pt = mf[t, B.POINTS + i * B.POINT_WORDS:]
+            ra = half[0, a[t]] * n if sphere[a[t]] else rotate(q[:, a[t]:a[t] + 1], pt[0:3, None].astype(np.float64))[:, 0]
+            rb = -half[0, b[t]] * n if sphere[b[t]] else rotate(q[:, b[t]:b[t] + 1], pt[3:6, None].astype(np.float64))[:, 0]
+            gap = float(np.dot((at[:, b[t]] + rb) - (at[:, a[t]] + ra), n))
+            va = vel[:, a[t]] + np.cross(omega[:, a[t]], ra)
+            vb = vel[:, b[t]] + np.cross(omega[:, b[t]], rb)
+            vn = float(np.dot(vb - va, n))
+            closing = h * max(0.0, -(vn + max(gap, 0.0) / h)) if gap <= margin else 0.0
+            out.append(max(closing, max(0.0, -gap)))
+    return np.sort(np.array(out))
+
+
+def test_gpu_contact_errors_match_the_host():
+    """The step-end complementarity error of every contact point (vxr_box_contact_errors) against the same
+    quantity in doubles from the state read back, as sorted sets (the GPU lists points in round order)."""
+    sc = scenes.large_mixed(2048, seed=4, volume=(16.0, 8.0, 16.0))
+    w = Lm.settled_world(sc, 90, 16)
+    got = np.sort(w.contact_errors())
+    h = B.bits_f32(sc["params"][B.H])
+    margin = B.bits_f32(sc["params"][B.MARGIN])
+    want = host_contact_errors(w, sc, h, margin)
+    assert len(got) == len(want) and len(got) > 100
+    np.testing.assert_allclose(got, want, atol=2e-6, rtol=1e-4)
+    assert want.max() > 0.0
+    w.close()

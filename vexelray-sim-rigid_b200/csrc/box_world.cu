@@ -207,6 +207,8 @@ struct vxr_box_world {
     int events_used = 0;
     double phase_ms[4] = {0, 0, 0, 0};
     long long* activity = nullptr;  // device scratch for vxr_box_activity
+    float* errors = nullptr;        // vxr_box_contact_errors' rows
+    int err_rows = 0;
     // batched scenes (vxr_box_create_batch): each scene's parameter words and grid, each body's scene
     int scenes = 0;
     int scene_params_set = 0;
@@ -1995,6 +1997,39 @@ __global__ void k_diag_contacts(const int* __restrict__ touching_n, const PairGe
     atomicMax(&d->max_penetration, __float_as_uint(fmaxf(deepest, 0.0f)));
 }
 
+// The positional complementarity error at each contact point of the last step, from the bodies' state at its end
+// (no reference counterpart; the reference has no residual): the depth the relative normal velocity would close
+// within a substep beyond what the gap allows, h max(0, -(vn + max(gap, 0) / h)) for a point within the margin, and
+// the depth the bodies already overlap, max(0, -gap); the larger. A row is (round-order position x 4 + point slot);
+// rows past a pair's point count are -1.
+__global__ void k_contact_errors(const int* __restrict__ touching_n, const PairGen last, const Bodies b, Params P,
+                                 float* __restrict__ out) {
+    const int total = *touching_n;
+    const float h = P.w[P_H], margin = P.w[P_MARGIN];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const int4 rec = last.pair[k];
+        const float4 nm = last.normal[k];
+        const float n[3] = {nm.x, nm.y, nm.z};
+        Held A, B;
+        A.load(b.pose[rec.x], b.turn[rec.x], b.half[rec.x], b.vel[rec.x], b.mom[rec.x], b.inv[rec.x]);
+        B.load(b.pose[rec.y], b.turn[rec.y], b.half[rec.y], b.vel[rec.y], b.mom[rec.y], b.inv[rec.y]);
+        for (int slot = 0; slot < MOST_POINTS; slot++) {
+            float e = -1.0f;
+            if (slot < rec.z) {
+                const size_t at = (size_t)last.pstart[k] + slot;
+                float rA[3], rB[3], rel[3];
+                point_of(A, B, n, last.pa[at], last.pb[at], rA, rB, rel);
+                float gap = 0.0f;
+                for (int j = 0; j < 3; j++) gap += ((B.at[j] + rB[j]) - (A.at[j] + rA[j])) * n[j];
+                const float vn = rel[0] * n[0] + rel[1] * n[1] + rel[2] * n[2];
+                const float closing = gap <= margin ? h * fmaxf(0.0f, -(vn + fmaxf(gap, 0.0f) / h)) : 0.0f;
+                e = fmaxf(closing, fmaxf(0.0f, -gap));
+            }
+            out[(size_t)k * MOST_POINTS + slot] = e;
+        }
+    }
+}
+
 // Boxes.show :801-820.
 __global__ void k_show(int n, const Bodies b, float* __restrict__ shown) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2807,6 +2842,30 @@ int32_t vxr_box_features(vxr_box_world* w, float* features16, float* targets2, i
         }
     *rows = k;
     return VXR_OK;
+}
+
+int32_t vxr_box_contact_errors(vxr_box_world* w, float* out, int32_t capacity) {
+    if (!w || capacity < 0) return -VXR_EINVAL;
+    if (!w->has_grid) return 0;
+    cudaSetDevice(w->device);
+    const PairGen& last = w->gen[w->cur ^ 1];
+    int touching = 0;
+    if (cudaMemcpy(&touching, last.tstart + w->n, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -fail(w, "reading the touching count");
+    const int rows = touching * MOST_POINTS;
+    if (!out) return rows;
+    if (capacity < rows) return -VXR_EINVAL;
+    if (rows == 0) return 0;
+    if (w->err_rows < rows) {
+        if (alloc(w, &w->errors, (size_t)rows)) return -VXR_ECUDA;
+        w->err_rows = rows;
+    }
+    k_contact_errors<<<w->sms * 4, THREADS, 0, w->stream>>>(last.tstart + w->n, last, w->b, w->params, w->errors);
+    if (cudaGetLastError() != cudaSuccess) return -fail(w, "contact errors kernel");
+    if (cudaMemcpyAsync(out, w->errors, sizeof(float) * rows, cudaMemcpyDeviceToHost, w->stream) != cudaSuccess ||
+        cudaStreamSynchronize(w->stream) != cudaSuccess)
+        return -fail(w, "reading the contact errors");
+    return rows;
 }
 
 int32_t vxr_box_diagnostics(vxr_box_world* w, vxr_box_diag* out) {

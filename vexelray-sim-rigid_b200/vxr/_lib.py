@@ -25,7 +25,7 @@ SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_c
            "vxr_box_measure", "vxr_box_wait_limit", "vxr_box_islands", "vxr_box_paths", "vxr_box_residuals", "vxr_box_create_batch", "vxr_box_scene_params",
            "vxr_box_scenes", "vxr_box_step_graph", "vxr_mlp_create", "vxr_mlp_destroy", "vxr_mlp_error",
            "vxr_mlp_set", "vxr_mlp_get", "vxr_mlp_forward", "vxr_mlp_gradients", "vxr_mlp_train", "vxr_box_learned",
-           "vxr_box_features", "vxr_box_diagnostics", "vxr_sphere_diagnostics", "vxr_ring_create", "vxr_ring_destroy",
+           "vxr_box_features", "vxr_box_diagnostics", "vxr_box_contact_errors", "vxr_sphere_diagnostics", "vxr_ring_create", "vxr_ring_destroy",
            "vxr_ring_error", "vxr_ring_install", "vxr_ring_back", "vxr_ring_publish", "vxr_ring_keep", "vxr_ring_take",
            "vxr_ring_wait", "vxr_ring_read", "vxr_ring_retired", "vxr_ring_live", "vxr_box_shown_device",
            "vxr_sphere_shown_device", "vxr_picture", "vxr_picture_host",
@@ -201,6 +201,8 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_features.restype = i32
         L.vxr_box_diagnostics.argtypes = [vp, ctypes.POINTER(Diag)]
         L.vxr_box_diagnostics.restype = i32
+        L.vxr_box_contact_errors.argtypes = [vp, vp, i32]
+        L.vxr_box_contact_errors.restype = i32
         L.vxr_sphere_diagnostics.argtypes = [vp, ctypes.POINTER(Diag)]
         L.vxr_sphere_diagnostics.restype = i32
         L.vxr_ring_create.argtypes = [i32]

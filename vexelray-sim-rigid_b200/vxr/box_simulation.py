@@ -286,6 +286,19 @@ class BoxSimulation:
         VXR_ETIMEOUT."""
         self._check(self.L.vxr_box_wait_limit(self.h, int(ns)))
 
+    def contact_errors(self) -> np.ndarray:
+        """The positional complementarity error (m) at every contact point of the last step, from the state at its
+        end: max(h max(0, -(vn + max(gap, 0) / h)) within the margin, max(0, -gap))."""
+        rows = self.L.vxr_box_contact_errors(self.h, None, 0)
+        if rows < 0:
+            raise VxrError(-rows, self.error())
+        out = np.zeros(max(rows, 1), np.float32)
+        got = self.L.vxr_box_contact_errors(self.h, ptr(out), rows)
+        if got < 0:
+            raise VxrError(-got, self.error())
+        out = out[:got]
+        return out[out >= 0.0]
+
     def islands(self, enable: bool = True) -> None:
         """Small components solved by island blocks (the default), or every body through the grid-wide phases; the
         results are the same either way."""
