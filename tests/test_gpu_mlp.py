@@ -7,9 +7,15 @@ from oracle import mlp as M
 
 pytestmark = pytest.mark.gpu
 
-# BF16 operands carry 8 significant bits; the products accumulate in FP32 on the GPU and in float64 in the oracle.
-OUT_TOL = 2e-2   # forward: relative to the outputs' scale
-GRAD_TOL = 3e-2  # gradients: relative to each gradient block's scale
+# The oracle rounds to BF16 exactly where the kernels do (weights, inputs, hidden activations, deltas), so the two
+# differ only by FP32 against float64 accumulation and by the SiLU's exponential (expf against exp). Either can move
+# an activation across a BF16 rounding boundary, which changes it by one BF16 step (2^-8 relative) and its
+# descendants by less. So the largest difference is held to 0.5% of a block's scale, and the typical one (the
+# median) to 1e-4 of it: a product laid out wrong (a K-chunk or a row block misplaced) moves most elements, and
+# fails the median however small its effect on the largest.
+OUT_TOL = 5e-3     # forward, largest difference: relative to the outputs' scale
+GRAD_TOL = 5e-3    # gradients, largest difference: relative to each gradient block's scale
+TYPICAL_TOL = 1e-4  # median difference, relative to the scale
 
 
 def net(seed=0):
@@ -21,6 +27,10 @@ def rel_err(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-12))
 
 
+def typical_err(a, b):
+    return float(np.median(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-12))
+
+
 def test_gpu_mlp_forward_matches_the_oracle():
     """1,000 rows (a ragged last tile) through the GPU's weights: the same outputs as the oracle's forward."""
     rng = np.random.default_rng(1)
@@ -29,7 +39,8 @@ def test_gpu_mlp_forward_matches_the_oracle():
     y = n.forward(x)
     p, mean, inv = n.get()
     want, _ = M.forward(p, (x - mean) * inv)
-    assert rel_err(y, want) < OUT_TOL
+    assert rel_err(y, want) < OUT_TOL, rel_err(y, want)
+    assert typical_err(y, want) < TYPICAL_TOL, typical_err(y, want)
     n.close()
 
 
@@ -44,8 +55,9 @@ def test_gpu_mlp_gradients_match_the_oracle():
     p, _, _ = n.get()
     want, want_loss = M.gradients(p, x, t)
     for k in want:
-        assert rel_err(g[k], want[k]) < GRAD_TOL, k
-    assert abs(loss - want_loss) / want_loss < 1e-2
+        assert rel_err(g[k], want[k]) < GRAD_TOL, (k, rel_err(g[k], want[k]))
+        assert typical_err(g[k], want[k]) < TYPICAL_TOL, (k, typical_err(g[k], want[k]))
+    assert abs(loss - want_loss) / want_loss < 1e-3
     n.close()
 
 
@@ -77,5 +89,7 @@ def test_gpu_mlp_training_fits_a_smooth_function():
     assert after < 0.1 * before, (before, after, losses)
     p, mean, inv = n.get()
     want, _ = M.forward(p, (x[:2000] - mean) * inv)
-    assert rel_err(n.forward(x[:2000]), want) < OUT_TOL
+    got = n.forward(x[:2000])
+    assert rel_err(got, want) < OUT_TOL, rel_err(got, want)
+    assert typical_err(got, want) < TYPICAL_TOL, typical_err(got, want)
     n.close()
