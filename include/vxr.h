@@ -452,7 +452,8 @@ typedef struct {
 } vxr_sphere_diag;
 int32_t vxr_sphere_diagnostics(vxr_sphere_world* world, vxr_sphere_diag* out);
 
-/* Blocks the world's kernel runs on, and kernels its steps have launched (reading the state back is not
+/* Blocks the world's kernel runs on (a cluster chosen by default that the GPU cannot place falls back to 8 blocks,
+ * then to one: this says which was taken), and kernels its steps have launched (reading the state back is not
  * counted). */
 int32_t vxr_sphere_blocks(const vxr_sphere_world* world);
 int64_t vxr_sphere_launches(const vxr_sphere_world* world);

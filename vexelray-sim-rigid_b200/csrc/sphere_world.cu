@@ -1495,27 +1495,42 @@ vxr_sphere_world* vxr_sphere_create(const vxr_sphere_config* cfg, int32_t* statu
     // 9.4 ms on one block; 12 and 16 blocks gain nothing more.
     // From VXR_SPHERE_CLUSTER_WIDE_FROM spheres, VXR_SPHERE_CLUSTER_WIDE blocks: on the reference's 4,096-sphere
     // pile, 3.28 ms a step against 4.05 on 8 (Gauss-Seidel until done, friction on).
-    int cluster = cfg->cluster;
-    if (cluster == 0 && cfg->blocks == 0 && n >= VXR_SPHERE_CLUSTER_FROM && n <= VXR_SPHERE_ONE_BLOCK)
-        cluster = n >= VXR_SPHERE_CLUSTER_WIDE_FROM ? VXR_SPHERE_CLUSTER_WIDE : VXR_SPHERE_CLUSTER;
-    if (cluster > 1) {  // one thread-block cluster of `cluster` blocks (at most 16, one a SM)
-        if (cluster > 16) return bad(VXR_EINVAL);
-        if (cluster > 8 &&
-            cudaFuncSetAttribute(k_sphere_steps, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
-            return bad(VXR_EINVAL);
+    // A cluster asked for by the caller must fit, or the world is refused; one chosen here falls back to 8 blocks,
+    // then to one block, where the GPU cannot place it (shared under MPS, or with fewer SMs free). vxr_sphere_blocks
+    // tells which was taken.
+    auto cluster_fits = [&](int size) {
+        if (size > 16) return false;
+        if (size > 8 &&
+            cudaFuncSetAttribute(k_sphere_steps, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
         cudaLaunchConfig_t c = {};
-        c.gridDim = dim3(cluster);
+        c.gridDim = dim3(size);
         c.blockDim = dim3(THREADS);
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = cluster;
+        attr[0].val.clusterDim.x = size;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
         c.attrs = attr;
         c.numAttrs = 1;
         int clusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_sphere_steps, &c) != cudaSuccess || clusters < 1)
-            return bad(VXR_EINVAL);
+        if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_sphere_steps, &c) != cudaSuccess || clusters < 1) {
+            cudaGetLastError();
+            return false;
+        }
+        return true;
+    };
+    int cluster = cfg->cluster;
+    if (cluster > 1) {  // asked for: one thread-block cluster of `cluster` blocks (at most 16, one a SM)
+        if (!cluster_fits(cluster)) return bad(VXR_EINVAL);
+    } else if (cluster == 0 && cfg->blocks == 0 && n >= VXR_SPHERE_CLUSTER_FROM && n <= VXR_SPHERE_ONE_BLOCK) {
+        cluster = n >= VXR_SPHERE_CLUSTER_WIDE_FROM ? VXR_SPHERE_CLUSTER_WIDE : VXR_SPHERE_CLUSTER;
+        if (!cluster_fits(cluster)) cluster = cluster > VXR_SPHERE_CLUSTER && cluster_fits(VXR_SPHERE_CLUSTER)
+                                                  ? VXR_SPHERE_CLUSTER : 1;
+    }
+    if (cluster > 1) {
         w->blocks = cluster;
         w->cluster = 1;
     }
