@@ -61,6 +61,8 @@ struct ListGen {
     int* next;     // [cap] the lower sphere's previous contact, or -1
     float4* imp;   // [2 cap] (normal, p), (q, -): what it has taken this substep
     int* head;     // [n] the lower sphere's last contact, or -1
+    int* start;    // [n + 1] where the lower sphere's contacts begin: they take places start .. head, one after
+                   // another, so its chain (head, next, ...) is that range from the top down
 };
 
 struct Counts {
@@ -93,7 +95,6 @@ struct Kernel {
     int* claims;       // [3 n]
     int* list_count;   // [n]
     int* part;         // [blocks] each block's slice total in a scan the blocks share
-    int* list_start;   // [n + 1]
     ListGen gen[2];
     Counts* counts;
     int* opening;      // [iterations] the rounds each pass's opening batch runs (SphereStepper.opening)
@@ -412,10 +413,14 @@ __device__ __forceinline__ int cell_key(const Kernel& K, float x, float y, float
 
 // Spheres.around :1207-1229: every sphere of s's cell and the 26 around it, each cell in the sort's order; with no
 // grid, every sphere in index order.
+// visit(o, pos[o]) for each. The spheres of a run are fetched four at a time, their order entries and then their
+// positions each as one batch of independent loads, before the four are visited in turn: the same spheres in the same
+// order, with one memory round trip a batch instead of two a sphere.
 template <typename Visit>
 __device__ __forceinline__ void around(const Kernel& K, int s, Visit visit) {
+    const float4* pos = K.s.pos;
     if (!K.gridded) {
-        for (int o = 0; o < K.n; o++) visit(o);
+        for (int o = 0; o < K.n; o++) visit(o, pos[o]);
         return;
     }
     const int key = K.keys[s];
@@ -428,7 +433,22 @@ __device__ __forceinline__ void around(const Kernel& K, int s, Visit visit) {
         if (!(jy >= 0 && jy < K.ny && jz >= 0 && jz < K.nz)) continue;
         const int first = x0 + K.nx * (jy + K.ny * jz);
         const int end = K.cell_start[first + (x1 - x0) + 1];
-        for (int k = K.cell_start[first]; k < end; k++) visit(K.order[k]);
+        for (int k = K.cell_start[first]; k < end; k += 4) {
+            const int m = min(4, end - k);
+            int o0 = K.order[k], o1 = 0, o2 = 0, o3 = 0;
+            if (m > 1) o1 = K.order[k + 1];
+            if (m > 2) o2 = K.order[k + 2];
+            if (m > 3) o3 = K.order[k + 3];
+            float4 p0 = pos[o0], p1 = p0, p2 = p0, p3 = p0;
+            if (m > 1) p1 = pos[o1];
+            if (m > 2) p2 = pos[o2];
+            if (m > 3) p3 = pos[o3];
+            for (int j = 0; j < m; j++) {
+                visit(o0, p0);
+                o0 = o1, o1 = o2, o2 = o3;
+                p0 = p1, p1 = p2, p2 = p3;
+            }
+        }
     }
 }
 
@@ -549,9 +569,8 @@ __device__ __forceinline__ void jacobi_solve(const Kernel& K, int s) {
     const float rs = me.w, ws = S.disp[s].w;
     float sum[3] = {0.0f, 0.0f, 0.0f};
     float contacts = 0.0f;
-    around(K, s, [&](int o) {
+    around(K, s, [&](int o, float4 other) {
         if (o == s) return;
-        const float4 other = S.pos[o];
         float d[3] = {mine[0] - other.x, mine[1] - other.y, mine[2] - other.z};
         const float d2 = d[0] * d[0] + (d[1] * d[1] + d[2] * d[2]);
         const float reach = rs + other.w;
@@ -620,9 +639,8 @@ __device__ __forceinline__ void bounce(const Kernel& K, int s) {
     const float4 v4 = S.vel[s], c4 = S.cvel[s];
     const float vel[3] = {v4.x, v4.y, v4.z}, was[3] = {c4.x, c4.y, c4.z};
     float sum[3] = {0.0f, 0.0f, 0.0f};
-    around(K, s, [&](int o) {
+    around(K, s, [&](int o, float4 other) {
         if (o == s) return;
-        const float4 other = S.pos[o];
         float d[3] = {mine[0] - other.x, mine[1] - other.y, mine[2] - other.z};
         const float d2 = d[0] * d[0] + (d[1] * d[1] + d[2] * d[2]);
         const float near = (ra + other.w) * (1.0f + LIST_MARGIN);
@@ -697,9 +715,8 @@ __device__ __forceinline__ void show(const Kernel& K, int s) {
             lean[a] = lean[a] + 1.0f * share;
         }
     }
-    around(K, s, [&](int o) {
+    around(K, s, [&](int o, float4 other) {
         if (o == s) return;
-        const float4 other = S.pos[o];
         float d[3] = {other.x - mine[0], other.y - mine[1], other.z - mine[2]};
         const float d2 = dotf(d, d);
         const float reach = rs + other.w;
@@ -730,9 +747,8 @@ __device__ __forceinline__ void show(const Kernel& K, int s) {
 __device__ __forceinline__ int count_near(const Kernel& K, int a) {
     const float4 me = K.s.pos[a];
     int found = 0;
-    around(K, a, [&](int o) {
+    around(K, a, [&](int o, float4 other) {
         if (!(o > a)) return;
-        const float4 other = K.s.pos[o];
         const float d0 = me.x - other.x, d1 = me.y - other.y, d2v = me.z - other.z;
         const float d2 = d0 * d0 + (d1 * d1 + d2v * d2v);
         const float near = (me.w + other.w) * (1.0f + LIST_MARGIN);
@@ -745,12 +761,15 @@ __device__ __forceinline__ int count_near(const Kernel& K, int a) {
 // impulses the pair took in the substep before (found by walking a's kept chain, at most MOST_KEPT places).
 __device__ __forceinline__ void fill_near(const Kernel& K, const ListGen& L, const ListGen& kept, int a) {
     const float4 me = K.s.pos[a];
-    const int first = K.list_start[a];
+    const int first = L.start[a];
     int slot = first;
     int last = -1;
-    around(K, a, [&](int o) {
+    // a's kept chain, at most MOST_KEPT places from its head: the places of that range, searched with independent
+    // loads (each partner is listed once, so the place found is the one the walk down the chain finds)
+    const int top = kept.head[a];
+    const int bottom = top >= 0 ? max(kept.start[a], top - (MOST_KEPT - 1)) : 0;
+    around(K, a, [&](int o, float4 other) {
         if (!(o > a)) return;
-        const float4 other = K.s.pos[o];
         const float d0 = me.x - other.x, d1 = me.y - other.y, d2v = me.z - other.z;
         const float d2 = d0 * d0 + (d1 * d1 + d2v * d2v);
         const float near = (me.w + other.w) * (1.0f + LIST_MARGIN);
@@ -762,16 +781,12 @@ __device__ __forceinline__ void fill_near(const Kernel& K, const ListGen& L, con
         L.next[at] = last;
         last = at;
         float4 w0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), w1 = w0;
-        int j = kept.head[a];
-        int walked = 0;
-        while (j >= 0 && walked < MOST_KEPT) {
-            if (kept.pair[j].y == o) {
+        for (int j = top; j >= bottom; j--) {
+            if (__ldg(&kept.pair[j].y) == o) {
                 w0 = kept.imp[2 * (size_t)j];
                 w1 = kept.imp[2 * (size_t)j + 1];
-                walked = MOST_KEPT;
+                break;
             }
-            j = kept.next[j];
-            walked++;
         }
         L.imp[2 * (size_t)at] = w0;
         L.imp[2 * (size_t)at + 1] = w1;
@@ -779,37 +794,68 @@ __device__ __forceinline__ void fill_near(const Kernel& K, const ListGen& L, con
     L.head[a] = last;
 }
 
+// The list places a thread owns for a substep (place gtid + j gsize for j < HELD_PLACES), their pairs held in
+// registers from the list's fill to the substep's end, and which of them this pass has done: a round reads neither
+// from memory. No other thread writes a place's pair or its done mark.
+constexpr int HELD_PLACES = 2;
+struct HeldPlaces {
+    int2 pair[HELD_PLACES];
+    unsigned done;
+};
+
+// One place of a dispatch: solve it if it won the dispatch before (its priority holds both spheres' claims), else
+// clear the spheres' checks and claim them for this dispatch (and note the pass still open). Returns whether it was
+// solved.
+__device__ __forceinline__ bool contact_place(const Kernel& K, const ListGen& L, int c, int2 ab, int checks,
+                                              int claims, int pass, int dispatch, int check_dispatch, int rubs,
+                                              const int* checked, int* claimed, int* cleared, bool& open) {
+    const int pair = ab.x * K.n + ab.y;
+    int won = 0;
+    if (checks > 0) {
+        const int last = priority(pair, check_dispatch);
+        if (checked[ab.x] == last && checked[ab.y] == last) won = 1;
+    }
+    if (won) {
+        contact(K, L.imp + 2 * (size_t)c, ab.x, ab.y, pass, rubs);
+        L.done[c] = pass;
+        return true;
+    }
+    cleared[ab.x] = 0;
+    cleared[ab.y] = 0;
+    if (claims > 0) {
+        open = true;
+        const int mine = priority(pair, dispatch);
+        atomicMax(&claimed[ab.x], mine);
+        atomicMax(&claimed[ab.y], mine);
+    } else {
+        atomicAdd(&K.counts->count[MISSED], 1);
+    }
+    return false;
+}
+
 // Spheres.contactRound :1076-1133, one dispatch over the list. The winners of a dispatch share no sphere (each
 // sphere's claim is held by one priority), so they solve in parallel with the result of any serial order.
 __device__ __forceinline__ void contact_round(const Kernel& K, const ListGen& L, int listed, int checks, int claims,
                                               int pass, int dispatch, int mark, int check_dispatch, int rubs,
-                                              const int* checked, int* claimed, int* cleared, int gtid, int gsize) {
+                                              const int* checked, int* claimed, int* cleared, int gtid, int gsize,
+                                              HeldPlaces& mine) {
     if (gtid == 0) K.counts->open[1 - mark] = 0;
-    for (int c = gtid; c < listed; c += gsize) {
-        if (L.done[c] == pass) continue;
-        const int2 ab = L.pair[c];
-        const int pair = ab.x * K.n + ab.y;
-        int won = 0;
-        if (checks > 0) {
-            const int last = priority(pair, check_dispatch);
-            if (checked[ab.x] == last && checked[ab.y] == last) won = 1;
-        }
-        if (won) {
-            contact(K, L.imp + 2 * (size_t)c, ab.x, ab.y, pass, rubs);
-            L.done[c] = pass;
-        } else {
-            cleared[ab.x] = 0;
-            cleared[ab.y] = 0;
-            if (claims > 0) {
-                K.counts->open[mark] = 1;
-                const int mine = priority(pair, dispatch);
-                atomicMax(&claimed[ab.x], mine);
-                atomicMax(&claimed[ab.y], mine);
-            } else {
-                atomicAdd(&K.counts->count[MISSED], 1);
-            }
-        }
+    bool open = false;
+#pragma unroll
+    for (int j = 0; j < HELD_PLACES; j++) {
+        const int c = gtid + j * gsize;
+        if (c < listed && !((mine.done >> j) & 1u) &&
+            contact_place(K, L, c, mine.pair[j], checks, claims, pass, dispatch, check_dispatch, rubs, checked,
+                          claimed, cleared, open))
+            mine.done |= 1u << j;
     }
+    for (int c = gtid + HELD_PLACES * gsize; c < listed; c += gsize) {
+        if (L.done[c] == pass) continue;
+        contact_place(K, L, c, L.pair[c], checks, claims, pass, dispatch, check_dispatch, rubs, checked, claimed,
+                      cleared, open);
+    }
+    // one store a warp that left a place open, not one a place
+    if (__any_sync(0xffffffffu, open) && (threadIdx.x & 31) == 0) K.counts->open[mark] = 1;
 }
 
 __device__ __forceinline__ int position(int k) { return k == 0 ? 0 : 1 + (k - 1) % CYCLE; }
@@ -960,10 +1006,11 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
             if (gs) {
                 for (int a = gtid; a < n; a += gsize) K.list_count[a] = count_near(K, a);
                 SYNC();
-                scan_slices(K, K.list_count, K.list_start, n);
+                int* start = K.gen[cur ^ 1].start;  // the new list's
+                scan_slices(K, K.list_count, start, n);
                 SYNC();
                 {
-                    const int whole = scan_finish(K, K.list_start, n);
+                    const int whole = scan_finish(K, start, n);
                     if (gtid == 0) K.counts->count[LISTED] = whole;
                 }
                 SYNC();
@@ -974,6 +1021,13 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
                 listed = min(read_int(&K.counts->count[LISTED]), K.cap);
             }
             const ListGen L = K.gen[cur];
+            HeldPlaces mine;
+            mine.done = 0u;
+#pragma unroll
+            for (int j = 0; j < HELD_PLACES; j++) {
+                const int c = gtid + j * gsize;
+                mine.pair[j] = gs && c < listed ? L.pair[c] : make_int2(0, 0);
+            }
             for (int it = 0; it < K.iterations; it++) {
                 if (K.solve == 0) {
                     for (int s = gtid; s < n; s += gsize) jacobi_solve(K, s);
@@ -984,11 +1038,12 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
                 }
                 if (K.solve == 2) {
                     // rounds 0..R on dispatches counted over the substep's passes (SphereStep.byContact :216-262)
+                    mine.done = 0u;
                     for (int k = 0; k <= K.rounds; k++) {
                         const int g = it * (K.rounds + 1) + k;
                         contact_round(K, L, listed, k == 0 ? 0 : 1, k == K.rounds ? 0 : 1, it + 1, g, g % 2, g - 1,
                                       0, K.claims + ((g + 2) % 3) * n, K.claims + (g % 3) * n,
-                                      K.claims + ((g + 1) % 3) * n, gtid, gsize);
+                                      K.claims + ((g + 1) % 3) * n, gtid, gsize, mine);
                         SYNC();
                     }
                     for (int s = gtid; s < n; s += gsize) walls(K, s);
@@ -999,12 +1054,13 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
                 int k = read_int(&K.opening[it]);
                 int waits = 0;
                 int from = 0;
+                mine.done = 0u;
                 for (;;) {
                     for (int j = from; j < k; j++) {
                         const int p = position(j);
                         contact_round(K, L, listed, p == 0 ? 0 : 1, 1, it + 1, it * CYCLE + p % CYCLE, p % 2,
                                       it * CYCLE + max(p - 1, 0) % CYCLE, 0, K.claims + ((p + 2) % 3) * n,
-                                      K.claims + (p % 3) * n, K.claims + ((p + 1) % 3) * n, gtid, gsize);
+                                      K.claims + (p % 3) * n, K.claims + ((p + 1) % 3) * n, gtid, gsize, mine);
                         SYNC();
                     }
                     waits++;
@@ -1023,12 +1079,13 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
                 }
                 if (K.friction) {
                     // the same dispatches again, rubbing (SphereStep.rubs :271-278)
+                    mine.done = 0u;
                     for (int j = 0; j < k; j++) {
                         const int p = position(j);
                         contact_round(K, L, listed, p == 0 ? 0 : 1, 1, K.iterations + it + 1,
                                       it * CYCLE + p % CYCLE, p % 2, it * CYCLE + max(p - 1, 0) % CYCLE, 1,
                                       K.claims + ((p + 2) % 3) * n, K.claims + (p % 3) * n,
-                                      K.claims + ((p + 1) % 3) * n, gtid, gsize);
+                                      K.claims + ((p + 1) % 3) * n, gtid, gsize, mine);
                         SYNC();
                     }
                 }
@@ -1091,9 +1148,8 @@ __global__ void k_sphere_diag(Kernel K, SDiag* d) {
         const float f[9] = {p.x, p.y, p.z, v.x, v.y, v.z, w.x, w.y, w.z};
         for (int k = 0; k < 9; k++)
             if (!isfinite(f[k])) broken = 1;
-        around(K, s, [&](int o) {
+        around(K, s, [&](int o, float4 q) {
             if (!(o > s)) return;
-            const float4 q = S.pos[o];
             const double dx = (double)p.x - q.x, dy = (double)p.y - q.y, dz = (double)p.z - q.z;
             const double depth = (double)(r + q.w) - sqrt(dx * dx + dy * dy + dz * dz);
             overlap = fmaxf(overlap, (float)(depth / fmin((double)r, (double)q.w)));
@@ -1153,7 +1209,7 @@ struct vxr_sphere_world {
     float* shown = nullptr;
     int *keys = nullptr, *order = nullptr, *cell_count = nullptr, *cell_start = nullptr;
     int* part = nullptr;  // [blocks] the blocks' slice totals of a shared scan
-    int *claims = nullptr, *list_count = nullptr, *list_start = nullptr;
+    int *claims = nullptr, *list_count = nullptr;
     ListGen gen[2]{};
     Counts* counts = nullptr;
     Counts* host_counts = nullptr;  // pinned
@@ -1251,6 +1307,7 @@ int write_state(vxr_sphere_world* w, const float* const* fields24, const float* 
     if (w->solve != 0) {
         for (int g = 0; g < 2; g++) {
             SPH_CUDA(cudaMemsetAsync(w->gen[g].head, 0xFF, sizeof(int) * (size_t)n, st));
+            SPH_CUDA(cudaMemsetAsync(w->gen[g].start, 0, sizeof(int) * ((size_t)n + 1), st));
             SPH_CUDA(cudaMemsetAsync(w->gen[g].done, 0, sizeof(int) * (size_t)w->cap, st));
         }
     }
@@ -1287,7 +1344,6 @@ Kernel kernel_of(vxr_sphere_world* w, int steps) {
     K.cell_start = w->cell_start;
     K.claims = w->claims;
     K.list_count = w->list_count;
-    K.list_start = w->list_start;
     K.part = w->part;
     K.gen[0] = w->gen[0];
     K.gen[1] = w->gen[1];
@@ -1472,8 +1528,8 @@ vxr_sphere_world* vxr_sphere_create(const vxr_sphere_config* cfg, int32_t* statu
     }
     if (w->solve != 0) {
         rc |= salloc(w, &w->list_count, n);
-        rc |= salloc(w, &w->list_start, (size_t)n + 1);
         for (int g = 0; g < 2; g++) {
+            rc |= salloc(w, &w->gen[g].start, (size_t)n + 1);
             rc |= salloc(w, &w->gen[g].pair, w->cap);
             rc |= salloc(w, &w->gen[g].done, w->cap);
             rc |= salloc(w, &w->gen[g].next, w->cap);
