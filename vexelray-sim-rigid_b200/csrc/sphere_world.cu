@@ -32,6 +32,7 @@ constexpr float COINCIDENT = 1e-12f;   // Spheres.java:157
 constexpr float LIST_MARGIN = 0.02f;   // Spheres.java:795
 constexpr float INERTIA = 0.4f;        // Spheres.java:247
 constexpr int MOST_KEPT = 32;          // Spheres.java:944
+constexpr int NEAR_KEPT = 16;          // near partners a sphere's count keeps for the list's fill
 constexpr int CYCLE = 48, BATCH = 8;   // SphereStep.java:53-59
 constexpr int SHRINK_AFTER = 120;      // SphereStepper.java:53
 constexpr int SHOWN = 40, PRESSED_BEFORE = 8, PRESSED_AFTER = 20, TURNED_BEFORE = 32, TURNED_AFTER = 36;
@@ -94,6 +95,7 @@ struct Kernel {
     int* cell_start;   // [cells + 1]
     int* claims;       // [3 n]
     int* list_count;   // [n]
+    int* near;         // [n * NEAR_KEPT] each sphere's first near partners, in the walk's order
     int* part;         // [blocks] each block's slice total in a scan the blocks share
     ListGen gen[2];
     Counts* counts;
@@ -413,14 +415,19 @@ __device__ __forceinline__ int cell_key(const Kernel& K, float x, float y, float
 
 // Spheres.around :1207-1229: every sphere of s's cell and the 26 around it, each cell in the sort's order; with no
 // grid, every sphere in index order.
-// visit(o, pos[o]) for each. The spheres of a run are fetched four at a time, their order entries and then their
-// positions each as one batch of independent loads, before the four are visited in turn: the same spheres in the same
-// order, with one memory round trip a batch instead of two a sphere.
-template <typename Visit>
+// visit(o, pos[o]) for each (with WEIGHTS, visit(o, pos[o], disp[o].w): the inverse mass comes in the same batch).
+// The spheres of a run are fetched four at a time, their order entries and then their positions each as one batch of
+// independent loads, before the four are visited in turn: the same spheres in the same order, with one memory round
+// trip a batch instead of two or three a sphere.
+template <bool WEIGHTS = false, typename Visit>
 __device__ __forceinline__ void around(const Kernel& K, int s, Visit visit) {
     const float4* pos = K.s.pos;
+    const float4* disp = K.s.disp;
     if (!K.gridded) {
-        for (int o = 0; o < K.n; o++) visit(o, pos[o]);
+        for (int o = 0; o < K.n; o++) {
+            if constexpr (WEIGHTS) visit(o, pos[o], disp[o].w);
+            else visit(o, pos[o]);
+        }
         return;
     }
     const int key = K.keys[s];
@@ -443,10 +450,19 @@ __device__ __forceinline__ void around(const Kernel& K, int s, Visit visit) {
             if (m > 1) p1 = pos[o1];
             if (m > 2) p2 = pos[o2];
             if (m > 3) p3 = pos[o3];
+            float w0 = 0.0f, w1 = 0.0f, w2 = 0.0f, w3 = 0.0f;
+            if constexpr (WEIGHTS) {
+                w0 = disp[o0].w;
+                if (m > 1) w1 = disp[o1].w;
+                if (m > 2) w2 = disp[o2].w;
+                if (m > 3) w3 = disp[o3].w;
+            }
             for (int j = 0; j < m; j++) {
-                visit(o0, p0);
+                if constexpr (WEIGHTS) visit(o0, p0, w0);
+                else visit(o0, p0);
                 o0 = o1, o1 = o2, o2 = o3;
                 p0 = p1, p1 = p2, p2 = p3;
+                w0 = w1, w1 = w2, w2 = w3;
             }
         }
     }
@@ -569,12 +585,12 @@ __device__ __forceinline__ void jacobi_solve(const Kernel& K, int s) {
     const float rs = me.w, ws = S.disp[s].w;
     float sum[3] = {0.0f, 0.0f, 0.0f};
     float contacts = 0.0f;
-    around(K, s, [&](int o, float4 other) {
+    around<true>(K, s, [&](int o, float4 other, float wo) {
         if (o == s) return;
         float d[3] = {mine[0] - other.x, mine[1] - other.y, mine[2] - other.z};
         const float d2 = d[0] * d[0] + (d[1] * d[1] + d[2] * d[2]);
         const float reach = rs + other.w;
-        const float wsum = ws + S.disp[o].w;
+        const float wsum = ws + wo;
         if (!(d2 < reach * reach)) return;
         if (!(d2 > COINCIDENT)) return;
         if (!(wsum > 0.0f)) return;
@@ -744,15 +760,21 @@ __device__ __forceinline__ void show(const Kernel& K, int s) {
 // --- the contact list ----------------------------------------------------------------------------------------
 
 // listContacts' first half: how many spheres of higher index are near sphere a (Spheres.listContacts :961-1022).
+// listContacts' first half: how many higher-numbered spheres are near a. The first NEAR_KEPT of them, in the walk's
+// order, are kept in K.near for the fill, which then needs no second walk.
 __device__ __forceinline__ int count_near(const Kernel& K, int a) {
     const float4 me = K.s.pos[a];
     int found = 0;
+    int* keep = K.near + (size_t)a * NEAR_KEPT;
     around(K, a, [&](int o, float4 other) {
         if (!(o > a)) return;
         const float d0 = me.x - other.x, d1 = me.y - other.y, d2v = me.z - other.z;
         const float d2 = d0 * d0 + (d1 * d1 + d2v * d2v);
         const float near = (me.w + other.w) * (1.0f + LIST_MARGIN);
-        if (d2 < near * near) found++;
+        if (d2 < near * near) {
+            if (found < NEAR_KEPT) keep[found] = o;
+            found++;
+        }
     });
     return found;
 }
@@ -768,12 +790,7 @@ __device__ __forceinline__ void fill_near(const Kernel& K, const ListGen& L, con
     // loads (each partner is listed once, so the place found is the one the walk down the chain finds)
     const int top = kept.head[a];
     const int bottom = top >= 0 ? max(kept.start[a], top - (MOST_KEPT - 1)) : 0;
-    around(K, a, [&](int o, float4 other) {
-        if (!(o > a)) return;
-        const float d0 = me.x - other.x, d1 = me.y - other.y, d2v = me.z - other.z;
-        const float d2 = d0 * d0 + (d1 * d1 + d2v * d2v);
-        const float near = (me.w + other.w) * (1.0f + LIST_MARGIN);
-        if (!(d2 < near * near)) return;
+    auto place = [&](int o) {
         const int at = slot++;
         if (!(at < K.cap)) return;
         L.pair[at] = make_int2(a, o);
@@ -790,7 +807,21 @@ __device__ __forceinline__ void fill_near(const Kernel& K, const ListGen& L, con
         }
         L.imp[2 * (size_t)at] = w0;
         L.imp[2 * (size_t)at + 1] = w1;
-    });
+    };
+    const int found = L.start[a + 1] - first;
+    if (found <= NEAR_KEPT) {  // the partners the count kept, in the walk's order
+        const int* keep = K.near + (size_t)a * NEAR_KEPT;
+        for (int i = 0; i < found; i++) place(keep[i]);
+    } else {  // more than were kept: the walk again, the same spheres in the same order
+        around(K, a, [&](int o, float4 other) {
+            if (!(o > a)) return;
+            const float d0 = me.x - other.x, d1 = me.y - other.y, d2v = me.z - other.z;
+            const float d2 = d0 * d0 + (d1 * d1 + d2v * d2v);
+            const float near = (me.w + other.w) * (1.0f + LIST_MARGIN);
+            if (!(d2 < near * near)) return;
+            place(o);
+        });
+    }
     L.head[a] = last;
 }
 
@@ -1209,7 +1240,7 @@ struct vxr_sphere_world {
     float* shown = nullptr;
     int *keys = nullptr, *order = nullptr, *cell_count = nullptr, *cell_start = nullptr;
     int* part = nullptr;  // [blocks] the blocks' slice totals of a shared scan
-    int *claims = nullptr, *list_count = nullptr;
+    int *claims = nullptr, *list_count = nullptr, *near = nullptr;
     ListGen gen[2]{};
     Counts* counts = nullptr;
     Counts* host_counts = nullptr;  // pinned
@@ -1344,6 +1375,7 @@ Kernel kernel_of(vxr_sphere_world* w, int steps) {
     K.cell_start = w->cell_start;
     K.claims = w->claims;
     K.list_count = w->list_count;
+    K.near = w->near;
     K.part = w->part;
     K.gen[0] = w->gen[0];
     K.gen[1] = w->gen[1];
@@ -1528,6 +1560,7 @@ vxr_sphere_world* vxr_sphere_create(const vxr_sphere_config* cfg, int32_t* statu
     }
     if (w->solve != 0) {
         rc |= salloc(w, &w->list_count, n);
+        rc |= salloc(w, &w->near, (size_t)n * NEAR_KEPT);
         for (int g = 0; g < 2; g++) {
             rc |= salloc(w, &w->gen[g].start, (size_t)n + 1);
             rc |= salloc(w, &w->gen[g].pair, w->cap);
