@@ -235,3 +235,41 @@ def test_gpu_towers_match_the_oracle():
     assert g.touching_pairs() == o.touching_pairs()
     o.close()
     g.close()
+
+
+@pytest.mark.parametrize("bodies", [8000, 16000], ids=["staged", "global"])
+def test_gpu_crowded_broad_phase_keeps_the_first_32_found(bodies):
+    """Small spheres crowded into one cubic metre, dozens of partners a body: each body's slots hold the first 32
+    bodies the reference's walk finds, sorted (BoxBroad.list :103-164), and the rest are counted unlisted. 8,000
+    bodies keep every block's neighbourhood within its shared memory; 16,000 overflow it, so the tiled list reads
+    those neighbourhoods from global memory. Candidate pairs, the report and the step's state equal the oracle's."""
+    from oracle.box import OracleBoxWorld
+    from vxr.box_simulation import BoxSimulation
+    rng = np.random.Generator(np.random.PCG64(12))
+    r = 0.05
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)  # noqa: E731
+    x, y, z = (f32(rng.uniform(1.5, 2.5, bodies)) for _ in range(3))
+    zero = np.zeros(bodies, np.float32)
+    fields = {"x": x, "y": y, "z": z, "u": zero, "v": zero, "w": zero, "lx": zero, "ly": zero, "lz": zero,
+              "qx": zero, "qy": zero, "qz": zero, "qw": np.ones(bodies, np.float32),
+              "im": np.full(bodies, 1.0 / 0.5, np.float32), "hx": np.full(bodies, r, np.float32),
+              "hy": np.full(bodies, r, np.float32), "hz": np.full(bodies, r, np.float32),
+              "shape": np.full(bodies, B.SPHERE_SHAPE, np.float32)}
+    order = ["x", "y", "z", "u", "v", "w", "lx", "ly", "lz", "qx", "qy", "qz", "qw", "im", "hx", "hy", "hz", "shape"]
+    grid = B.grid(4.0, 4.0, 4.0, r, 0.005)
+    params = B.params(1 / 240, 0.0, -9.81, 0.0, 4.0, 4.0, 4.0, 0.5, 0.5, 0.005, 0.1)
+    o = OracleBoxWorld(bodies, 1, 2, False, grid, threads=True)
+    for k in order:
+        o.set_field(k, fields[k])
+    o.set_params(params)
+    g = BoxSimulation(bodies, 1, 2, False, grid)
+    g.load_state([fields[k] for k in order], params)
+    ro = o.step(1)
+    rg = g.step_and_wait(1)
+    assert ro == tuple(rg)
+    assert ro[4] > 0  # bodies with more than 32 partners
+    np.testing.assert_array_equal(g.candidate_pairs(), o.candidate_pairs())
+    for name, a in zip(order[:13], g.state()):
+        assert np.array_equal(a.view(np.int32), o.field(name).view(np.int32)), name
+    o.close()
+    g.close()

@@ -402,6 +402,169 @@ __global__ void k_list(int n, GridDims g, SceneGrids sg, float margin, const flo
     if (found > SLOTS) atomicAdd(&counters->unlisted, found - SLOTS);
 }
 
+// The broad phase's list over a tile of cells (BoxBroad.list :103-164 with around :230-252, reach one cell): a block
+// takes TILE_X consecutive cells of one x-row and stages the bodies of their 27-cell neighbourhoods (nine runs of
+// the sorted order, one for each (y, z) row: cells along x have consecutive keys) in shared memory, each with its
+// centre and its world half-extents. A warp then takes one of the tile's own bodies at a time. Its 32 lanes test 32
+// of the body's candidates at once, in the reference's visiting order (the nine rows in turn, each row's three cells
+// x-first, each cell in sorted order); a ballot marks the close ones and each found body moves to the lane of its
+// place in the found order (popc and __fns over the ballot). The first 32 found, sorted ascending across the lanes
+// (bitonic), are the body's slots: the reference's insertion into 32 ascending slots of what it finds, in its order.
+// A neighbourhood too large to stage is read from global memory by the same warps.
+constexpr int TILE_X = 16;
+constexpr int STAGE_CAP = 1280;  // staged bodies a block
+
+__device__ __forceinline__ int bitonic_ascending(int v, int lane) {
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int other = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool up = (lane & k) == 0, lower = (lane & j) == 0;
+            v = (lower == up) ? min(v, other) : max(v, other);
+        }
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(256) k_list_tiled(GridDims g, float margin, const float4* __restrict__ pose,
+                                                    const float4* __restrict__ reach, const int* __restrict__ keys,
+                                                    const int* __restrict__ cell_start, const int* __restrict__ order,
+                                                    int* __restrict__ partner, int* __restrict__ found_out,
+                                                    int* __restrict__ kept_out, Counters* counters) {
+    __shared__ float4 spose[STAGE_CAP], sreach[STAGE_CAP];  // reach .w: the body's index, as bits
+    __shared__ int row_base[10];        // staged rows' first places (the last: the total)
+    __shared__ int row_first[9];        // each row's first cell key (the staged column xs0), -1 if outside the grid
+    __shared__ int staged;              // 1 when the neighbourhood fits in shared memory
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int tiles_x = (nx + TILE_X - 1) / TILE_X;
+    const int tile = blockIdx.x;
+    const int tx = tile % tiles_x, iy = (tile / tiles_x) % ny, iz = tile / (tiles_x * ny);
+    const int x0 = tx * TILE_X, x1 = min(x0 + TILE_X, nx) - 1;  // the tile's own cells, inclusive
+    const int own_lo = cell_start[x0 + nx * (iy + ny * iz)], own_hi = cell_start[x1 + nx * (iy + ny * iz) + 1];
+    if (own_lo == own_hi) return;  // no body to list (block-uniform)
+    const int xs0 = max(x0 - 1, 0), xs1 = min(x1 + 1, nx - 1);  // the staged columns
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    if (threadIdx.x < 32) {  // the nine rows' runs: their lengths, scanned across the first lanes
+        int len = 0, first = -1;
+        if (lane < 9) {
+            const int jy = iy + (lane % 3 - 1), jz = iz + (lane / 3 - 1);
+            if (jy >= 0 && jy < ny && jz >= 0 && jz < nz) {
+                first = xs0 + nx * (jy + ny * jz);
+                len = cell_start[first + (xs1 - xs0) + 1] - cell_start[first];
+            }
+        }
+        int sum = len;
+#pragma unroll
+        for (int o = 1; o < 16; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, sum, o);
+            if (lane >= o) sum += y;
+        }
+        if (lane < 9) {
+            row_base[lane] = sum - len;
+            row_first[lane] = first;
+        }
+        if (lane == 8) {
+            row_base[9] = sum;
+            staged = sum <= STAGE_CAP ? 1 : 0;
+        }
+    }
+    __syncthreads();
+    const int use_shared = staged;
+    if (use_shared) {
+        for (int r = 0; r < 9; r++) {
+            const int first = row_first[r];
+            if (first < 0) continue;
+            const int g0 = cell_start[first], base = row_base[r], len = row_base[r + 1] - base;
+            for (int i = threadIdx.x; i < len; i += blockDim.x) {
+                const int o = order[g0 + i];
+                const float4 p = pose[o], q = reach[o];
+                spose[base + i] = p;
+                sreach[base + i] = make_float4(q.x, q.y, q.z, __int_as_float(o));
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = own_lo + warp; i < own_hi; i += warps) {
+        const int s = order[i];
+        const float4 ps = pose[s], rs = reach[s];
+        const int ix = keys[s] % nx;
+        // this body's nine runs: for row r, the cells ix-1 .. ix+1 inside the grid; lo in staged places (or global
+        // order places), and the runs' lengths scanned so every lane can map a candidate's number to its run
+        int lo = 0, len = 0;
+        if (lane < 9) {
+            const int first = row_first[lane];
+            if (first >= 0) {
+                const int c_lo = first + (max(ix - 1, 0) - xs0), c_hi = first + (min(ix + 1, nx - 1) - xs0);
+                const int a = cell_start[c_lo], b = cell_start[c_hi + 1];
+                len = b - a;
+                lo = use_shared ? row_base[lane] + (a - cell_start[first]) : a;
+            }
+        }
+        int end = len;
+#pragma unroll
+        for (int o = 1; o < 16; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, end, o);
+            if (lane >= o) end += y;
+        }
+        // every lane holds the nine runs' ends, places and lengths
+        int run_end[9], run_lo[9], run_len[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            run_end[k] = __shfl_sync(0xffffffffu, end, k);
+            run_lo[k] = __shfl_sync(0xffffffffu, lo, k);
+            run_len[k] = __shfl_sync(0xffffffffu, len, k);
+        }
+        const int total = run_end[8];
+        int found = 0, mine = 0x7fffffff;  // lane f holds the f-th body found, while f < 32
+        for (int base = 0; base < total; base += 32) {
+            const int f = base + lane;
+            bool close = false;
+            int o = 0;
+            if (f < total) {
+                int at = 0;
+                bool seen = false;
+#pragma unroll
+                for (int k = 0; k < 9; k++) {  // the run this candidate falls in: the first whose end passes f
+                    if (!seen && f < run_end[k]) {
+                        at = run_lo[k] + (f - (run_end[k] - run_len[k]));
+                        seen = true;
+                    }
+                }
+                float4 po, ro;
+                if (use_shared) {
+                    po = spose[at];
+                    ro = sreach[at];
+                    o = __float_as_int(ro.w);
+                } else {
+                    o = order[at];
+                    po = pose[o];
+                    ro = reach[o];
+                }
+                close = o > s && !(fabsf(po.x - ps.x) > (rs.x + ro.x) + margin) &&
+                        !(fabsf(po.y - ps.y) > (rs.y + ro.y) + margin) &&
+                        !(fabsf(po.z - ps.z) > (rs.z + ro.z) + margin);
+            }
+            const unsigned hits = __ballot_sync(0xffffffffu, close);
+            const int got = __popc(hits);
+            // lane d takes the (d - found)-th hit of this batch, while d < 32
+            const int want = lane - found;
+            const int src = (want >= 0 && want < got) ? (int)__fns(hits, 0, want + 1) : lane;
+            const int moved = __shfl_sync(0xffffffffu, o, src);
+            if (want >= 0 && want < got) mine = moved;
+            found += got;
+        }
+        const int kept = min(found, SLOTS);
+        const int sorted = bitonic_ascending(mine, lane);
+        if (lane < kept) partner[(long)s * SLOTS + lane] = sorted;
+        if (lane == 0) {
+            found_out[s] = found;
+            kept_out[s] = kept;
+            if (found > SLOTS) atomicAdd(&counters->unlisted, found - SLOTS);
+        }
+    }
+}
+
 __global__ void k_candidates(int n, int cap, const int* __restrict__ kept, const int* __restrict__ cand_start,
                              const int* __restrict__ partner, int* __restrict__ cand_a, int* __restrict__ cand_b,
                              Counters* counters) {
@@ -2174,8 +2337,14 @@ int enqueue_step(vxr_box_world* w) {
         k_scatter<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->keys, w->cell_start, w->cell_fill,
                                                              w->order_tmp);
         k_stable<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->keys, w->cell_start, w->order_tmp, w->order);
-        k_list<<<blocks_for(n, 128), 128, 0, st>>>(n, g, sg, margin, w->b.pose, w->reach, w->keys, w->cell_start,
-                                                  w->order, w->partner, w->found, w->kept, w->counters);
+        if (!w->body_scene && w->reach_cells == 1) {  // the tiled list: a block a run of cells, a warp a body
+            const int tiles = ((w->nx + TILE_X - 1) / TILE_X) * w->ny * w->nz;
+            k_list_tiled<<<tiles, 256, 0, st>>>(g, margin, w->b.pose, w->reach, w->keys, w->cell_start, w->order,
+                                                w->partner, w->found, w->kept, w->counters);
+        } else {  // batched scenes' grids, or a neighbourhood wider than 27 cells: a thread a body
+            k_list<<<blocks_for(n, 128), 128, 0, st>>>(n, g, sg, margin, w->b.pose, w->reach, w->keys, w->cell_start,
+                                                      w->order, w->partner, w->found, w->kept, w->counters);
+        }
         exclusive_scan(w->kept, w->cand_start, n, w->scan_tiles, st);
         k_candidates<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->cap, w->kept, w->cand_start, w->partner,
                                                                 w->cand_a, w->cand_b, w->counters);
