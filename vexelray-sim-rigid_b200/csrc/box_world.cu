@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(256) k_list_tiled(GridDims g, float margin, co
             found += got;
         }
         const int kept = min(found, SLOTS);
-        const int sorted = bitonic_ascending(mine, lane);
+        const int sorted = kept > 1 ? bitonic_ascending(mine, lane) : mine;  // kept is the same in every lane
         if (lane < kept) partner[(long)s * SLOTS + lane] = sorted;
         if (lane == 0) {
             found_out[s] = found;
