@@ -118,6 +118,39 @@ def gather(world, steps: int, rows_wanted: int, sweeps_cap: int = 64, tolerance:
     return f, t
 
 
+def gather_many(plan, rows_wanted: int, sweeps_cap: int = 64, tolerance: float = 1e-6, device: int = 0):
+    """Training rows from several worlds and phases of the drop: `plan` lists (scene, steps to settle first); each
+    entry gives an equal share of `rows_wanted`, from as many steps as that takes (the plain solver run to `tolerance`,
+    at most `sweeps_cap` sweeps a half-substep). Returns the features, the targets and each row's plan entry."""
+    share = max(1, rows_wanted // max(len(plan), 1))
+    feats, targets, source = [], [], []
+    for k, (scene, settle) in enumerate(plan):
+        w = settled_world(scene, settle, sweeps_cap, device=device)
+        f, t = gather(w, steps=64, rows_wanted=share, sweeps_cap=sweeps_cap, tolerance=tolerance)
+        w.close()
+        feats.append(f)
+        targets.append(t)
+        source.append(np.full(len(f), k, np.int32))
+    return np.concatenate(feats), np.concatenate(targets), np.concatenate(source)
+
+
+def prediction_errors(net, feats, targets) -> dict:
+    """How close each start is to the impulses the plain solver reaches (both scaled by the pair's effective mass
+    x |g| x h, as the features and targets are): the network's (its outputs, negatives clipped to zero, as the step
+    applies them) against the carried impulses (features 7 and 8) on the points that carried something, and against
+    zero on those that carried nothing. Root mean square over the rows, normal and tangential together."""
+    f = np.asarray(feats, np.float32)
+    t = np.asarray(targets, np.float32)
+    pred = np.maximum(net.forward(f), 0.0)
+    carried = (f[:, 7] != 0.0) | (f[:, 8] != 0.0)
+    rms = lambda a, b: float(np.sqrt(np.mean(np.sum((a - b) ** 2, 1)))) if len(a) else None  # noqa: E731
+    return {"rows": int(len(f)), "carried_rows": int(carried.sum()),
+            "carried": {"network": rms(pred[carried], t[carried]), "carried_impulses": rms(f[carried][:, 7:9],
+                                                                                             t[carried])},
+            "new": {"network": rms(pred[~carried], t[~carried]),
+                    "zero": rms(np.zeros_like(t[~carried]), t[~carried])}}
+
+
 def sweeps_to_residual(world, steps: int, tolerance: float, cap: int, mode: int, net=None, cold: bool = False):
     """Mean solve sweeps a substep takes to reach the residual (at most `cap`), over `steps` steps, and the share of
     substeps that reached it: the plain warm start (mode 0, or cold = from zero) or the network's (mode 2 or 3)."""
