@@ -436,6 +436,7 @@ __global__ void __launch_bounds__(256) k_list_tiled(GridDims g, float margin, co
     __shared__ int row_base[10];        // staged rows' first places (the last: the total)
     __shared__ int row_first[9];        // each row's first cell key (the staged column xs0), -1 if outside the grid
     __shared__ int staged;              // 1 when the neighbourhood fits in shared memory
+    __shared__ int col_start[9][TILE_X + 3];  // staged place where each staged column's cell begins (and the end)
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int tiles_x = (nx + TILE_X - 1) / TILE_X;
     const int tile = blockIdx.x;
@@ -482,9 +483,52 @@ __global__ void __launch_bounds__(256) k_list_tiled(GridDims g, float margin, co
                 spose[base + i] = p;
                 sreach[base + i] = make_float4(q.x, q.y, q.z, __int_as_float(o));
             }
+            for (int c = threadIdx.x; c <= xs1 - xs0 + 1; c += blockDim.x)
+                col_start[r][c] = base + (cell_start[first + c] - g0);
         }
     }
     __syncthreads();
+    // A sparse neighbourhood (few candidates a body: about 3 x the staged bodies over the staged columns) would leave
+    // most of a warp's lanes idle; then each thread lists one of the tile's bodies itself, walking the staged runs in
+    // the same order and keeping its first 32 found in ascending slots as the reference inserts them.
+    if (use_shared && 3 * row_base[9] < 24 * (xs1 - xs0 + 1)) {
+        for (int i = own_lo + threadIdx.x; i < own_hi; i += blockDim.x) {
+            const int s = order[i];
+            const float4 ps = pose[s], rs = reach[s];
+            const int cx_lo = max(keys[s] % nx - 1, 0) - xs0, cx_hi = min(keys[s] % nx + 1, nx - 1) - xs0;
+            int slot[SLOTS];
+            int found = 0;
+            for (int r = 0; r < 9; r++) {
+                if (row_first[r] < 0) continue;
+                const int end = col_start[r][cx_hi + 1];
+                for (int k = col_start[r][cx_lo]; k < end; k++) {
+                    const float4 ro = sreach[k];
+                    const int o = __float_as_int(ro.w);
+                    if (!(o > s)) continue;
+                    const float4 po = spose[k];
+                    const bool close = !(fabsf(po.x - ps.x) > (rs.x + ro.x) + margin) &&
+                                       !(fabsf(po.y - ps.y) > (rs.y + ro.y) + margin) &&
+                                       !(fabsf(po.z - ps.z) > (rs.z + ro.z) + margin);
+                    if (!close) continue;
+                    if (found < SLOTS) {
+                        int place = found;
+                        while (place > 0 && slot[place - 1] > o) {
+                            slot[place] = slot[place - 1];
+                            place--;
+                        }
+                        slot[place] = o;
+                    }
+                    found++;
+                }
+            }
+            const int kept = found < SLOTS ? found : SLOTS;
+            for (int m = 0; m < kept; m++) partner[(long)s * SLOTS + m] = slot[m];
+            found_out[s] = found;
+            kept_out[s] = kept;
+            if (found > SLOTS) atomicAdd(&counters->unlisted, found - SLOTS);
+        }
+        return;
+    }
     for (int i = own_lo + warp; i < own_hi; i += warps) {
         const int s = order[i];
         const float4 ps = pose[s], rs = reach[s];

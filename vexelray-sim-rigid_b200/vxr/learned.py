@@ -134,6 +134,13 @@ def gather_many(plan, rows_wanted: int, sweeps_cap: int = 64, tolerance: float =
     return np.concatenate(feats), np.concatenate(targets), np.concatenate(source)
 
 
+def new_contacts(feats) -> np.ndarray:
+    """The rows of points that carried nothing from the step before (features 7 and 8, the carried impulses, zero):
+    where the reference's start is zero, and where the network's start replaces it (mode 3)."""
+    f = np.asarray(feats, np.float32)
+    return (f[:, 7] == 0.0) & (f[:, 8] == 0.0)
+
+
 def prediction_errors(net, feats, targets) -> dict:
     """How close each start is to the impulses the plain solver reaches (both scaled by the pair's effective mass
     x |g| x h, as the features and targets are): the network's (its outputs, negatives clipped to zero, as the step
