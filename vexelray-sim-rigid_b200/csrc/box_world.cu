@@ -177,6 +177,7 @@ struct vxr_box_world {
     int *bucket_most = nullptr, *bucket_pstart = nullptr;  // by bucket: most points of a pair, first point
     // islands (connected components of the placed touching pairs), rebuilt every step
     int islands = 1;                  // small components solved by warps (0: every body through the grid phases)
+    int list_tiled = 0;               // the broad phase's list by tiles of cells staged in shared memory
     unsigned long long wait_limit_ns = 2000000000ull;  // the longest a device-wide wait may last
     int groups_max = 0;               // groups the bodies can fill
     int *parent = nullptr;            // [n] union-find parent
@@ -2381,7 +2382,7 @@ int enqueue_step(vxr_box_world* w) {
         k_scatter<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->keys, w->cell_start, w->cell_fill,
                                                              w->order_tmp);
         k_stable<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->keys, w->cell_start, w->order_tmp, w->order);
-        if (!w->body_scene && w->reach_cells == 1) {  // the tiled list: a block a run of cells, a warp a body
+        if (w->list_tiled && !w->body_scene && w->reach_cells == 1) {  // the tiled list: a block a run of cells
             const int tiles = ((w->nx + TILE_X - 1) / TILE_X) * w->ny * w->nz;
             k_list_tiled<<<tiles, 256, 0, st>>>(g, margin, w->b.pose, w->reach, w->keys, w->cell_start, w->order,
                                                 w->partner, w->found, w->kept, w->counters);
@@ -3477,6 +3478,13 @@ int32_t vxr_box_wait_limit(vxr_box_world* w, int64_t ns) {
     if (!w) return VXR_EINVAL;
     drop_graph(w);
     w->wait_limit_ns = ns > 0 ? (unsigned long long)ns : 2000000000ull;
+    return VXR_OK;
+}
+
+int32_t vxr_box_list_kernel(vxr_box_world* w, int32_t tiled) {
+    if (!w || tiled < 0 || tiled > 1) return VXR_EINVAL;
+    drop_graph(w);
+    w->list_tiled = tiled;
     return VXR_OK;
 }
 

@@ -22,7 +22,7 @@ SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_c
            "vxr_box_step_async", "vxr_box_sync", "vxr_box_stream", "vxr_box_state", "vxr_box_read_shown",
            "vxr_box_touching", "vxr_box_candidates", "vxr_box_walls", "vxr_box_colour_waves", "vxr_collide",
            "vxr_box_launches", "vxr_box_profile", "vxr_box_activity", "vxr_box_trace", "vxr_box_broadphase_static",
-           "vxr_box_measure", "vxr_box_wait_limit", "vxr_box_islands", "vxr_box_paths", "vxr_box_residuals", "vxr_box_create_batch", "vxr_box_scene_params",
+           "vxr_box_measure", "vxr_box_list_kernel", "vxr_box_wait_limit", "vxr_box_islands", "vxr_box_paths", "vxr_box_residuals", "vxr_box_create_batch", "vxr_box_scene_params",
            "vxr_box_scenes", "vxr_box_step_graph", "vxr_mlp_create", "vxr_mlp_destroy", "vxr_mlp_error",
            "vxr_mlp_set", "vxr_mlp_get", "vxr_mlp_forward", "vxr_mlp_gradients", "vxr_mlp_train", "vxr_box_learned",
            "vxr_box_features", "vxr_box_diagnostics", "vxr_box_contact_errors", "vxr_sphere_diagnostics", "vxr_ring_create", "vxr_ring_destroy",
@@ -160,6 +160,8 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_trace.restype = i32
         L.vxr_box_measure.argtypes = [vp, i32, i32, i32, ctypes.c_float]
         L.vxr_box_measure.restype = i32
+        L.vxr_box_list_kernel.argtypes = [vp, i32]
+        L.vxr_box_list_kernel.restype = i32
         L.vxr_box_wait_limit.argtypes = [vp, ctypes.c_int64]
         L.vxr_box_wait_limit.restype = i32
         L.vxr_box_islands.argtypes = [vp, i32]

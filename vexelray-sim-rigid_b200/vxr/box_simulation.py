@@ -281,6 +281,11 @@ class BoxSimulation:
                                            float(tolerance)))
         self.active_sweeps = sweeps or self.sweeps
 
+    def list_kernel(self, tiled: bool) -> None:
+        """The broad phase's list by tiles of cells staged in shared memory (True) or a thread a body walking its 27
+        cells (False, the default); the pairs are the same either way."""
+        self._check(self.L.vxr_box_list_kernel(self.h, int(bool(tiled))))
+
     def wait_limit(self, ns: int = 0) -> None:
         """The longest a device-wide wait of a step may last (0: the default of 2 s); past it the step stops with
         VXR_ETIMEOUT."""
