@@ -101,10 +101,11 @@ def test_gpu_gather_train_judge():
 
 def test_gpu_the_network_is_measured_against_its_baselines_on_a_held_out_world():
     """What training buys, on a held-out world: a network trained on the new contacts (points that carried nothing)
-    of two worlds of the large scene's distribution, its error on a third world's new contacts against the untrained
-    network's and against the reference's start for them, zero (root mean square of the scaled impulses). Training
-    must cut the untrained network's error at least in half; how it compares with zero is reported, not assumed:
-    measured here it is about zero's (3.33 against 3.31), the ceiling a per-contact predictor of these features meets."""
+    of two worlds of the large scene's distribution, its error on a third world's new contacts against the reference's
+    start for them, zero (root mean square of the scaled impulses). Training must lower its loss, and the network must
+    start new contacts no further from their solution than zero does (within 10%): it is used only there. Measured, it
+    is about as close as zero (3.33 against 3.31 here; 1.89 against 1.94 on the bench's 2M rows): a per-contact
+    predictor of these features sees too little of the pile to do better, the ceiling the bench's sweeps show too."""
     from vxr.learned import Mlp
     plan = [(scenes.sub_volume(262_144, 16_384 / 262_144, seed=31), 30),
             (scenes.sub_volume(262_144, 16_384 / 262_144, seed=32), 60)]
@@ -115,11 +116,9 @@ def test_gpu_the_network_is_measured_against_its_baselines_on_a_held_out_world()
     hf, ht = Lm.gather(held, steps=4, rows_wanted=20_000)
     held.close()
     net = Mlp(seed=3)
-    before = Lm.prediction_errors(net, hf, ht)
-    net.train(f[new], t[new], epochs=20, batch=1024, lr=1e-3, seed=4)
+    losses = net.train(f[new], t[new], epochs=20, batch=1024, lr=1e-3, seed=4)
+    assert losses[-1] < losses[0]
     after = Lm.prediction_errors(net, hf, ht)
     assert after["rows"] > 1000 and after["rows"] - after["carried_rows"] > 100
-    assert after["new"]["network"] < 0.5 * before["new"]["network"], (before, after)
-    assert after["new"]["zero"] == before["new"]["zero"]
-    assert after["new"]["network"] < 1.5 * after["new"]["zero"], after
+    assert after["new"]["network"] <= 1.1 * after["new"]["zero"], after
     net.close()
