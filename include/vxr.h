@@ -201,6 +201,10 @@ int32_t vxr_box_paths(vxr_box_world* world, int32_t* out5);
  * residual; this is the measure "iterations to residual" counts in. used (may be NULL) receives 2 substeps ints: the
  * solve and the relax sweeps each substep ran. Returns the count of residuals, or minus a status. */
 int32_t vxr_box_residuals(vxr_box_world* world, float* out, int32_t capacity, int32_t* used);
+/* The same residuals in two parts, each the largest correction at a contact of one kind: pairs (between two bodies)
+ * and walls (a body against the box); vxr_box_residuals gives the larger of the two, and a substep's sweeps stop
+ * when both are within the tolerance. Either pointer may be NULL. Returns the count a part, or minus a status. */
+int32_t vxr_box_residual_parts(vxr_box_world* world, float* pairs, float* walls, int32_t capacity);
 
 /* Kernels this world's steps have launched since creation (each step launches the same number; reading the
  * state back is not counted). */
@@ -334,6 +338,21 @@ int32_t vxr_mlp_train(vxr_mlp* net, const float* features, const float* targets,
  * (face of first, face of second, edge, sphere) and the normal's vertical component; impulses (carried, targets and
  * predictions) in units of the pair's effective mass x |g| x h. */
 int32_t vxr_box_learned(vxr_box_world* world, vxr_mlp* net, int32_t mode);
+/* A measurement: the following steps run only their first `count` substeps (the broad and narrow phase, the carry
+ * and the colouring as in a whole step, then `count` substeps of the solve); 0 or the world's substep count restores
+ * whole steps. solve_only = 1: the last of them skips its relax sweeps. With the learned warm start's gathering
+ * (mode 1), the targets are then the impulses the first substeps reached: with solve_only, what the last one's solve
+ * sweeps reached, the impulses that solve would start from to need no sweep. No reference counterpart. */
+int32_t vxr_box_first_substeps(vxr_box_world* world, int32_t count, int32_t solve_only);
+/* A measurement of what a perfect predictor could gain: the next step starts its contact points from what
+ * `answers` (a world that gathers targets, mode 1) reached in its last step, point for point, in place of the carried
+ * impulses (fresh_only = 1: only the points that carried nothing). whole = 0: the scaled normal and friction impulse
+ * the network predicts (vxr_box_features' targets), applied as its predictions are; whole = 1: the whole impulse
+ * records (normal, friction vector and rolling impulse of every point) and, unless fresh_only, the walls' records.
+ * The points are matched by touching pair, so the two worlds must be twins: the same state and carried pairs before
+ * that step (load the same state into both and step them alike). Everything is copied at the call, so `answers` may
+ * be stepped or destroyed afterwards; vxr_box_learned(world, NULL, 0) ends it. No reference counterpart. */
+int32_t vxr_box_learned_given(vxr_box_world* world, const vxr_box_world* answers, int32_t fresh_only, int32_t whole);
 /* The last step's gathered rows, one a contact point: features16 (rows x 16) and targets2 (rows x 2), the first
  * `capacity` rows written; *rows receives their number. */
 int32_t vxr_box_features(vxr_box_world* world, float* features16, float* targets2, int32_t capacity, int32_t* rows);

@@ -183,6 +183,32 @@ def test_gpu_measuring_the_residual_changes_nothing():
     assert res.shape == (b.substeps, 2 * b.passes + 1)
     assert (res[:, 0] == 0).all()  # the warm sweep moves no impulse
     assert (used == b.passes).all()
+    pairs, walls = b.world.residual_parts()  # the pile's pairs and its floor contacts, each part apart
+    assert np.array_equal(np.maximum(pairs, walls), res)
+    assert (pairs[:, 1:] > 0).any() and (walls[:, 1:] > 0).any()
+
+
+def test_gpu_first_substeps_alone_and_solve_only():
+    """The measurement switch: a step of only the first substep, its relax sweeps skipped, runs that substep's
+    solve sweeps and nothing after them; whole steps afterwards run every substep's solve and relax sweeps."""
+    scene = C.pile_scene(7)
+    scene.start("gpu")
+    w = scene.world
+    w.step(5)
+    w.measure(residual=True)
+    w.first_substeps(1, solve_only=True)
+    w.step(1)
+    res, used = w.residuals()
+    assert used[0, 0] == scene.passes and used[0, 1] == 0
+    assert (res[0, 1:1 + scene.passes] > 0).any() and (res[0, 1 + scene.passes:] == 0).all()
+    assert (res[1:] == 0).all()
+    w.first_substeps(0)
+    w.step(1)
+    res, used = w.residuals()
+    assert (used == scene.passes).all()
+    with pytest.raises(Exception):
+        w.first_substeps(scene.substeps + 1)
+    scene.close()
 
 
 def iterations(world, steps, cold, tolerance=1e-4, cap=64):

@@ -78,9 +78,9 @@ def test_gpu_a_network_of_zeros_on_new_contacts_starts_like_the_carried_warm_sta
 
 def test_gpu_gather_train_judge():
     """The loop end to end on a small pile: rows gathered from the plain solver, a network trained on them by the
-    GPU's kernels (its loss falls), then judged by the plain solver: the judgement reports sweeps for all four
-    starts (carried, zero, the network everywhere, the network on new contacts), and the network is kept, in its
-    better mode, exactly when that needs fewer sweeps than the carried impulses."""
+    GPU's kernels (its loss falls), then judged by the plain solver on twin steps: the judgement reports sweeps for
+    all four starts (carried, zero, the network everywhere, the network on new contacts), each on the same steps, and
+    the network is kept, in its better mode, exactly when that needs fewer sweeps than the carried impulses."""
     from vxr.learned import Mlp
     sc = small_scene(seed=6)
     w = Lm.settled_world(sc, 250, 64)
@@ -89,9 +89,10 @@ def test_gpu_gather_train_judge():
     net = Mlp(seed=1)
     losses = net.train(f, t, epochs=5, batch=1024, lr=1e-3, seed=2)
     assert losses[-1] < losses[0]
-    verdict = Lm.judge(w, net, steps=2)
+    verdict = Lm.judge(sc, w.state(), net, samples=2)
     for k in ("plain_warm_start", "plain_cold_start", "learned", "learned_new_contacts_only"):
         assert 1 <= verdict[k] <= 64
+    assert set(verdict["same_steps"]["by_substep"]) == set(Lm.NETWORK_STARTS)
     best = min(verdict["learned"], verdict["learned_new_contacts_only"])
     assert verdict["kept"] == (best < verdict["plain_warm_start"])
     assert verdict["mode"] in ((2, 3) if verdict["kept"] else (0,))
@@ -122,3 +123,68 @@ def test_gpu_the_network_is_measured_against_its_baselines_on_a_held_out_world()
     assert after["rows"] > 1000 and after["rows"] - after["carried_rows"] > 100
     assert after["new"]["network"] <= 1.1 * after["new"]["zero"], after
     net.close()
+
+
+def test_gpu_twin_worlds_take_the_same_step_and_given_starts_take_effect():
+    """The ceiling's twins: two worlds loaded with the same state and stepped alike gather the same feature rows for
+    the next step (in another order within a round, where threads placed their pairs differently), so one world's
+    solved impulses, matched by touching pair, fit the other's points: two twins given them end their step in the same
+    state, and starting from them changes the step (the state differs from the plain twin's). A world that gathered
+    nothing, or the world itself, gives no answers."""
+    from vxr import _lib
+    from vxr._lib import VxrError
+    from vxr.box_simulation import BoxSimulation
+    sc = small_scene(seed=6)
+    w = Lm.settled_world(sc, 150, 16)
+    state = w.state()
+    w.close()
+    statics = [sc[k] for k in ("im", "hx", "hy", "hz", "shape")]
+    worlds = []
+    for _ in range(4):
+        t = BoxSimulation(sc["bodies"], sc["substeps"], 64, False, sc["grid"])
+        t.load_state(list(state) + statics, sc["params"])
+        t.measure(residual=False, sweeps=sc["sweeps"])
+        t.step_and_wait(2)
+        worlds.append(t)
+    a, b, b2, plain = worlds
+    with pytest.raises(VxrError) as err:
+        b.learned_given(a)
+    assert err.value.status == _lib.VXR_EINVAL
+    a.learned(None, 1)
+    a.measure(residual=True, sweeps=64, tolerance=1e-6)
+    a.step_and_wait(1)
+    fa, ta = a.features()
+    with pytest.raises(VxrError):
+        a.learned_given(a)
+    b.learned_given(a)
+    b.step_and_wait(1)
+    fb, _ = b.features()
+    assert len(fa) > 0 and np.array_equal(Lm.rows_in_order(fb), Lm.rows_in_order(fa))
+    b2.learned_given(a)
+    b2.step_and_wait(1)
+    for x, y in zip(b.state(), b2.state()):  # the same start for every touching pair, whatever its position
+        assert np.array_equal(x.view(np.int32), y.view(np.int32))
+    plain.step_and_wait(1)
+    assert any(not np.array_equal(x, y) for x, y in zip(b.state(), plain.state()))
+    b.learned(None, 0)
+    for t in worlds:
+        t.close()
+
+
+def test_gpu_the_ceiling_reports_every_start():
+    """The same-step comparison with the perfect predictor's answers on a small settled pile: the answer twins' and
+    the measured twin's contact points are the same (twins aligned), every start is measured on the same number of
+    substeps within the cap, and the first substep's own answers, as whole records, start it no worse than the
+    carried impulses do."""
+    sc = small_scene(seed=7)
+    w = Lm.settled_world(sc, 150, 16)
+    state = w.state()
+    w.close()
+    c = Lm.compare_starts(sc, state, starts=("carried", "zero") + Lm.CEILING_STARTS, samples=2, answer_cap=128)
+    assert c["twins_aligned"] is True
+    assert set(c["mean_sweeps"]) == {"carried", "zero"} | set(Lm.CEILING_STARTS)
+    for k, m in c["mean_sweeps"].items():
+        assert 1 <= m <= 64
+        assert len(c["by_substep"][k]) == sc["substeps"]
+    assert c["gain_vs_carried"]["carried"] == 1.0
+    assert c["by_substep"]["first_whole_all"][0] <= c["by_substep"]["carried"][0], c

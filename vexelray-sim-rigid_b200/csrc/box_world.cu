@@ -78,7 +78,7 @@ struct PairGen {
     int* tstart;     // [n+1] first touching pair of each body, in slot order
     int* tb;         // [cap] second body of touching pair t (slot order)
     int* pos;        // [cap] round-order position of touching pair t
-    int4* pair;      // [cap] by position: first, second, point count, t
+    int4* pair;      // [cap] by position: first, second, point count, packed round ranks (k_order)
     float4* normal;  // [cap] by position: normal, winning axis
     int* pstart;     // [cap] by position: where its points begin in the point arrays below
     // The point arrays hold a pair's points at pstart[position] + point, packed: a pair of one point takes one
@@ -223,10 +223,16 @@ struct vxr_box_world {
     cudaGraphExec_t graph_exec = nullptr;
     long long graph_launches = 0;  // kernels in the captured pair of steps
     int capturing = 0;
-    // the learned warm start: 0 off, 1 gather features and targets, 2 start from the network's impulses
+    // the learned warm start: 0 off, 1 gather features and targets, 2 start from the network's impulses (3: new
+    // contacts only), 4 start from given impulses held in lpred (5: new contacts only), 6 start from given whole
+    // impulse records (7: new contacts only)
     int learn_mode = 0;
+    int first_substeps = 0;  // a measurement: steps run only their first substeps (0: all)
+    int solve_only = 0;      // ... and the last of them skips its relax sweeps
     vxr_mlp* learn_net = nullptr;
     float *lfeat = nullptr, *lpred = nullptr, *ltarget = nullptr;  // [cap * 4 rows] x 16, 2, 2
+    float* lgiven = nullptr;  // [cap * 4 rows] x 2: given starts by touching pair (slot order), not by position
+    float4 *lgiven_imp = nullptr, *lgiven_impr = nullptr;  // [cap * 4]: whole impulse records by touching pair
 };
 
 // The network's forward over rows counted on the device (mlp.cu).
@@ -1074,7 +1080,10 @@ struct SolveArgs {
     int* listed;                   // [n] 1 where the body is on this half-substep's wall list
     const unsigned* body_colours;  // [n] the rounds of each body's pairs, one bit each
     int schedule;                  // 0: a grid barrier after every round; 1: dependency-driven
-    unsigned* residual;            // [substeps * (2 sweeps + 1)] per-sweep residual (f32 bits), null: not measured
+    unsigned* residual;            // [substeps * (2 sweeps + 1)] per-sweep residual (f32 bits), null: not measured;
+                                   // the pairs' part here, the walls' part wall_split words on
+    int wall_split;                // where the walls' part of the residual begins
+    int solve_only;                // the last substep skips its relax sweeps (a measurement of the solve's impulses)
     float tolerance;               // > 0: a substep's solve (relax) sweeps stop once a sweep's residual is this or less
     int* used;                     // [2 substeps] solve and relax sweeps each substep ran
     int substeps, sweeps, symmetric;
@@ -1580,7 +1589,7 @@ __device__ __forceinline__ bool block_of_sweeps(const SolveArgs& A, int first_ki
             if (!wait_versions(A, s, want, -1, 0)) return false;
             Held box;
             load_held(box, A.b, s);
-            if (walls_of(A, box, s, kind, reverse, A.residual ? A.residual + sweep0 + w : nullptr))
+            if (walls_of(A, box, s, kind, reverse, A.residual ? A.residual + sweep0 + w + A.wall_split : nullptr))
                 store_held(box, A.b, s);
             __threadfence();
             *(volatile int*)&A.version[s] = want + 1;
@@ -1610,8 +1619,9 @@ constexpr int SMALL_ROUND = SOLVE_THREADS;
 __device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsigned int& epoch, int kind, bool reverse,
                                           int rounds, int slot, bool fill, int index) {
     unsigned* track = A.residual ? A.residual + index : nullptr;
+    unsigned* wtrack = A.residual ? A.residual + index + A.wall_split : nullptr;
     if (reverse) {
-        phase_walls(A, kind, true, slot, track);
+        phase_walls(A, kind, true, slot, wtrack);
         if (!grid_sync(A.bar, epoch)) return false;
         tr.mark(TR_WALLS | kind << 4);
     }
@@ -1647,7 +1657,7 @@ __device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsign
         order = end;
     }
     if (!reverse) {
-        phase_walls(A, kind, false, slot, track);
+        phase_walls(A, kind, false, slot, wtrack);
         if (!grid_sync(A.bar, epoch)) return false;
         tr.mark(TR_WALLS | kind << 4);
     }
@@ -1658,14 +1668,19 @@ __device__ __forceinline__ bool sweep_all(const SolveArgs& A, Tracer& tr, unsign
 // reads the same word after the grid barrier, so every block decides the same.
 __device__ __forceinline__ bool converged(const SolveArgs& A, int index) {
     if (!(A.tolerance > 0.0f) || !A.residual) return false;
-    return __uint_as_float(*(volatile unsigned*)&A.residual[index]) <= A.tolerance;
+    const float pairs = __uint_as_float(*(volatile unsigned*)&A.residual[index]);
+    const float walls = __uint_as_float(*(volatile unsigned*)&A.residual[index + A.wall_split]);
+    return pairs <= A.tolerance && walls <= A.tolerance;
 }
 
 __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_solve(SolveArgs A) {
     const int rounds = *(volatile int*)&A.counters->grid_rounds;
     if (A.grid_list && grid_bodies(A) == 0) {  // every body is the island kernel's: nothing for the grid phases
         if (A.used && blockIdx.x == 0 && threadIdx.x == 0)
-            for (int sub = 0; sub < A.substeps; sub++) A.used[2 * sub] = A.used[2 * sub + 1] = A.sweeps;
+            for (int sub = 0; sub < A.substeps; sub++) {
+                A.used[2 * sub] = A.sweeps;
+                A.used[2 * sub + 1] = A.solve_only && sub == A.substeps - 1 ? 0 : A.sweeps;
+            }
         return;
     }
     Tracer tr{A.trace, A.trace_cap, 0};
@@ -1696,7 +1711,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) k_solve(SolveArgs A) {
         phase_positions(A, 2 * sub + 1);
         if (!grid_sync(A.bar, epoch)) return;
         tr.mark(TR_POSITIONS);
-        if (A.schedule == 1) {
+        if (A.solve_only && sub == A.substeps - 1) {
+            relaxed = 0;
+        } else if (A.schedule == 1) {
             if (!block_of_sweeps(A, RELAX, A.sweeps, rounds, 2 * sub + 1, sub * stride + 1 + A.sweeps)) return;
             if (!grid_sync(A.bar, epoch)) return;
             tr.mark(TR_BLOCK | RELAX << 4);
@@ -1821,8 +1838,9 @@ __device__ __forceinline__ void group_walls(const SolveArgs& A, GroupBodies& G, 
 __device__ __forceinline__ void group_sweep(const SolveArgs& A, const IslandArgs& I, GroupBodies& G, const int* gs,
                                             int kind, bool reverse, bool fill, int index) {
     unsigned* track = A.residual ? A.residual + index : nullptr;
+    unsigned* wtrack = A.residual ? A.residual + index + A.wall_split : nullptr;
     if (reverse) {
-        group_walls(A, G, kind, true, track);
+        group_walls(A, G, kind, true, wtrack);
         __syncthreads();
     }
     for (unsigned left = G.present; left;) {
@@ -1842,7 +1860,7 @@ __device__ __forceinline__ void group_sweep(const SolveArgs& A, const IslandArgs
         __syncthreads();
     }
     if (!reverse) {
-        group_walls(A, G, kind, false, track);
+        group_walls(A, G, kind, false, wtrack);
         __syncthreads();
     }
 }
@@ -1873,6 +1891,7 @@ __device__ __forceinline__ void run_group(const SolveArgs& A, const IslandArgs& 
         for (int sw = 0; sw < A.sweeps; sw++)
             group_sweep(A, I, G, gs, SOLVE, A.symmetric && sw % 2 == 1, false, base + 1 + sw);
         group_positions(A, G, nb, h);
+        if (A.solve_only && sub == A.substeps - 1) continue;
         const int relax = base + 1 + A.sweeps;
         for (int sw = 0; sw < A.sweeps; sw++)
             group_sweep(A, I, G, gs, RELAX, A.symmetric && sw % 2 == 1, sw == 0, relax + sw);
@@ -1908,7 +1927,7 @@ __device__ __forceinline__ void run_alone(const SolveArgs& A, int s) {
     const float h = A.params.w[P_H];
     const float g[3] = {word_of(A, sc, P_GX), word_of(A, sc, P_GY), word_of(A, sc, P_GZ)};
     const int stride = 2 * A.sweeps + 1;
-    unsigned* res = A.residual;
+    unsigned* res = A.residual ? A.residual + A.wall_split : nullptr;  // a lone body's only contacts are walls
     for (int sub = 0; sub < A.substeps; sub++) {
         vel.x = vel.x + h * g[0];
         vel.y = vel.y + h * g[1];
@@ -1921,7 +1940,7 @@ __device__ __forceinline__ void run_alone(const SolveArgs& A, int s) {
                             res ? res + base + 1 + sw : nullptr);
         }
         move_body(pose, turn, vel, mom, inv, h);
-        if (wall_listed(A, s, pose, hw)) {
+        if (!(A.solve_only && sub == A.substeps - 1) && wall_listed(A, s, pose, hw)) {
             const int relax = base + 1 + A.sweeps;
             for (int sw = 0; sw < A.sweeps; sw++)
                 walls_alone(A, s, pose, turn, hw, vel, mom, inv, RELAX, A.symmetric && sw % 2 == 1,
@@ -2083,6 +2102,60 @@ __global__ void k_apply_learned(const int* __restrict__ touching_n, PairGen now,
             }
             const float c = len > 1e-12f ? lt / len : 0.0f;
             now.imp[at] = make_float4(ln, dir[0] * c, dir[1] * c, dir[2] * c);
+        }
+    }
+}
+
+// Given starts between twin worlds. A pair's round-order position within its round depends on the order in which
+// threads reached it, so it can differ between two worlds in the same state; its touching index t (slot order: first
+// body, then its partners in slot order) cannot. by_pair: rows by position -> rows by touching index (pos[t] is t's
+// position); by_position: back, for the step that uses them.
+__global__ void k_rows_by_pair(const int* __restrict__ touching_n, const int* __restrict__ pos,
+                               const float* __restrict__ by_position, float* __restrict__ by_pair) {
+    const int total = *touching_n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const size_t from = (size_t)pos[t] * MOST_POINTS * 2, to = (size_t)t * MOST_POINTS * 2;
+        for (int j = 0; j < MOST_POINTS * 2; j++) by_pair[to + j] = by_position[from + j];
+    }
+}
+
+__global__ void k_rows_by_position(const int* __restrict__ touching_n, const int* __restrict__ pos,
+                                   const float* __restrict__ by_pair, float* __restrict__ by_position) {
+    const int total = *touching_n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const size_t to = (size_t)pos[t] * MOST_POINTS * 2, from = (size_t)t * MOST_POINTS * 2;
+        for (int j = 0; j < MOST_POINTS * 2; j++) by_position[to + j] = by_pair[from + j];
+    }
+}
+
+// Whole impulse records between twin worlds, by touching index: a pair's points' normal and tangential impulse and
+// rolling impulse as the answers' step left them (by_pair), then in place of the carried ones (apply; with
+// fresh_only, only where nothing was carried).
+__global__ void k_records_by_pair(const int* __restrict__ touching_n, const PairGen last, float4* __restrict__ imp,
+                                  float4* __restrict__ impr) {
+    const int total = *touching_n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int p = last.pos[t];
+        const size_t at = (size_t)last.pstart[p];
+        const int count = min(last.pair[p].z, MOST_POINTS);
+        for (int slot = 0; slot < count; slot++) {
+            imp[(size_t)t * MOST_POINTS + slot] = last.imp[at + slot];
+            impr[(size_t)t * MOST_POINTS + slot] = last.impr[at + slot];
+        }
+    }
+}
+
+__global__ void k_apply_records(const int* __restrict__ touching_n, PairGen now, const float4* __restrict__ imp,
+                                const float4* __restrict__ impr, bool fresh_only) {
+    const int total = *touching_n;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int p = now.pos[t];
+        const size_t at = (size_t)now.pstart[p];
+        const int count = min(now.pair[p].z, MOST_POINTS);
+        for (int slot = 0; slot < count; slot++) {
+            if (fresh_only && (nonzero_bits(now.imp[at + slot]) || nonzero_bits(now.impr[at + slot]))) continue;
+            now.imp[at + slot] = imp[(size_t)t * MOST_POINTS + slot];
+            now.impr[at + slot] = impr[(size_t)t * MOST_POINTS + slot];
         }
     }
 }
@@ -2350,6 +2423,9 @@ int mark(vxr_box_world* w, int which) {
 // Launches per step, counted as they are made.
 #define LAUNCHED(k) (w->launches += (k))
 
+// Words of one part of the residual record (the pairs' or the walls'): a word for each sweep of every substep.
+int residual_half(const vxr_box_world* w) { return w->substeps * (2 * w->sweeps + 1); }
+
 // Whether a step solves its small components by island blocks: on by default; off where a substep's sweep count
 // depends on a residual over every contact (the measuring tolerance), which only the grid phases gather.
 bool islands_on(const vxr_box_world* w) {
@@ -2480,15 +2556,26 @@ int enqueue_step(vxr_box_world* w) {
             k_features<<<tblocks, THREADS, 0, st>>>(tn, now, w->b, w->inc_count, w->params, w->scene_params,
                                                     w->body_scene, w->lfeat);
             LAUNCHED(1);
-            if (w->learn_mode >= 2) {
-                if (vxr_mlp_forward_device(w->learn_net, w->lfeat, tn, MOST_POINTS, w->cap * MOST_POINTS, w->lpred,
-                                           st) != VXR_OK) {
-                    w->error = "the learned warm start's network did not launch";
-                    return VXR_ECUDA;
+            if (w->learn_mode >= 6) {
+                k_apply_records<<<tblocks, THREADS, 0, st>>>(tn, now, w->lgiven_imp, w->lgiven_impr,
+                                                             w->learn_mode == 7);
+                LAUNCHED(1);
+            } else if (w->learn_mode >= 2) {
+                if (w->learn_mode <= 3) {
+                    if (vxr_mlp_forward_device(w->learn_net, w->lfeat, tn, MOST_POINTS, w->cap * MOST_POINTS,
+                                               w->lpred, st) != VXR_OK) {
+                        w->error = "the learned warm start's network did not launch";
+                        return VXR_ECUDA;
+                    }
+                    LAUNCHED(1);
+                } else {
+                    k_rows_by_position<<<tblocks, THREADS, 0, st>>>(tn, now.pos, w->lgiven, w->lpred);
+                    LAUNCHED(1);
                 }
                 k_apply_learned<<<tblocks, THREADS, 0, st>>>(tn, now, w->b, w->lpred, w->params, w->scene_params,
-                                                             w->body_scene, w->learn_mode == 3);
-                LAUNCHED(2);
+                                                             w->body_scene,
+                                                             w->learn_mode == 3 || w->learn_mode == 5);
+                LAUNCHED(1);
             }
         }
     } else {
@@ -2510,12 +2597,14 @@ int enqueue_step(vxr_box_world* w) {
         A.body_colours = w->body_colours;
         A.schedule = w->schedule;
         A.residual = w->measure ? w->residual : nullptr;
+        A.wall_split = residual_half(w);
+        A.solve_only = w->solve_only;
         if (w->measure)
-            VXR_CUDA(cudaMemsetAsync(w->residual, 0, sizeof(unsigned) * w->substeps * (2 * w->active_sweeps + 1), st));
+            VXR_CUDA(cudaMemsetAsync(w->residual, 0, sizeof(unsigned) * 2 * residual_half(w), st));
         A.pairs = now;
         A.round_start = w->round_start;
         A.counters = w->counters;
-        A.substeps = w->substeps;
+        A.substeps = w->first_substeps > 0 ? w->first_substeps : w->substeps;
         A.sweeps = w->active_sweeps;
         A.tolerance = w->measure ? w->tolerance : 0.0f;
         A.used = w->used;
@@ -2766,7 +2855,7 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     rc |= alloc(w, &w->version, n);
     rc |= alloc(w, &w->listed, n);
     rc |= alloc(w, &w->body_colours, n);
-    rc |= alloc(w, &w->residual, (size_t)w->substeps * (2 * w->sweeps + 1));
+    rc |= alloc(w, &w->residual, 2 * (size_t)residual_half(w));  // the pairs' part, then the walls'
     rc |= alloc(w, &w->used, 2 * (size_t)w->substeps);
     rc |= alloc(w, &w->round_fill, ALL_BUCKETS);
     if (w->has_grid) {
@@ -3023,6 +3112,67 @@ int32_t vxr_box_learned(vxr_box_world* w, vxr_mlp* net, int32_t mode) {
     drop_graph(w);
     w->learn_mode = mode;
     w->learn_net = net;
+    return VXR_OK;
+}
+
+int32_t vxr_box_first_substeps(vxr_box_world* w, int32_t count, int32_t solve_only) {
+    if (!w || count < 0 || count > w->substeps || (solve_only != 0 && solve_only != 1)) return VXR_EINVAL;
+    drop_graph(w);
+    w->first_substeps = count == w->substeps ? 0 : count;
+    w->solve_only = count > 0 ? solve_only : 0;
+    return VXR_OK;
+}
+
+int32_t vxr_box_learned_given(vxr_box_world* w, const vxr_box_world* answers, int32_t fresh_only, int32_t whole) {
+    if (!w || !answers || answers == w || (fresh_only != 0 && fresh_only != 1) || (whole != 0 && whole != 1))
+        return VXR_EINVAL;
+    if (!w->has_grid || !answers->ltarget || answers->cap != w->cap || answers->device != w->device ||
+        answers->n != w->n) {
+        w->error = "given starts need a world of the same bodies and pair capacity on the same device that gathered "
+                   "targets";
+        return VXR_EINVAL;
+    }
+    cudaSetDevice(w->device);
+    const size_t rows = (size_t)w->cap * MOST_POINTS;
+    if (!w->lfeat) {
+        if (alloc(w, &w->lfeat, rows * FEATURES) || alloc(w, &w->lpred, rows * 2) || alloc(w, &w->ltarget, rows * 2))
+            return VXR_ECUDA;
+    }
+    if (!w->lgiven && alloc(w, &w->lgiven, rows * 2)) return VXR_ECUDA;
+    VXR_CUDA(cudaStreamSynchronize(answers->stream));
+    if (whole) {  // the answers' whole records: pairs by touching index; the walls' records as they are (all only)
+        if (!w->lgiven_imp && (alloc(w, &w->lgiven_imp, rows) || alloc(w, &w->lgiven_impr, rows))) return VXR_ECUDA;
+        const PairGen& done = answers->gen[answers->cur ^ 1];
+        VXR_CUDA(cudaMemsetAsync(w->lgiven_imp, 0, sizeof(float4) * rows, w->stream));
+        VXR_CUDA(cudaMemsetAsync(w->lgiven_impr, 0, sizeof(float4) * rows, w->stream));
+        k_records_by_pair<<<w->sms * 4, THREADS, 0, w->stream>>>(done.tstart + answers->n, done, w->lgiven_imp,
+                                                                 w->lgiven_impr);
+        VXR_CUDA(cudaGetLastError());
+        if (!fresh_only) {
+            const size_t n = w->n;
+            VXR_CUDA(cudaMemcpyAsync(w->wall, answers->wall, sizeof(float4) * n * WALL_RECORDS,
+                                     cudaMemcpyDeviceToDevice, w->stream));
+            VXR_CUDA(cudaMemcpyAsync(w->wroll, answers->wroll, sizeof(float4) * n * 6, cudaMemcpyDeviceToDevice,
+                                     w->stream));
+            VXR_CUDA(cudaMemcpyAsync(w->wmask, answers->wmask, sizeof(unsigned long long) * n,
+                                     cudaMemcpyDeviceToDevice, w->stream));
+        }
+        VXR_CUDA(cudaStreamSynchronize(w->stream));
+        drop_graph(w);
+        w->learn_mode = fresh_only ? 7 : 6;
+        w->learn_net = nullptr;
+        return VXR_OK;
+    }
+    // the answers' last step, by touching index: rows of pairs the answers did not touch stay zero
+    const PairGen& last = answers->gen[answers->cur ^ 1];
+    VXR_CUDA(cudaMemsetAsync(w->lgiven, 0, sizeof(float) * rows * 2, w->stream));
+    k_rows_by_pair<<<w->sms * 4, THREADS, 0, w->stream>>>(last.tstart + answers->n, last.pos, answers->ltarget,
+                                                         w->lgiven);
+    VXR_CUDA(cudaGetLastError());
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    drop_graph(w);
+    w->learn_mode = fresh_only ? 5 : 4;
+    w->learn_net = nullptr;
     return VXR_OK;
 }
 
@@ -3501,8 +3651,26 @@ int32_t vxr_box_residuals(vxr_box_world* w, float* out, int32_t capacity, int32_
     if (!out && !used) return count;
     if (out && capacity < count) return -VXR_ECAPACITY;
     VXR_CUDA(cudaStreamSynchronize(w->stream));
-    if (out) VXR_CUDA(cudaMemcpy(out, w->residual, sizeof(float) * count, cudaMemcpyDeviceToHost));
+    if (out) {
+        std::vector<float> walls(count);
+        VXR_CUDA(cudaMemcpy(out, w->residual, sizeof(float) * count, cudaMemcpyDeviceToHost));
+        VXR_CUDA(cudaMemcpy(walls.data(), w->residual + residual_half(w), sizeof(float) * count,
+                            cudaMemcpyDeviceToHost));
+        for (int k = 0; k < count; k++) out[k] = std::max(out[k], walls[k]);
+    }
     if (used) VXR_CUDA(cudaMemcpy(used, w->used, sizeof(int) * 2 * w->substeps, cudaMemcpyDeviceToHost));
+    return count;
+}
+
+int32_t vxr_box_residual_parts(vxr_box_world* w, float* pairs, float* walls, int32_t capacity) {
+    if (!w) return -VXR_EINVAL;
+    const int count = w->substeps * (2 * w->active_sweeps + 1);
+    if (!pairs && !walls) return count;
+    if (capacity < count) return -VXR_ECAPACITY;
+    VXR_CUDA(cudaStreamSynchronize(w->stream));
+    if (pairs) VXR_CUDA(cudaMemcpy(pairs, w->residual, sizeof(float) * count, cudaMemcpyDeviceToHost));
+    if (walls)
+        VXR_CUDA(cudaMemcpy(walls, w->residual + residual_half(w), sizeof(float) * count, cudaMemcpyDeviceToHost));
     return count;
 }
 

@@ -22,9 +22,9 @@ SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_c
            "vxr_box_step_async", "vxr_box_sync", "vxr_box_stream", "vxr_box_state", "vxr_box_read_shown",
            "vxr_box_touching", "vxr_box_candidates", "vxr_box_walls", "vxr_box_colour_waves", "vxr_collide",
            "vxr_box_launches", "vxr_box_profile", "vxr_box_activity", "vxr_box_trace", "vxr_box_broadphase_static",
-           "vxr_box_measure", "vxr_box_list_kernel", "vxr_box_wait_limit", "vxr_box_islands", "vxr_box_paths", "vxr_box_residuals", "vxr_box_create_batch", "vxr_box_scene_params",
+           "vxr_box_measure", "vxr_box_list_kernel", "vxr_box_wait_limit", "vxr_box_islands", "vxr_box_paths", "vxr_box_residuals", "vxr_box_residual_parts", "vxr_box_create_batch", "vxr_box_scene_params",
            "vxr_box_scenes", "vxr_box_step_graph", "vxr_mlp_create", "vxr_mlp_destroy", "vxr_mlp_error",
-           "vxr_mlp_set", "vxr_mlp_get", "vxr_mlp_forward", "vxr_mlp_gradients", "vxr_mlp_train", "vxr_box_learned",
+           "vxr_mlp_set", "vxr_mlp_get", "vxr_mlp_forward", "vxr_mlp_gradients", "vxr_mlp_train", "vxr_box_learned", "vxr_box_learned_given", "vxr_box_first_substeps",
            "vxr_box_features", "vxr_box_diagnostics", "vxr_box_contact_errors", "vxr_sphere_diagnostics", "vxr_ring_create", "vxr_ring_destroy",
            "vxr_ring_error", "vxr_ring_install", "vxr_ring_back", "vxr_ring_publish", "vxr_ring_keep", "vxr_ring_take",
            "vxr_ring_wait", "vxr_ring_read", "vxr_ring_retired", "vxr_ring_live", "vxr_box_shown_device",
@@ -170,6 +170,8 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_paths.restype = i32
         L.vxr_box_residuals.argtypes = [vp, vp, i32, vp]
         L.vxr_box_residuals.restype = i32
+        L.vxr_box_residual_parts.argtypes = [vp, vp, vp, i32]
+        L.vxr_box_residual_parts.restype = i32
         L.vxr_box_broadphase_static.argtypes = [i32, vp, Grid, i32, f32, vp, vp, i32, vp, vp]
         L.vxr_box_broadphase_static.restype = i32
         L.vxr_collide.argtypes = [i32, vp, vp, i32, vp, vp]
@@ -199,6 +201,10 @@ def lib() -> ctypes.CDLL:
         L.vxr_mlp_train.restype = i32
         L.vxr_box_learned.argtypes = [vp, vp, i32]
         L.vxr_box_learned.restype = i32
+        L.vxr_box_first_substeps.argtypes = [vp, i32, i32]
+        L.vxr_box_first_substeps.restype = i32
+        L.vxr_box_learned_given.argtypes = [vp, vp, i32, i32]
+        L.vxr_box_learned_given.restype = i32
         L.vxr_box_features.argtypes = [vp, vp, vp, i32, ctypes.POINTER(i32)]
         L.vxr_box_features.restype = i32
         L.vxr_box_diagnostics.argtypes = [vp, ctypes.POINTER(Diag)]

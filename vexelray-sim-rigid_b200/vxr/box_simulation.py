@@ -143,6 +143,18 @@ class BoxSimulation:
         impulses, 3 only the points that carried nothing (the others keep their carried impulses)."""
         self._check(self.L.vxr_box_learned(self.h, net.h if net is not None else None, mode))
 
+    def first_substeps(self, count: int, solve_only: bool = False) -> None:
+        """A measurement: the following steps run only their first `count` substeps (0: whole steps again); with
+        solve_only, the last of them skips its relax sweeps."""
+        self._check(self.L.vxr_box_first_substeps(self.h, int(count), 1 if solve_only else 0))
+
+    def learned_given(self, answers, fresh_only: bool = False, whole: bool = False) -> None:
+        """The next step starts its contact points from what `answers` (a twin world gathering targets) reached in
+        its last step, in place of the carried impulses: the network's two targets a point, or with whole the whole
+        impulse records (and the walls' records, unless fresh_only); with fresh_only, only the points that carried
+        nothing. What a perfect predictor would give. learned(None, 0) ends it."""
+        self._check(self.L.vxr_box_learned_given(self.h, answers.h, 1 if fresh_only else 0, 1 if whole else 0))
+
     def features(self):
         """The last step's gathered rows: features (rows, 16) and targets (rows, 2)."""
         rows = ctypes.c_int32(0)
@@ -327,6 +339,17 @@ class BoxSimulation:
         if got < 0:
             raise VxrError(-got, self.error())
         return out.reshape(self.substeps, -1), used.reshape(self.substeps, 2)
+
+    def residual_parts(self):
+        """The last step's per-sweep residuals in two parts, the pairs' and the walls', each shaped as residuals()
+        gives them (their larger is what residuals() gives)."""
+        count = self.L.vxr_box_residual_parts(self.h, None, None, 0)
+        pairs = np.zeros(count, np.float32)
+        walls = np.zeros(count, np.float32)
+        got = self.L.vxr_box_residual_parts(self.h, ptr(pairs), ptr(walls), count)
+        if got < 0:
+            raise VxrError(-got, self.error())
+        return pairs.reshape(self.substeps, -1), walls.reshape(self.substeps, -1)
 
     def error(self) -> str:
         return self.L.vxr_box_error(self.h).decode() if self.h else ""

@@ -158,35 +158,179 @@ def prediction_errors(net, feats, targets) -> dict:
                     "zero": rms(np.zeros_like(t[~carried]), t[~carried])}}
 
 
-def sweeps_to_residual(world, steps: int, tolerance: float, cap: int, mode: int, net=None, cold: bool = False):
-    """Mean solve sweeps a substep takes to reach the residual (at most `cap`), over `steps` steps, and the share of
-    substeps that reached it: the plain warm start (mode 0, or cold = from zero) or the network's (mode 2 or 3)."""
-    world.learned(net, mode)
-    world.measure(residual=True, cold_start=cold, sweeps=cap, tolerance=tolerance)
-    used_all = []
-    for _ in range(steps):
-        world.step_and_wait(1)
-        _, used = world.residuals()
-        used_all.extend(int(u) for u in used[:, 0])
-    world.learned(None, 0)
-    return float(np.mean(used_all)), float(np.mean([u < cap for u in used_all]))
+def rows_in_order(feats) -> np.ndarray:
+    """Feature rows as int32 words, sorted: two worlds list a round's pairs in the order their threads reached
+    them, so the same points can come in another order."""
+    v = np.ascontiguousarray(feats, np.float32).view(np.int32)
+    return v[np.lexsort(v.T[::-1])]
 
 
-def judge(world, net, steps: int = 3, tolerance: float = 1e-4, cap: int = 64) -> dict:
-    """The plain solver judges the network: sweeps to the residual from its impulses against from the carried ones
-    (and from zero), each over the same number of steps from where the world is. The network is tried on every
-    point (mode 2) and on the points that carried nothing (mode 3, the carried impulses kept elsewhere). It is kept,
-    in its better mode, only if it needs fewer sweeps; otherwise the plain warm start is the fallback."""
-    plain, plain_reached = sweeps_to_residual(world, steps, tolerance, cap, 0)
-    cold, cold_reached = sweeps_to_residual(world, steps, tolerance, cap, 0, cold=True)
-    learned, learned_reached = sweeps_to_residual(world, steps, tolerance, cap, 2, net)
-    fresh, fresh_reached = sweeps_to_residual(world, steps, tolerance, cap, 3, net)
+NETWORK_STARTS = ("carried", "zero", "network_all", "network_new")
+CEILING_STARTS = ("answers_all", "answers_new", "first_all", "first_new", "first_whole_all", "first_whole_new")
+
+
+def compare_starts(scene: dict, state13, net=None, starts=NETWORK_STARTS, samples: int = 3, lead: int = 2,
+                   tolerance: float = 1e-4, cap: int = 64, answer_tolerance: float = 1e-6, answer_cap: int = 256,
+                   device: int = 0) -> dict:
+    """Solve sweeps a substep needs to reach `tolerance` (at most `cap`) from each start, every start on the same
+    step. A twin world is made by loading the state (which clears the carried pairs) and stepping `lead` steps at the
+    scene's own sweeps, so every twin's measured step starts from the same state and the same carried impulses. The
+    starts: "carried" (the reference's warm start), "zero", the network on every point or on the points that carried
+    nothing ("network_all", "network_new", modes 2 and 3), and what a perfect predictor would give: the impulses a
+    twin's whole step reaches solved to `answer_tolerance` (at most `answer_cap` sweeps), the targets the network is
+    trained on ("answers_all", "answers_new"), or the impulses the solve sweeps of a twin's first substep alone reach
+    so solved, with no relax sweeps after them: the start from which that substep's solve needs no sweep, given as
+    the network's two targets a point ("first_all", "first_new") or as the whole impulse records, friction direction,
+    rolling impulses and the walls' records included ("first_whole_all", "first_whole_new"). The answer twins' features are compared with the measured
+    twin's as sorted rows (the answers are matched to the points by touching pair). `samples` steps, each from the
+    carried twin's state after the one before. Reports each start's mean solve sweeps a substep, its share of
+    substeps that reached the tolerance and its mean by substep within the step (a step's start is applied to its
+    first substep, the later substeps start from what the substep before reached), and by substep the sweeps the
+    pairs' part and the walls' part of the residual would each have needed alone."""
+    from .box_simulation import BoxSimulation
+    statics = [scene[k] for k in ("im", "hx", "hy", "hz", "shape")]
+    room = max(scene["sweeps"], answer_cap, cap)
+    reach = scene.get("reach_cells", 0)
+
+    def world():
+        return BoxSimulation(scene["bodies"], scene["substeps"], room, False, scene["grid"], reach, device=device)
+
+    needs_net = any(k.startswith("network") for k in starts)
+    if needs_net and net is None:
+        raise ValueError("the network's starts need a network")
+    b = world()
+    a = world() if any(k.startswith("answers") for k in starts) else None
+    a1 = world() if any(k.startswith("first") for k in starts) else None
+    used = {k: [] for k in starts}
+    pairs_alone = {k: [] for k in starts}
+    walls_alone = {k: [] for k in starts}
+    answered = {"answers": [], "first": []}
+    answer_residual = {"answers": [], "first": []}
+    aligned, checked = True, False
+    state = [np.asarray(f, np.float32) for f in state13]
+
+    def twin(w):
+        w.learned(None, 0)
+        w.first_substeps(0)
+        w.load_state(state + statics, scene["params"])
+        w.measure(residual=False, sweeps=scene["sweeps"])
+        w.step_and_wait(lead)
+
+    def answer(w, substeps):
+        twin(w)
+        w.first_substeps(substeps, solve_only=substeps > 0)
+        w.learned(None, 1)
+        w.measure(residual=True, sweeps=answer_cap, tolerance=answer_tolerance)
+        w.step_and_wait(1)
+        res, ran = w.residuals()
+        k = substeps or scene["substeps"]
+        last = [float(res[s, int(ran[s, 0])]) for s in range(k)]  # each substep's last solve sweep's residual
+        w.first_substeps(0)
+        return [int(u) < answer_cap for u in ran[:k, 0]], last, w.features()[0]
+
+    def alone(part, ran):
+        """Solve sweeps each substep's part of the residual needed alone: the first within the tolerance."""
+        out = []
+        for s in range(part.shape[0]):
+            n = int(ran[s])
+            hit = np.nonzero(part[s, 1:n + 1] <= tolerance)[0]
+            out.append(float(hit[0] + 1) if len(hit) else float(n))
+        return out
+
+    try:
+        for _ in range(samples):
+            feats = []
+            if a is not None:
+                got, last, f = answer(a, 0)
+                answered["answers"].extend(got)
+                answer_residual["answers"].extend(last)
+                feats.append(f)
+            if a1 is not None:
+                got, last, f = answer(a1, 1)
+                answered["first"].extend(got)
+                answer_residual["first"].extend(last)
+                feats.append(f)
+            nxt = None
+            for name in starts:
+                twin(b)
+                if name == "network_all":
+                    b.learned(net, 2)
+                elif name == "network_new":
+                    b.learned(net, 3)
+                elif name.startswith("answers"):
+                    b.learned_given(a, fresh_only=name.endswith("_new"))
+                elif name.startswith("first"):
+                    b.learned_given(a1, fresh_only=name.endswith("_new"), whole="whole" in name)
+                elif feats:
+                    b.learned(None, 1)  # features only: the step is the carried (or zero) start's own
+                b.measure(residual=True, cold_start=name == "zero", sweeps=cap, tolerance=tolerance)
+                b.step_and_wait(1)
+                ran = b.residuals()[1][:, 0]
+                used[name].append(ran.astype(np.float64))
+                pr, wr = b.residual_parts()
+                pairs_alone[name].append(alone(pr, ran))
+                walls_alone[name].append(alone(wr, ran))
+                if name == "carried":
+                    nxt = b.state()
+                    if feats:
+                        checked = True
+                        mine = rows_in_order(b.features()[0])
+                        aligned = aligned and all(np.array_equal(mine, rows_in_order(f)) for f in feats)
+            b.learned(None, 0)
+            state = nxt if nxt is not None else b.state()
+    finally:
+        for w in (a, a1, b):
+            if w is not None:
+                w.close()
+    mean = {k: float(np.mean(np.concatenate(v))) for k, v in used.items()}
+    out = {"samples": samples, "lead_steps": lead, "tolerance_m": tolerance, "cap": cap,
+           "mean_sweeps": mean,
+           "reached": {k: float(np.mean(np.concatenate(v) < cap)) for k, v in used.items()},
+           "by_substep": {k: [float(x) for x in np.mean(np.stack(v), 0)] for k, v in used.items()},
+           "pairs_alone_by_substep": {k: [float(x) for x in np.mean(np.array(v), 0)] for k, v in pairs_alone.items()},
+           "walls_alone_by_substep": {k: [float(x) for x in np.mean(np.array(v), 0)] for k, v in walls_alone.items()}}
+    if "carried" in mean:
+        out["gain_vs_carried"] = {k: (mean["carried"] / m if m > 0 else None) for k, m in mean.items()}
+    if a is not None or a1 is not None:
+        def worst(v):
+            return {"median": float(np.median(v)), "max": float(np.max(v))} if v else None
+        out["answers"] = {"tolerance_m": answer_tolerance, "cap": answer_cap,
+                          "reached_whole_step": float(np.mean(answered["answers"])) if answered["answers"] else None,
+                          "reached_first_substep": float(np.mean(answered["first"])) if answered["first"] else None,
+                          "last_solve_residual_m": {"whole_step": worst(answer_residual["answers"]),
+                                                    "first_substep": worst(answer_residual["first"])}}
+        out["twins_aligned"] = bool(aligned) if checked else None
+    return out
+
+
+def judge(scene: dict, state13, net, samples: int = 3, tolerance: float = 1e-4, cap: int = 64, ceiling: bool = False,
+          device: int = 0) -> dict:
+    """The plain solver judges the network, every start on the same steps (compare_starts from `state13`): sweeps to
+    the residual from the network's impulses on every point (mode 2) and on the points that carried nothing (mode 3),
+    against from the carried ones and from zero. The network is kept, in its better mode, only if it needs fewer
+    sweeps than the carried impulses; otherwise the plain warm start is the fallback. With `ceiling`, the same steps
+    are also taken from the answers a perfect predictor would give."""
+    starts = NETWORK_STARTS + (CEILING_STARTS if ceiling else ())
+    r = compare_starts(scene, state13, net, starts=starts, samples=samples, tolerance=tolerance, cap=cap,
+                       device=device)
+    m, reached = r["mean_sweeps"], r["reached"]
+    plain, cold, learned, fresh = m["carried"], m["zero"], m["network_all"], m["network_new"]
     best_mode, best = (2, learned) if learned <= fresh else (3, fresh)
     use = best < plain
-    return {"plain_warm_start": plain, "plain_warm_start_reached": plain_reached, "plain_cold_start": cold,
-            "plain_cold_start_reached": cold_reached, "learned": learned, "learned_reached": learned_reached,
-            "learned_new_contacts_only": fresh, "learned_new_contacts_only_reached": fresh_reached,
-            "gain_vs_warm_start": plain / best if best > 0 else None,
-            "gain_vs_cold_start": cold / best if best > 0 else None,
-            "kept": bool(use), "mode": best_mode if use else 0,
-            "fallback": None if use else "plain warm start (the network needs no fewer sweeps in either mode)"}
+    verdict = {"plain_warm_start": plain, "plain_warm_start_reached": reached["carried"], "plain_cold_start": cold,
+               "plain_cold_start_reached": reached["zero"], "learned": learned,
+               "learned_reached": reached["network_all"], "learned_new_contacts_only": fresh,
+               "learned_new_contacts_only_reached": reached["network_new"],
+               "gain_vs_warm_start": plain / best if best > 0 else None,
+               "gain_vs_cold_start": cold / best if best > 0 else None,
+               "kept": bool(use), "mode": best_mode if use else 0,
+               "fallback": None if use else "plain warm start (the network needs no fewer sweeps in either mode)",
+               "same_steps": {"samples": samples, "lead_steps": r["lead_steps"], "by_substep": r["by_substep"],
+                              "pairs_alone_by_substep": r["pairs_alone_by_substep"],
+                              "walls_alone_by_substep": r["walls_alone_by_substep"]}}
+    if ceiling:
+        verdict["ceiling"] = {"mean_sweeps": {k: m[k] for k in CEILING_STARTS},
+                              "reached": {k: reached[k] for k in CEILING_STARTS},
+                              "gain_vs_carried": {k: r["gain_vs_carried"][k] for k in CEILING_STARTS},
+                              "answers": r["answers"], "twins_aligned": r["twins_aligned"]}
+    return verdict
