@@ -38,6 +38,9 @@ constexpr int SHRINK_AFTER = 120;      // SphereStepper.java:53
 constexpr int SHOWN = 40, PRESSED_BEFORE = 8, PRESSED_AFTER = 20, TURNED_BEFORE = 32, TURNED_AFTER = 36;
 constexpr int LISTED = 0, MISSED = 1, LONGEST = 2;
 constexpr int THREADS = 512;
+static_assert(THREADS % 32 == 0, "spheres are dealt out to the blocks by whole warps");
+constexpr int SLICES_MOST = 1024;
+constexpr int STAGE_MOST = 200 * 1024;  // shared memory a block may give a staged walk (the SM has 227 KB a block)  // blocks of a shared scan: a GPU holds at most 2048 / THREADS blocks an SM
 
 struct SParams {
     float w[P_COUNT];
@@ -97,6 +100,10 @@ struct Kernel {
     int* list_count;   // [n]
     int* near;         // [n * NEAR_KEPT] each sphere's first near partners, in the walk's order
     int* part;         // [blocks] each block's slice total in a scan the blocks share
+    int* scan_tmp;     // [max(cells, n) + 1] a shared scan's slice-local prefixes
+    const float* weight;  // the inverse masses a neighbour walk reads, weight[o * wstride]
+    int wstride;
+    int stage;         // 1: each block stages a walk's reads in its shared memory (staged_kernel)
     ListGen gen[2];
     Counts* counts;
     int* opening;      // [iterations] the rounds each pass's opening batch runs (SphereStepper.opening)
@@ -422,10 +429,9 @@ __device__ __forceinline__ int cell_key(const Kernel& K, float x, float y, float
 template <bool WEIGHTS = false, typename Visit>
 __device__ __forceinline__ void around(const Kernel& K, int s, Visit visit) {
     const float4* pos = K.s.pos;
-    const float4* disp = K.s.disp;
     if (!K.gridded) {
         for (int o = 0; o < K.n; o++) {
-            if constexpr (WEIGHTS) visit(o, pos[o], disp[o].w);
+            if constexpr (WEIGHTS) visit(o, pos[o], K.weight[(size_t)o * K.wstride]);
             else visit(o, pos[o]);
         }
         return;
@@ -452,10 +458,10 @@ __device__ __forceinline__ void around(const Kernel& K, int s, Visit visit) {
             if (m > 3) p3 = pos[o3];
             float w0 = 0.0f, w1 = 0.0f, w2 = 0.0f, w3 = 0.0f;
             if constexpr (WEIGHTS) {
-                w0 = disp[o0].w;
-                if (m > 1) w1 = disp[o1].w;
-                if (m > 2) w2 = disp[o2].w;
-                if (m > 3) w3 = disp[o3].w;
+                w0 = K.weight[(size_t)o0 * K.wstride];
+                if (m > 1) w1 = K.weight[(size_t)o1 * K.wstride];
+                if (m > 2) w2 = K.weight[(size_t)o2 * K.wstride];
+                if (m > 3) w3 = K.weight[(size_t)o3 * K.wstride];
             }
             for (int j = 0; j < m; j++) {
                 if constexpr (WEIGHTS) visit(o0, p0, w0);
@@ -578,6 +584,8 @@ __device__ __forceinline__ void walls(const Kernel& K, int s) {
 }
 
 // Spheres.solve(grid) :302-347 / Solving :1245-1298: Jacobi's move into cx, cy, cz.
+constexpr int CONTACTS_HELD = 16;  // a sphere's contacts a Jacobi walk lists before solving them
+
 __device__ __forceinline__ void jacobi_solve(const Kernel& K, int s) {
     const State& S = K.s;
     const float4 me = S.pos[s];
@@ -585,21 +593,49 @@ __device__ __forceinline__ void jacobi_solve(const Kernel& K, int s) {
     const float rs = me.w, ws = S.disp[s].w;
     float sum[3] = {0.0f, 0.0f, 0.0f};
     float contacts = 0.0f;
-    around<true>(K, s, [&](int o, float4 other, float wo) {
-        if (o == s) return;
-        float d[3] = {mine[0] - other.x, mine[1] - other.y, mine[2] - other.z};
+    // Whether o touches s, and if so its share of the move: the same arithmetic in both passes below.
+    auto touching = [&](float4 other, float wo, float* d, float& reach, float& wsum) {
+        d[0] = mine[0] - other.x, d[1] = mine[1] - other.y, d[2] = mine[2] - other.z;
         const float d2 = d[0] * d[0] + (d[1] * d[1] + d[2] * d[2]);
-        const float reach = rs + other.w;
-        const float wsum = ws + wo;
-        if (!(d2 < reach * reach)) return;
-        if (!(d2 > COINCIDENT)) return;
-        if (!(wsum > 0.0f)) return;
+        reach = rs + other.w;
+        wsum = ws + wo;
+        return d2 < reach * reach && d2 > COINCIDENT && wsum > 0.0f;
+    };
+    auto add = [&](const float* d, float reach, float wsum) {
+        const float d2 = d[0] * d[0] + (d[1] * d[1] + d[2] * d[2]);
         const float dist = sqrtf(d2);
         const float share = ((reach - dist) * (ws / wsum)) / dist;
 #pragma unroll
         for (int a = 0; a < 3; a++) sum[a] = sum[a] + share * d[a];
         contacts = contacts + 1.0f;
+    };
+    // First the walk lists the touching spheres in its order (a cheap test a candidate), then they are solved in
+    // that order: the lanes of a warp, each walking its own sphere, then run the square root and the divisions once
+    // a contact, not once for every candidate any lane finds touching. A sphere touching more than CONTACTS_HELD
+    // walks again, solving as it goes.
+    int held[CONTACTS_HELD];
+    int count = 0;
+    around<true>(K, s, [&](int o, float4 other, float wo) {
+        if (o == s) return;
+        float d[3], reach, wsum;
+        if (!touching(other, wo, d, reach, wsum)) return;
+        if (count < CONTACTS_HELD) held[count] = o;
+        count++;
     });
+    if (count <= CONTACTS_HELD) {
+        for (int k = 0; k < count; k++) {
+            const int o = held[k];
+            float d[3], reach, wsum;
+            touching(S.pos[o], K.weight[(size_t)o * K.wstride], d, reach, wsum);
+            add(d, reach, wsum);
+        }
+    } else {
+        around<true>(K, s, [&](int o, float4 other, float wo) {
+            if (o == s) return;
+            float d[3], reach, wsum;
+            if (touching(other, wo, d, reach, wsum)) add(d, reach, wsum);
+        });
+    }
     const float omega = K.p.w[OMEGA];
     float scale = omega;
     if (K.p.w[AVERAGED] > 0.0f) scale = omega / fmaxf(contacts, 1.0f);
@@ -781,9 +817,8 @@ __device__ __forceinline__ int count_near(const Kernel& K, int a) {
 
 // listContacts' second half: sphere a's contacts written at the places the scan gave it, chained, each with the
 // impulses the pair took in the substep before (found by walking a's kept chain, at most MOST_KEPT places).
-__device__ __forceinline__ void fill_near(const Kernel& K, const ListGen& L, const ListGen& kept, int a) {
+__device__ __forceinline__ void fill_near(const Kernel& K, const ListGen& L, const ListGen& kept, int a, int first) {
     const float4 me = K.s.pos[a];
-    const int first = L.start[a];
     int slot = first;
     int last = -1;
     // a's kept chain, at most MOST_KEPT places from its head: the places of that range, searched with independent
@@ -808,7 +843,7 @@ __device__ __forceinline__ void fill_near(const Kernel& K, const ListGen& L, con
         L.imp[2 * (size_t)at] = w0;
         L.imp[2 * (size_t)at + 1] = w1;
     };
-    const int found = L.start[a + 1] - first;
+    const int found = K.list_count[a];
     if (found <= NEAR_KEPT) {  // the partners the count kept, in the walk's order
         const int* keep = K.near + (size_t)a * NEAR_KEPT;
         for (int i = 0; i < found; i++) place(keep[i]);
@@ -938,14 +973,42 @@ __device__ __forceinline__ void scan_slices(const Kernel& K, const int* in, int*
     const int total = block_scan_range(in, out, lo, hi);
     if (threadIdx.x == 0) K.part[blockIdx.x] = total;
 }
-__device__ __forceinline__ int scan_finish(const Kernel& K, int* out, int m) {
+// After the barrier that follows scan_slices: the slice totals' exclusive prefix in this block's shared memory
+// (slice b's offset at offs[b], the whole at offs[gridDim.x]), summed by one warp.
+__device__ __forceinline__ void slice_offsets(const Kernel& K, int* offs) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int carry = 0;
+        for (int base = 0; base < (int)gridDim.x; base += 32) {
+            const int b = base + lane;
+            const int v = b < (int)gridDim.x ? *(const volatile int*)&K.part[b] : 0;
+            int x = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (b < (int)gridDim.x) offs[b] = carry + x - v;
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (lane == 0) offs[gridDim.x] = carry;
+    }
+    __syncthreads();
+}
+
+// Element i of the scan scan_slices left slice-local in `local`: any slice's, in the same pass as the finish.
+__device__ __forceinline__ int scan_value(const int* local, const int* offs, int i, int m) {
+    const int per = (m + gridDim.x - 1) / gridDim.x;
+    return local[i] + offs[i / per];
+}
+
+// The block's own slice of the scan made whole into `out` (out[m]: the whole, from the last block); returns the whole.
+__device__ __forceinline__ int scan_finish(const int* local, const int* offs, int* out, int m) {
     const int per = (m + gridDim.x - 1) / gridDim.x;
     const int lo = min(m, (int)blockIdx.x * per), hi = min(m, lo + per);
-    int offset = 0;
-    for (int b = 0; b < (int)blockIdx.x; b++) offset += *(const volatile int*)&K.part[b];
-    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) out[i] += offset;
-    int whole = 0;
-    for (int b = 0; b < (int)gridDim.x; b++) whole += *(const volatile int*)&K.part[b];
+    const int offset = offs[blockIdx.x];
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) out[i] = local[i] + offset;
+    const int whole = offs[gridDim.x];
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[m] = whole;
     return whole;
 }
@@ -971,22 +1034,127 @@ __device__ __forceinline__ void cluster_sync() {
         }                                                         \
     } while (0)
 
+__device__ __forceinline__ unsigned shared_addr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// One bulk copy (the TMA engine, no multicast) from global memory into this block's shared memory, counted on `bar`;
+// both addresses 16-byte aligned, `bytes` a multiple of 16.
+__device__ __forceinline__ void bulk_to_shared(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(shared_addr(dst)), "l"(src), "r"(bytes), "r"(shared_addr(bar))
+                 : "memory");
+}
+
+// Waits for phase `parity` of `bar` to complete, at most limit_ns; false when the wait ran out.
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity, unsigned long long limit_ns) {
+    const unsigned long long start = global_ns();
+    unsigned spins = 0;
+    for (;;) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(shared_addr(bar)), "r"(parity)
+                     : "memory");
+        if (done) return true;
+        if (((++spins & 255u) == 0u || spins == 1u) && global_ns() - start > limit_ns) return false;
+    }
+}
+
+// Bytes of a block's staged copy for n spheres over `cells` cells: positions and displacements (whose .w is the
+// inverse mass) as float4, then the sort's order and the cell starts, each padded to 16 bytes.
+__host__ __device__ constexpr long staged_bytes(long n, long cells) {
+    return 32 * n + 4 * ((n + 3) & ~3L) + 4 * ((cells + 1 + 3) & ~3L);
+}
+
+// A neighbour walk's reads (positions, inverse masses, the sort's order, the cell starts), copied into the block's
+// shared memory by bulk copies after the barrier that ended their writes, and K reading them from there: a pass that
+// writes none of them walks shared memory instead of making its chain of loads from L2. The same values in the same
+// order, so the same results. Without staging (a scene too large for it), or once a copy's wait has run out (the
+// status word then says so), K itself. Every thread of the block calls it, right after a barrier.
+struct Stage {
+    unsigned long long* bar;  // the copies' mbarrier
+    int* broken;              // nonzero once a wait ran out: the walks read global memory from then on
+    unsigned parity;          // the phase the next copies complete
+};
+
+__device__ __forceinline__ Kernel staged_kernel(const Kernel& K, float4* smem, Stage& st) {
+    Kernel KS = K;
+    if (!K.stage || *st.broken) return KS;
+    const int n = K.n;
+    float4* spos = smem;
+    float4* sdisp = spos + n;
+    int* sorder = reinterpret_cast<int*>(sdisp + n);
+    int* sstart = sorder + ((n + 3) & ~3);
+    const unsigned order_bulk = 4u * (unsigned)(n & ~3), start_bulk = 4u * (unsigned)((K.cells + 1) & ~3);
+    if (threadIdx.x == 0) {
+        // the sources' writes (ordered before by the barrier) and this block's reads of the old copy, before the
+        // copy engine's accesses
+        asm volatile("fence.proxy.async.global;\n\tfence.proxy.async.shared::cta;" ::: "memory");
+        const unsigned bytes = 32u * (unsigned)n + order_bulk + start_bulk;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(shared_addr(st.bar)), "r"(bytes)
+                     : "memory");
+        bulk_to_shared(spos, K.s.pos, 16u * (unsigned)n, st.bar);
+        bulk_to_shared(sdisp, K.s.disp, 16u * (unsigned)n, st.bar);
+        if (order_bulk) bulk_to_shared(sorder, K.order, order_bulk, st.bar);
+        if (start_bulk) bulk_to_shared(sstart, K.cell_start, start_bulk, st.bar);
+    }
+    for (int i = (n & ~3) + threadIdx.x; i < n; i += blockDim.x) sorder[i] = K.order[i];  // the ragged ends
+    for (int i = ((K.cells + 1) & ~3) + threadIdx.x; i <= K.cells; i += blockDim.x) sstart[i] = K.cell_start[i];
+    bool ok = bar_wait(st.bar, st.parity, K.bar.limit_ns);
+    if (!ok) ok = bar_wait(st.bar, st.parity, K.bar.limit_ns);  // the copies in flight, once more
+    st.parity ^= 1u;
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) {
+            *st.broken = 1;
+            atomicCAS(&K.counts->status, ST_OK, ST_TIMEOUT);
+        }
+        __syncthreads();
+        return KS;
+    }
+    KS.s.pos = spos;
+    KS.order = sorder;
+    KS.cell_start = sstart;
+    KS.weight = reinterpret_cast<const float*>(sdisp) + 3;  // sdisp[o].w
+    KS.wstride = 4;
+    return KS;
+}
+
 // `steps` whole steps (SphereStep's pass list :184-196; SphereStepper.step :66-103 when run until done).
 __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
+    extern __shared__ float4 staged[];
+    __shared__ unsigned long long stage_bar;
+    __shared__ int stage_broken;
+    Stage stage{&stage_bar, &stage_broken, 0u};
+    if (K.stage) {
+        if (threadIdx.x == 0) {
+            stage_broken = 0;
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(shared_addr(&stage_bar)) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+    }
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gsize = gridDim.x * blockDim.x;
+    // Spheres (and cells) are dealt out a warp's run of 32 at a time, in turn to each block, so that every block has
+    // a share when there are fewer spheres than threads: a permutation of 0 .. gsize - 1, as gtid is.
+    const int stid = ((threadIdx.x >> 5) * gridDim.x + blockIdx.x) * 32 + (threadIdx.x & 31);
     const int n = K.n;
     unsigned int epoch = 0;
     int cur = read_int(&K.counts->cur);
     const bool gs = K.solve != 0;
     const int limit = K.limit;
+    // Without restitution the bounce pass changes nothing, so neither it nor the barriers around it are needed.
+    const bool bouncing = K.p.w[RESTITUTION] > 0.0f;
+    __shared__ int offs[SLICES_MOST + 1];
     for (int step = 0; step < K.steps; step++) {
         if (gtid == 0) {
             for (int k = 0; k < 4; k++) K.counts->last[k] = 0;
         }
         for (int sub = 0; sub < K.substeps; sub++) {
             // predict; the cell of each centre, counted; the walls' warm start; every claim cleared
-            for (int s = gtid; s < n; s += gsize) {
+            for (int s = stid; s < n; s += gsize) {
                 if (sub > 0) bounced(K, s);
                 predict(K, s);
                 if (K.gridded) {
@@ -1008,18 +1176,19 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
             }
             SYNC();
             if (K.gridded) {
-                scan_slices(K, K.cell_count, K.cell_start, K.cells);
+                scan_slices(K, K.cell_count, K.scan_tmp, K.cells);
                 SYNC();
-                scan_finish(K, K.cell_start, K.cells);
-                SYNC();
-                // a place in its cell for each sphere; the counts return to zero for the next substep
-                for (int s = gtid; s < n; s += gsize) {
+                // the scan made whole, and in the same pass a place in its cell for each sphere (each block adds the
+                // slice offsets itself); the counts return to zero for the next substep
+                slice_offsets(K, offs);
+                scan_finish(K.scan_tmp, offs, K.cell_start, K.cells);
+                for (int s = stid; s < n; s += gsize) {
                     const int key = K.keys[s];
-                    K.order[K.cell_start[key] + atomicSub(&K.cell_count[key], 1) - 1] = s;
+                    K.order[scan_value(K.scan_tmp, offs, key, K.cells) + atomicSub(&K.cell_count[key], 1) - 1] = s;
                 }
                 SYNC();
                 // within a cell, ascending index: the stable counting sort's order
-                for (int c = gtid; c < K.cells; c += gsize) {
+                for (int c = stid; c < K.cells; c += gsize) {
                     const int begin = K.cell_start[c], end = K.cell_start[c + 1];
                     for (int i = begin + 1; i < end; i++) {
                         const int v = K.order[i];
@@ -1035,19 +1204,21 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
             }
             int listed = 0;
             if (gs) {
-                for (int a = gtid; a < n; a += gsize) K.list_count[a] = count_near(K, a);
+                // the walks of the count and the fill read the staged copy (positions change in neither)
+                const Kernel KS = staged_kernel(K, staged, stage);
+                for (int a = stid; a < n; a += gsize) K.list_count[a] = count_near(KS, a);
                 SYNC();
                 int* start = K.gen[cur ^ 1].start;  // the new list's
-                scan_slices(K, K.list_count, start, n);
+                scan_slices(K, K.list_count, K.scan_tmp, n);
                 SYNC();
+                slice_offsets(K, offs);
                 {
-                    const int whole = scan_finish(K, start, n);
+                    const int whole = scan_finish(K.scan_tmp, offs, start, n);
                     if (gtid == 0) K.counts->count[LISTED] = whole;
                 }
-                SYNC();
                 cur ^= 1;
                 const ListGen L = K.gen[cur], kept = K.gen[cur ^ 1];
-                for (int a = gtid; a < n; a += gsize) fill_near(K, L, kept, a);
+                for (int a = stid; a < n; a += gsize) fill_near(KS, L, kept, a, scan_value(K.scan_tmp, offs, a, n));
                 SYNC();
                 listed = min(read_int(&K.counts->count[LISTED]), K.cap);
             }
@@ -1061,10 +1232,20 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
             }
             for (int it = 0; it < K.iterations; it++) {
                 if (K.solve == 0) {
-                    for (int s = gtid; s < n; s += gsize) jacobi_solve(K, s);
+                    {
+                        const Kernel KS = staged_kernel(K, staged, stage);
+                        for (int s = stid; s < n; s += gsize) jacobi_solve(KS, s);
+                    }
                     SYNC();
-                    for (int s = gtid; s < n; s += gsize) jacobi_apply(K, s);
-                    SYNC();
+                    if (it == K.iterations - 1) {  // the last: each sphere's velocity right after its move
+                        for (int s = stid; s < n; s += gsize) {
+                            jacobi_apply(K, s);
+                            velocity(K, s);
+                        }
+                    } else {
+                        for (int s = stid; s < n; s += gsize) jacobi_apply(K, s);
+                        SYNC();
+                    }
                     continue;
                 }
                 if (K.solve == 2) {
@@ -1077,7 +1258,7 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
                                       K.claims + ((g + 1) % 3) * n, gtid, gsize, mine);
                         SYNC();
                     }
-                    for (int s = gtid; s < n; s += gsize) walls(K, s);
+                    for (int s = stid; s < n; s += gsize) walls(K, s);
                     SYNC();
                     continue;
                 }
@@ -1120,7 +1301,7 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
                         SYNC();
                     }
                 }
-                for (int s = gtid; s < n; s += gsize) walls(K, s);
+                for (int s = stid; s < n; s += gsize) walls(K, s);
                 if (gtid == 0) {
                     Counts* c = K.counts;
                     const int unlisted = max(0, c->count[LISTED] - K.cap);
@@ -1143,15 +1324,24 @@ __global__ void __launch_bounds__(THREADS) k_sphere_steps(Kernel K) {
                 }
                 SYNC();
             }
-            for (int s = gtid; s < n; s += gsize) velocity(K, s);
-            SYNC();
-            for (int s = gtid; s < n; s += gsize) bounce(K, s);
-            SYNC();
+            if (K.solve != 0)
+                for (int s = stid; s < n; s += gsize) velocity(K, s);
+            if (bouncing) {  // bounce reads the neighbours' velocities
+                SYNC();
+                for (int s = stid; s < n; s += gsize) bounce(K, s);
+                SYNC();
+            } else if (sub == K.substeps - 1) {
+                SYNC();  // the picture reads the neighbours' positions
+            }
         }
-        // the last substep's restitution added, then the picture's buffer
-        for (int s = gtid; s < n; s += gsize) {
-            bounced(K, s);
-            show(K, s);
+        // the last substep's restitution added, then the picture's buffer (its walk reads the staged copy: neither
+        // pass moves a sphere)
+        {
+            const Kernel KS = staged_kernel(K, staged, stage);
+            for (int s = stid; s < n; s += gsize) {
+                bounced(K, s);
+                show(KS, s);
+            }
         }
         SYNC();
     }
@@ -1240,6 +1430,8 @@ struct vxr_sphere_world {
     float* shown = nullptr;
     int *keys = nullptr, *order = nullptr, *cell_count = nullptr, *cell_start = nullptr;
     int* part = nullptr;  // [blocks] the blocks' slice totals of a shared scan
+    int* scan_tmp = nullptr;  // [max(cells, n) + 1] the slice-local prefixes of a shared scan
+    int stage_bytes = 0;      // each block's shared memory for a staged walk (0: the walks read global memory)
     int *claims = nullptr, *list_count = nullptr, *near = nullptr;
     ListGen gen[2]{};
     Counts* counts = nullptr;
@@ -1377,6 +1569,10 @@ Kernel kernel_of(vxr_sphere_world* w, int steps) {
     K.list_count = w->list_count;
     K.near = w->near;
     K.part = w->part;
+    K.scan_tmp = w->scan_tmp;
+    K.weight = reinterpret_cast<const float*>(w->s.disp) + 3;  // disp[o].w
+    K.wstride = 4;
+    K.stage = w->stage_bytes > 0;
     K.gen[0] = w->gen[0];
     K.gen[1] = w->gen[1];
     K.counts = w->counts;
@@ -1400,11 +1596,12 @@ int launch_steps(vxr_sphere_world* w, int steps) {
     void* args[] = {&K};
     cudaError_t e;
     if (w->blocks == 1) {
-        e = cudaLaunchKernel((const void*)k_sphere_steps, dim3(1), dim3(THREADS), args, 0, st);
+        e = cudaLaunchKernel((const void*)k_sphere_steps, dim3(1), dim3(THREADS), args, w->stage_bytes, st);
     } else if (w->cluster) {  // every block in one cluster: co-scheduled by the hardware, the cluster barrier between
         cudaLaunchConfig_t c = {};
         c.gridDim = dim3(w->blocks);
         c.blockDim = dim3(THREADS);
+        c.dynamicSmemBytes = w->stage_bytes;
         c.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1415,7 +1612,8 @@ int launch_steps(vxr_sphere_world* w, int steps) {
         c.numAttrs = 1;
         e = cudaLaunchKernelExC(&c, (const void*)k_sphere_steps, args);
     } else {
-        e = cudaLaunchCooperativeKernel((const void*)k_sphere_steps, dim3(w->blocks), dim3(THREADS), args, 0, st);
+        e = cudaLaunchCooperativeKernel((const void*)k_sphere_steps, dim3(w->blocks), dim3(THREADS), args,
+                                        w->stage_bytes, st);
     }
     if (e != cudaSuccess) return sfail(w, VXR_ECUDA, std::string("sphere step launch: ") + cudaGetErrorString(e));
     w->launches++;
@@ -1447,7 +1645,10 @@ int finish(vxr_sphere_world* w, vxr_sphere_report* report) {
     if (c.status == ST_ROUNDS)
         return sfail(w, VXR_EROUNDS, "a pass is still open after " + std::to_string(c.rounds_at) +
                                          " rounds, on a list of " + std::to_string(c.count[LISTED]));
-    if (c.status == ST_TIMEOUT) return sfail(w, VXR_ETIMEOUT, "a grid barrier's wait ran out; the step stopped");
+    if (c.status == ST_TIMEOUT)
+        return sfail(w, VXR_ETIMEOUT,
+                     "a device wait ran out (a grid barrier's, or a staged copy's); the step stopped or walked global "
+                     "memory from then on");
     if (c.status != ST_OK) return sfail(w, VXR_ECUDA, "device status " + std::to_string(c.status));
     return VXR_OK;
 }
@@ -1572,9 +1773,20 @@ vxr_sphere_world* vxr_sphere_create(const vxr_sphere_config* cfg, int32_t* statu
     }
     if (rc) return bad(VXR_ECUDA);
     if (cudaMallocHost(&w->host_counts, sizeof(Counts)) != cudaSuccess) return bad(VXR_ECUDA);
+    // A staged walk's copy (positions, displacements, the sort's order, cell starts) where one block's shared
+    // memory holds it: the 4,096-sphere pile takes 180 KB.
+    if (w->gridded) {
+        const size_t bytes = (size_t)staged_bytes(n, w->cells);
+        if (bytes <= (size_t)STAGE_MOST &&
+            cudaFuncSetAttribute(k_sphere_steps, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_MOST) ==
+                cudaSuccess)
+            w->stage_bytes = (int)bytes;
+        else
+            cudaGetLastError();
+    }
     // One block while the scene is small enough that a block's barrier beats a grid's; otherwise every SM.
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sphere_steps, THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sphere_steps, THREADS, w->stage_bytes);
     const int most = std::max(1, per_sm) * w->sms;
     const long work = std::max<long>(n, w->solve != 0 ? 3L * n : n);
     int blocks = cfg->blocks > 0 ? cfg->blocks : (n <= VXR_SPHERE_ONE_BLOCK ? 1 : (int)((work + THREADS - 1) / THREADS));
@@ -1597,6 +1809,7 @@ vxr_sphere_world* vxr_sphere_create(const vxr_sphere_config* cfg, int32_t* statu
         cudaLaunchConfig_t c = {};
         c.gridDim = dim3(size);
         c.blockDim = dim3(THREADS);
+        c.dynamicSmemBytes = w->stage_bytes;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = size;
@@ -1623,7 +1836,9 @@ vxr_sphere_world* vxr_sphere_create(const vxr_sphere_config* cfg, int32_t* statu
         w->blocks = cluster;
         w->cluster = 1;
     }
+    if (w->blocks > SLICES_MOST) return bad(VXR_EINVAL);
     if (salloc(w, &w->part, (size_t)std::max(w->blocks, 1)) != VXR_OK) return bad(VXR_ECUDA);
+    if (salloc(w, &w->scan_tmp, (size_t)std::max(w->cells, n) + 1) != VXR_OK) return bad(VXR_ECUDA);
     // the stepper's batch sizing starts at BATCH a pass (SphereStepper.java:59-64)
     std::vector<int> batch(w->iterations, BATCH);
     if (cudaMemcpy(w->opening, batch.data(), sizeof(int) * w->iterations, cudaMemcpyHostToDevice) != cudaSuccess)
