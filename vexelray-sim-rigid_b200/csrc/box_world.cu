@@ -49,14 +49,24 @@ constexpr int BUCKETS = (MOST_ROUNDS + 1) * PAIR_KINDS;
 constexpr int ALL_BUCKETS = 2 * BUCKETS;
 // Islands: connected components of the placed touching pairs. A component of at most ISLAND_MOST bodies is solved
 // whole by one block, its bodies in shared memory, its rounds apart by block barriers; larger ones go through the grid
-// phases. Components are packed into groups in order of their roots: a group takes components until GROUP_BASE bodies
-// have been placed, so it holds at most GROUP_BASE + ISLAND_MOST - 1 bodies.
+// phases. Components are packed into groups in order of their roots: a group takes components until `base` bodies
+// have been placed, so it holds at most base + ISLAND_MOST - 1 bodies. The base is chosen each step so that the island
+// blocks take one group each where the small components' bodies allow it (group_base_of).
 constexpr int ISLAND_MOST = 256;
-constexpr int GROUP_BASE = 256;
-constexpr int GROUP_CAP = 512;
+constexpr int GROUP_BASE_LEAST = 256;
+constexpr int GROUP_CAP = 640;  // a group's bodies in a block's shared memory (44 KB, under the 48 KB of static memory)
 constexpr int GROUP_ROUNDS = MOST_ROUNDS;                // placed pairs only
 constexpr int GROUP_LISTS = GROUP_ROUNDS * PAIR_KINDS;  // a group's pairs listed by (round, kind)
 constexpr int ISLAND_THREADS = 256;                      // a block a group
+
+// Bodies placed before a group's components stop: the small components' bodies shared evenly by the island blocks,
+// at least GROUP_BASE_LEAST and at most GROUP_CAP - ISLAND_MOST (a group then holds at most GROUP_CAP - 1 bodies).
+// With 107,445 such bodies and 296 blocks (the large scene early in its drop) that is 363: 296 groups, where a base of
+// 256 made 420 and left 124 blocks two groups in turn.
+__host__ __device__ inline int group_base_of(int island_bodies, int blocks) {
+    const int even = (island_bodies + (blocks > 0 ? blocks : 1) - 1) / (blocks > 0 ? blocks : 1);
+    return even < GROUP_BASE_LEAST ? GROUP_BASE_LEAST : (even > GROUP_CAP - ISLAND_MOST ? GROUP_CAP - ISLAND_MOST : even);
+}
 
 // ------------------------------------------------------------------------------------------------------------
 // Device buffers of a world.
@@ -918,16 +928,16 @@ __global__ void k_classify(int n, const int* __restrict__ root, const int* __res
 }
 
 // Where each group's bodies begin: the place of its first component (a component that began in the group before may
-// reach past the group's GROUP_BASE boundary, so a group's places start at its own first component, not there).
+// reach past its group's boundary, so a group's places start at its own first component, not there).
 __global__ void k_group_base(int n, const int* __restrict__ root, const int* __restrict__ size,
                              const int* __restrict__ offset, const int* __restrict__ body_group,
-                             int* __restrict__ group_base) {
+                             int* __restrict__ group_base, int blocks) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n || root[s] != s || body_group[s] == -2) return;
     const int m = size[s];
     if (m == 1) return;
     const int at = offset[s];
-    atomicMin(&group_base[at / GROUP_BASE], at);
+    atomicMin(&group_base[at / group_base_of(offset[n], blocks)], at);
 }
 
 // A small component's bodies: the group its root's place falls in, and places in that group one after another from
@@ -935,14 +945,14 @@ __global__ void k_group_base(int n, const int* __restrict__ root, const int* __r
 __global__ void k_assign(int n, const int* __restrict__ root, const int* __restrict__ size,
                          const int* __restrict__ offset, const int* __restrict__ group_base, int* __restrict__ fill,
                          int* __restrict__ body_group, int* __restrict__ body_local, int* __restrict__ group_body,
-                         int* __restrict__ group_count) {
+                         int* __restrict__ group_count, int blocks) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const int r = root[s];
     const int m = size[r];
     if (m == 1 || body_group[s] == -2) return;
     const int at = offset[r];
-    const int g = at / GROUP_BASE;
+    const int g = at / group_base_of(offset[n], blocks);
     const int local = (at - group_base[g]) + atomicAdd(&fill[r], 1);
     body_group[s] = g;
     body_local[s] = local;
@@ -1956,7 +1966,9 @@ __device__ __forceinline__ void run_alone(const SolveArgs& A, int s) {
 // Blocks take items from a counter: the groups first (the longer chains), then runs of lone bodies, one a thread.
 __global__ void __launch_bounds__(ISLAND_THREADS, 2) k_islands(SolveArgs A, IslandArgs I) {
     __shared__ GroupBodies G;
-    const int ngroups = (*I.island_n + GROUP_BASE - 1) / GROUP_BASE;
+    const int island = *I.island_n;
+    const int base = group_base_of(island, gridDim.x);
+    const int ngroups = (island + base - 1) / base;
     const int nfree = *(volatile const int*)&A.counters->free_n;
     const int items = ngroups + (nfree + ISLAND_THREADS - 1) / ISLAND_THREADS;
     for (;;) {
@@ -2520,10 +2532,11 @@ int enqueue_step(vxr_box_world* w) {
             VXR_CUDA(cudaMemsetAsync(w->group_count, 0, sizeof(int) * w->groups_max, st));
             VXR_CUDA(cudaMemsetAsync(w->group_base, 0x7f, sizeof(int) * w->groups_max, st));
             k_group_base<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_offset,
-                                                                    w->body_group, w->group_base);
+                                                                    w->body_group, w->group_base, w->island_blocks);
             k_assign<<<blocks_for(n, THREADS), THREADS, 0, st>>>(n, w->comp, w->isl_size, w->isl_offset,
                                                                 w->group_base, w->isl_fill, w->body_group,
-                                                                w->body_local, w->group_body, w->group_count);
+                                                                w->body_local, w->group_body, w->group_count,
+                                                                w->island_blocks);
             VXR_CUDA(cudaMemsetAsync(w->gr_count, 0, sizeof(int) * (size_t)w->groups_max * GROUP_LISTS, st));
             VXR_CUDA(cudaMemsetAsync(w->gr_fill, 0, sizeof(int) * (size_t)w->groups_max * GROUP_LISTS, st));
             LAUNCHED(7 + 3);  // init, link, flatten, largest, classify, group base, assign, scan
@@ -2841,8 +2854,8 @@ vxr_box_world* vxr_box_create(const vxr_box_config* cfg, int32_t* status) {
     rc |= alloc(w, &w->shown, (size_t)n * SHOWN_STRIDE);
     rc |= alloc(w, &w->counters, 1);
     rc |= alloc(w, &w->totals, 1);
-    // groups the bodies can fill: one a GROUP_BASE placed, plus the last part-filled one
-    w->groups_max = n / GROUP_BASE + 2;
+    // groups the bodies can fill: one for every GROUP_BASE_LEAST placed (the least base), plus the last part-filled one
+    w->groups_max = n / GROUP_BASE_LEAST + 2;
     rc |= alloc(w, &w->scan_tiles,
                 scan_tiles_for(std::max(std::max(n, w->cells), w->groups_max * GROUP_LISTS + 1)) + 1);
     rc |= alloc(w, &w->round_count, ALL_BUCKETS);
@@ -3717,7 +3730,7 @@ int32_t vxr_box_paths(vxr_box_world* w, int32_t* out5) {
     out4[0] = isl ? c.grid_n : w->n;
     out4[1] = isl ? island : 0;
     out4[2] = isl ? c.free_n : 0;
-    out4[3] = isl ? (island + GROUP_BASE - 1) / GROUP_BASE : 0;
+    out4[3] = isl ? (island + group_base_of(island, w->island_blocks) - 1) / group_base_of(island, w->island_blocks) : 0;
     out5[4] = islands_on(w) ? c.largest : 0;
     return VXR_OK;
 }
