@@ -196,8 +196,8 @@ LANDED_STEP = 480
 # is the island kernel and the grid kernel exits at once: its traffic is the island kernel's. Late in the drop (the
 # step after 480, the state saved at step 480 and loaded) one pile holds nearly every body and the grid kernel does
 # the solve; there the pair records outgrow L2. Each launch's own algorithmic bytes are given beside it.
-EARLY_SOLVE_TRAFFIC = {"step": 5, "kernel": "k_islands", "dram_bytes": 45.83e6, "dram_read_bytes": 43.26e6,
-                       "dram_write_bytes": 2.57e6, "algorithmic_bytes": 1.72e9, "ms": 6.74,
+EARLY_SOLVE_TRAFFIC = {"step": 5, "kernel": "k_islands", "dram_bytes": 45.11e6, "dram_read_bytes": 41.78e6,
+                       "dram_write_bytes": 3.33e6, "algorithmic_bytes": 1.72e9, "ms": 5.87,
                        "source": "ncu, one launch, one pass"}
 LATE_SOLVE_TRAFFIC = {"step": 481, "kernel": "k_solve", "dram_bytes": 5.17e9, "dram_read_bytes": 3.76e9,
                       "dram_write_bytes": 1.41e9, "algorithmic_bytes": 7.85e9, "ms": 18.85, "source": "ncu, one launch"}
