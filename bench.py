@@ -56,15 +56,16 @@ class Clocks:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, every_ms: int = 50):
         self.device = device
+        self.every_ms = every_ms
         self.samples = []
         self.proc = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.every_ms)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -1077,7 +1078,9 @@ def main():
         for _ in range(LANDED_STEP // 20):
             wl.step_async(20)
             wl.sync()
-        ms_l = timed_steps(wl, torch.cuda.ExternalStream(wl.stream), flush, args.steps)
+        with Clocks(local) as clocks_l:  # its clocks join the timed window's record
+            ms_l = timed_steps(wl, torch.cuda.ExternalStream(wl.stream), flush, args.steps)
+        clocks.samples += clocks_l.samples
         slow_l = all_max(pg, float(sum(ms_l)))
         landed = {"steps": f"{LANDED_STEP}..{LANDED_STEP + args.steps - 1}", "ms_per_step": slow_l / args.steps,
                   "value": bodies_all * args.steps / (slow_l / 1e3), "touching": wl.last().touching,
