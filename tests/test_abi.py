@@ -68,3 +68,14 @@ def test_static_broad_phase_refuses_a_reach_beyond_the_grid():
     one = ctypes.c_void_p(1)
     for reach in (-1, 7, 645, 1 << 30):
         assert L.vxr_box_broadphase_static(8, dummy, g, reach, 0.0, one, one, 0, one, None) == _lib.VXR_EINVAL
+
+
+def test_measurement_entry_points_refuse_a_missing_world():
+    """The measurement calls (given starts, first substeps, the residual's parts, the list kernel, the island switch)
+    answer a null world with VXR_EINVAL before they touch a device."""
+    L = _lib.lib()
+    assert L.vxr_box_first_substeps(None, 1, 1) == _lib.VXR_EINVAL
+    assert L.vxr_box_learned_given(None, None, 0, 1) == _lib.VXR_EINVAL
+    assert L.vxr_box_residual_parts(None, None, None, 0) == -_lib.VXR_EINVAL
+    assert L.vxr_box_residuals(None, None, 0, None) == -_lib.VXR_EINVAL
+    assert L.vxr_box_learned(None, None, 0) == _lib.VXR_EINVAL
