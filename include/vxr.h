@@ -135,6 +135,14 @@ void* vxr_box_stream(vxr_box_world* world);
 /* The state read back into 13 caller arrays x y z u v w lx ly lz qx qy qz qw: replaces BoxSimulation.state
  * (gui/BoxSimulation.java:153-160). */
 int32_t vxr_box_state(vxr_box_world* world, float* const* out13);
+/* The same read-back without waiting: the state after the steps enqueued so far is split into slot `slot` (0 or 1)
+ * on the device and copied into out13 on a stream of its own, so the next steps run while it travels. The arrays
+ * must stay valid, and should be pinned, until vxr_box_state_wait(world, slot) returns; a slot is reused only after
+ * its copy before has finished. Reads of this kind, one a step into alternating slots, hide the copies behind the
+ * steps. */
+int32_t vxr_box_state_async(vxr_box_world* world, float* const* out13, int32_t slot);
+/* Waits until slot `slot`'s last copy is in the caller's arrays. */
+int32_t vxr_box_state_wait(vxr_box_world* world, int32_t slot);
 
 /* The last step's `shown`, 20 floats a body: replaces BoxSimulation.readShown (gui/BoxSimulation.java:163-165). */
 int32_t vxr_box_read_shown(vxr_box_world* world, float* out);

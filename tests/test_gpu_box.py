@@ -324,3 +324,30 @@ def test_gpu_tiled_list_matches_the_per_thread_walk_through_the_drop():
             assert np.array_equal(x.view(np.int32), y.view(np.int32))
     for w in worlds:
         w.close()
+
+
+def test_gpu_state_read_back_without_waiting_equals_the_waited_one():
+    """Steps read back with vxr_box_state_async into two sets of arrays in turn (each copy travelling while the next
+    step runs) give, step by step, the very words a twin world's waited read-back gives."""
+    a = C.mixed_pile_scene()
+    b = C.mixed_pile_scene()
+    a.start("gpu")
+    b.start("gpu")
+    n = a.n
+    sets = [[np.zeros(n, np.float32) for _ in range(13)] for _ in range(2)]
+    want = []
+    for k in range(6):
+        a.world.step_async(1)
+        a.world.state_async(sets[k % 2], k % 2)
+        b.world.step(1)
+        want.append([x.copy() for x in b.world.state()])
+        if k > 0:
+            a.world.state_wait((k - 1) % 2)
+            for x, y in zip(sets[(k - 1) % 2], want[k - 1]):
+                assert np.array_equal(x.view(np.int32), y.view(np.int32)), f"step {k}"
+    a.world.state_wait(1)
+    for x, y in zip(sets[1], want[5]):
+        assert np.array_equal(x.view(np.int32), y.view(np.int32))
+    a.world.sync()
+    a.close()
+    b.close()

@@ -209,6 +209,10 @@ struct vxr_box_world {
     Totals* host_totals = nullptr;  // pinned
     float* pinned = nullptr;        // pinned staging for state transfers
     float* state13 = nullptr;       // [13 n] the state split into fields, for vxr_box_state
+    // vxr_box_state_async: two slots of split fields, copied out on their own stream while the next step runs
+    float* state_slot[2] = {nullptr, nullptr};
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t slot_split[2] = {nullptr, nullptr}, slot_copied[2] = {nullptr, nullptr};
     size_t pinned_bytes = 0;
     std::vector<void*> allocations;
     long long launches = 0;  // kernels this world has launched
@@ -2986,6 +2990,14 @@ void vxr_box_destroy(vxr_box_world* w) {
     if (w->ev0) cudaEventDestroy(w->ev0);
     if (w->ev1) cudaEventDestroy(w->ev1);
     for (cudaEvent_t e : w->events) cudaEventDestroy(e);
+    if (w->copy_stream) {
+        cudaStreamSynchronize(w->copy_stream);
+        for (int k = 0; k < 2; k++) {
+            cudaEventDestroy(w->slot_split[k]);
+            cudaEventDestroy(w->slot_copied[k]);
+        }
+        cudaStreamDestroy(w->copy_stream);
+    }
     if (w->stream) cudaStreamDestroy(w->stream);
     delete w;
 }
@@ -3474,6 +3486,42 @@ int32_t vxr_box_state(vxr_box_world* w, float* const* out) {
             VXR_CUDA(cudaMemcpyAsync(out[f], w->state13 + (size_t)f * n, sizeof(float) * (size_t)n,
                                      cudaMemcpyDeviceToHost, w->stream));
     VXR_CUDA(cudaStreamSynchronize(w->stream));
+    return VXR_OK;
+}
+
+int32_t vxr_box_state_async(vxr_box_world* w, float* const* out, int32_t slot) {
+    if (!w || !out || slot < 0 || slot > 1) return VXR_EINVAL;
+    cudaSetDevice(w->device);
+    const int n = w->n;
+    if (!w->copy_stream) {
+        if (alloc(w, &w->state_slot[0], (size_t)13 * n) || alloc(w, &w->state_slot[1], (size_t)13 * n))
+            return VXR_ECUDA;
+        VXR_CUDA(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; k++) {
+            VXR_CUDA(cudaEventCreateWithFlags(&w->slot_split[k], cudaEventDisableTiming));
+            VXR_CUDA(cudaEventCreateWithFlags(&w->slot_copied[k], cudaEventDisableTiming));
+        }
+    }
+    // the slot's copy before is done before its fields are written again; the fields split after the steps enqueued
+    // so far, then copied out on the copy stream while the world's stream goes on
+    VXR_CUDA(cudaStreamWaitEvent(w->stream, w->slot_copied[slot], 0));
+    k_state13<<<blocks_for(n, THREADS), THREADS, 0, w->stream>>>(n, w->b, w->state_slot[slot]);  // not a step's launch
+    VXR_CUDA(cudaGetLastError());
+    VXR_CUDA(cudaEventRecord(w->slot_split[slot], w->stream));
+    VXR_CUDA(cudaStreamWaitEvent(w->copy_stream, w->slot_split[slot], 0));
+    for (int f = 0; f < 13; f++)
+        if (out[f])
+            VXR_CUDA(cudaMemcpyAsync(out[f], w->state_slot[slot] + (size_t)f * n, sizeof(float) * (size_t)n,
+                                     cudaMemcpyDeviceToHost, w->copy_stream));
+    VXR_CUDA(cudaEventRecord(w->slot_copied[slot], w->copy_stream));
+    return VXR_OK;
+}
+
+int32_t vxr_box_state_wait(vxr_box_world* w, int32_t slot) {
+    if (!w || slot < 0 || slot > 1) return VXR_EINVAL;
+    if (!w->copy_stream) return VXR_OK;
+    cudaSetDevice(w->device);
+    VXR_CUDA(cudaEventSynchronize(w->slot_copied[slot]));
     return VXR_OK;
 }
 

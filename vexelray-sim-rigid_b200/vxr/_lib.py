@@ -19,7 +19,7 @@ STATUS_NAMES = {0: "VXR_OK", 1: "VXR_EINVAL", 2: "VXR_ECAPACITY", 3: "VXR_EROUND
 #: Every symbol include/vxr.h declares (checked by the CPU test suite).
 SYMBOLS = ["vxr_version", "vxr_box_make_params", "vxr_box_make_grid", "vxr_box_create", "vxr_box_destroy",
            "vxr_box_error", "vxr_box_start", "vxr_box_load_state", "vxr_box_params", "vxr_box_step",
-           "vxr_box_step_async", "vxr_box_sync", "vxr_box_stream", "vxr_box_state", "vxr_box_read_shown",
+           "vxr_box_step_async", "vxr_box_sync", "vxr_box_stream", "vxr_box_state", "vxr_box_state_async", "vxr_box_state_wait", "vxr_box_read_shown",
            "vxr_box_touching", "vxr_box_candidates", "vxr_box_walls", "vxr_box_colour_waves", "vxr_collide",
            "vxr_box_launches", "vxr_box_profile", "vxr_box_activity", "vxr_box_trace", "vxr_box_broadphase_static",
            "vxr_box_measure", "vxr_box_list_kernel", "vxr_box_wait_limit", "vxr_box_islands", "vxr_box_paths", "vxr_box_residuals", "vxr_box_residual_parts", "vxr_box_create_batch", "vxr_box_scene_params",
@@ -140,6 +140,10 @@ def lib() -> ctypes.CDLL:
         L.vxr_box_stream.restype = vp
         L.vxr_box_state.argtypes = [vp, vp]
         L.vxr_box_state.restype = i32
+        L.vxr_box_state_async.argtypes = [vp, vp, i32]
+        L.vxr_box_state_async.restype = i32
+        L.vxr_box_state_wait.argtypes = [vp, i32]
+        L.vxr_box_state_wait.restype = i32
         L.vxr_box_read_shown.argtypes = [vp, vp]
         L.vxr_box_read_shown.restype = i32
         L.vxr_box_touching.argtypes = [vp, vp, vp, vp, vp, vp, i32]

@@ -192,6 +192,19 @@ class BoxSimulation:
         self._check(self.L.vxr_box_state(self.h, ptr_array(out)))
         return out
 
+    def state_async(self, out, slot: int) -> None:
+        """The state after the steps enqueued so far, read back into `out` (13 contiguous float32 arrays of n, best
+        pinned) without waiting: split into slot 0 or 1 on the device and copied on a stream of its own while the next
+        steps run. `out` must stay untouched until state_wait(slot)."""
+        if len(out) != len(STATE_FIELDS) or any(a.dtype != np.float32 or a.shape != (self.n,) or
+                                                 not a.flags.c_contiguous for a in out):
+            raise ValueError(f"out holds {len(STATE_FIELDS)} contiguous float32 arrays of {self.n}")
+        self._check(self.L.vxr_box_state_async(self.h, ptr_array(out), int(slot)))
+
+    def state_wait(self, slot: int) -> None:
+        """Waits until slot `slot`'s last read-back is in its arrays."""
+        self._check(self.L.vxr_box_state_wait(self.h, int(slot)))
+
     def field(self, name: str) -> np.ndarray:
         return self.state()[STATE_FIELDS.index(name)]
 
