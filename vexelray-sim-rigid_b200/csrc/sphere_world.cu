@@ -872,14 +872,16 @@ struct HeldPlaces {
 // One place of a dispatch: solve it if it won the dispatch before (its priority holds both spheres' claims), else
 // clear the spheres' checks and claim them for this dispatch (and note the pass still open). Returns whether it was
 // solved.
+// checked_a, checked_b: the spheres' check words, read by the caller (the claim arrays a dispatch checks are not
+// written while it runs, so they may be read ahead).
 __device__ __forceinline__ bool contact_place(const Kernel& K, const ListGen& L, int c, int2 ab, int checks,
                                               int claims, int pass, int dispatch, int check_dispatch, int rubs,
-                                              const int* checked, int* claimed, int* cleared, bool& open) {
+                                              int checked_a, int checked_b, int* claimed, int* cleared, bool& open) {
     const int pair = ab.x * K.n + ab.y;
     int won = 0;
     if (checks > 0) {
         const int last = priority(pair, check_dispatch);
-        if (checked[ab.x] == last && checked[ab.y] == last) won = 1;
+        if (checked_a == last && checked_b == last) won = 1;
     }
     if (won) {
         contact(K, L.imp + 2 * (size_t)c, ab.x, ab.y, pass, rubs);
@@ -907,18 +909,27 @@ __device__ __forceinline__ void contact_round(const Kernel& K, const ListGen& L,
                                               HeldPlaces& mine) {
     if (gtid == 0) K.counts->open[1 - mark] = 0;
     bool open = false;
+    // the held places' check words, all loaded before the first place is solved
+    int check_a[HELD_PLACES], check_b[HELD_PLACES];
+#pragma unroll
+    for (int j = 0; j < HELD_PLACES; j++) {
+        const bool live = checks > 0 && gtid + j * gsize < listed && !((mine.done >> j) & 1u);
+        check_a[j] = live ? checked[mine.pair[j].x] : 0;
+        check_b[j] = live ? checked[mine.pair[j].y] : 0;
+    }
 #pragma unroll
     for (int j = 0; j < HELD_PLACES; j++) {
         const int c = gtid + j * gsize;
         if (c < listed && !((mine.done >> j) & 1u) &&
-            contact_place(K, L, c, mine.pair[j], checks, claims, pass, dispatch, check_dispatch, rubs, checked,
-                          claimed, cleared, open))
+            contact_place(K, L, c, mine.pair[j], checks, claims, pass, dispatch, check_dispatch, rubs, check_a[j],
+                          check_b[j], claimed, cleared, open))
             mine.done |= 1u << j;
     }
     for (int c = gtid + HELD_PLACES * gsize; c < listed; c += gsize) {
         if (L.done[c] == pass) continue;
-        contact_place(K, L, c, L.pair[c], checks, claims, pass, dispatch, check_dispatch, rubs, checked, claimed,
-                      cleared, open);
+        const int2 ab = L.pair[c];
+        contact_place(K, L, c, ab, checks, claims, pass, dispatch, check_dispatch, rubs,
+                      checks > 0 ? checked[ab.x] : 0, checks > 0 ? checked[ab.y] : 0, claimed, cleared, open);
     }
     // one store a warp that left a place open, not one a place
     if (__any_sync(0xffffffffu, open) && (threadIdx.x & 31) == 0) K.counts->open[mark] = 1;
