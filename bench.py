@@ -958,6 +958,9 @@ def main():
     ap.add_argument("--no-landed", action="store_true", help="large scene: skip the landed-pile window")
     ap.add_argument("--no-islands", action="store_true",
                     help="every body through the grid-wide phases (small components not solved by island blocks)")
+    ap.add_argument("--list-kernel", default="thread", choices=["thread", "tiled"],
+                    help="large scene: the broad phase's list, a thread a body (default) or tiles of cells staged in "
+                         "shared memory; both list the same pairs")
     ap.add_argument("--workload", default="large-mixed",
                     choices=["large-mixed", "sphere-lattice", "batched-scenes", "towers", "sphere-pile"])
     args = ap.parse_args()
@@ -986,6 +989,7 @@ def main():
     if args.cell > 0:
         with_cell(scene, args.cell)
     w = make_world(scene, local, args.max_pairs, args.schedule, args.solve_blocks_per_sm, not args.no_islands)
+    w.list_kernel(args.list_kernel == "tiled")
     if args.load_state:  # a state saved by --save-state: the 13 moving fields; shapes, masses and params the scene's
         z = np.load(args.load_state)
         moving = [z[f"arr_{i}"] for i in range(13)]
@@ -1192,6 +1196,7 @@ def main():
                    "timed_steps": f"{args.warmup}..{args.warmup + args.steps - 1} of the drop",
                    "l2": "flushed (256 MiB write) before every timed step",
                    "schedule": args.schedule, "solve_blocks_per_sm": args.solve_blocks_per_sm,
+                   "list_kernel": args.list_kernel,
                    "parallelism": "replicas" if world_size > 1 else "single"},
         "phase_ms_per_step": {"broad": phases[0] / args.steps, "narrow": phases[1] / args.steps,
                               "colour": phases[2] / args.steps, "solve": phases[3] / args.steps},
