@@ -88,3 +88,21 @@ def test_last_step_keeps_the_colouring_when_the_final_sync_has_nothing_new(steps
     assert last["touching"] > 0 and last["rounds"] > 0
     assert last["steps_reported"] == steps
     assert last["unplaced_total"] == steps and last["unlisted_total"] == 2 * steps
+
+
+def test_clock_samples_give_the_median_the_peak_and_every_throttle_reason_seen():
+    """The clock record a line carries, from nvidia-smi's CSV rows (index, clocks.sm, clocks.max.sm, power, active
+    mask, then the hw_slowdown, hw_thermal_slowdown, sw_thermal_slowdown and sw_power_cap states): the median SM clock
+    under load, the highest maximum, and every reason any sample saw active. Samples of two timed windows merge."""
+    import bench
+    row = lambda sm, hw="Not Active", sw_power="Not Active": ["0", str(sm), "1965", "900.0", "0x0", hw,  # noqa: E731
+                                                              "Not Active", "Not Active", sw_power]
+    a = bench.Clocks(0)
+    a.samples = [row(1965), row(1950, sw_power="Active")]
+    b = bench.Clocks(0)
+    b.samples = [row(1965), row(1800, hw="Active"), row(1965)]
+    a.samples += b.samples
+    s = a.summary()
+    assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0 and s["samples"] == 5
+    assert s["reasons"] == ["hw_slowdown", "sw_power_cap"]
+    assert bench.Clocks(0).summary()["reasons"] == ["unsampled"]
